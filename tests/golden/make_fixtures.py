@@ -1,0 +1,66 @@
+"""Regenerate the golden fixtures under tests/golden/ from the FerriX checkout.
+
+    python tests/golden/make_fixtures.py [path-to-ferrix-checkout]
+
+Writes
+  decks/<name>.inp.gz   gzip copies of the reference's four test decks
+                        (tests/data/*.inp of the FerriX repository), so the
+                        GPU parity tests can run where the checkout is absent;
+  oracle_<name>.npz     the oracle's full displacement vector after every step
+                        of that deck (default initial temperature 20.0, as in
+                        tests/calculix_parity.rs:29,91,187,279);
+  calculix.json         the CalculiX displacement goldens and tolerances that
+                        the reference's tests/calculix_parity.rs asserts.
+"""
+from __future__ import annotations
+
+import gzip
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import inp, static_step  # noqa: E402
+
+DECKS = ["C3D4_staticstep", "C3D4_2staticstep", "NLGEOM_test", "C3D20"]
+
+# tests/calculix_parity.rs:65-70, 125-128, 162-165, 219-222, 254-257, 315-319
+CALCULIX = {
+    "C3D4_staticstep": {"node": 17, "tol": 1e-6, "steps": [[9.356107e-06, -1.313901e-04, 1.719218e-03]]},
+    "C3D4_2staticstep": {"node": 17, "tol": 1e-6, "steps": [[9.356107e-06, -1.313901e-04, 1.719218e-03],
+                                                            [2.603480e-04, -1.377070e-04, 1.001299e-03]]},
+    "NLGEOM_test": {"node": 1, "tol": 5e-3, "steps": [[-9.163880e-02, 3.500324e-01, 1.324598e-01],
+                                                      [8.591845e-01, 3.624377e-01, 2.653401e-01]]},
+    "C3D20": {"node": 17, "tol": 1e-6, "steps": [[5.752112e-02, -2.497816e-04, -8.074951e-03]]},
+}
+
+
+def main(ref: str) -> None:
+    os.makedirs(os.path.join(HERE, "decks"), exist_ok=True)
+    for name in DECKS:
+        src = os.path.join(ref, "tests", "data", name + ".inp")
+        with open(src, "rb") as fh:
+            raw = fh.read()
+        with gzip.GzipFile(os.path.join(HERE, "decks", name + ".inp.gz"), "wb", mtime=0, compresslevel=9) as gz:
+            gz.write(raw)
+        p = inp.parse_inp_text(raw.decode())
+        p.default_initial_temperature = 20.0
+        runner = static_step.Runner(p)
+        state = static_step.new_state(p)
+        timer = inp.SolverTime()
+        out = {"node_ids": np.asarray(p.index_to_node_id, dtype=np.int64)}
+        for k in range(len(p.steps)):
+            runner.solve_step(k, state, timer)
+            out[f"step{k + 1}"] = state.displacements.copy()
+        np.savez_compressed(os.path.join(HERE, f"oracle_{name}.npz"), **out)
+        print(name, "steps", len(p.steps), "dof", len(state.displacements))
+    with open(os.path.join(HERE, "calculix.json"), "w") as fh:
+        json.dump(CALCULIX, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,133 @@
+"""Oracle unit checks pinned to the reference's own unit-test values."""
+import numpy as np
+import pytest
+
+from oracle import elem, inp
+
+
+def test_lut_interpolation():
+    # src/solver/material.rs:285-295
+    lut = inp.LUT()
+    for t, v in [(0.0, 100.0), (100.0, 200.0), (200.0, 400.0)]:
+        lut.push(t, v)
+    t = np.array([d[0] for d in lut.data]); v = np.array([d[1] for d in lut.data])
+    for temp, want in [(-10, 100), (0, 100), (50, 150), (100, 200), (150, 300), (200, 400), (250, 400)]:
+        assert lut.interpolate(temp) == want
+        assert elem.lut_interp(t, v, temp) == want
+
+
+def test_base_material_elastic():
+    # src/solver/material.rs:299-319
+    e = inp.LUT(); nu = inp.LUT()
+    e.push(0.0, 210000.0); e.push(500.0, 150000.0)
+    nu.push(0.0, 0.3); nu.push(500.0, 0.35)
+    assert e.interpolate(0.0) == 210000.0 and nu.interpolate(0.0) == 0.3
+    assert e.interpolate(250.0) == 180000.0
+    assert abs(nu.interpolate(250.0) - 0.325) < 1e-12
+
+
+def test_amplitude_interpolate():
+    # src/solver/amplitude.rs:108-141
+    ts, vs = [0.0, 10.0, 20.0], [0.0, 100.0, 200.0]
+    f = inp.amplitude_interpolate
+    assert abs(f(10.0, ts, vs, 0.0, 0.0) - 100.0) < 1e-15
+    assert abs(f(5.0, ts, vs, 0.0, 0.0) - 50.0) < 1e-15
+    assert abs(f(15.0, ts, vs, 5.0, 20.0) - 120.0) < 1e-15
+    assert f(-10.0, ts, vs, 0.0, 0.0) == 0.0 and f(30.0, ts, vs, 0.0, 0.0) == 200.0
+
+
+def test_preprocess_and_arguments():
+    # src/solver/parser.rs:951-971
+    raw = "**comment\n word  \n \t*keyword\n123.4\n4, 5, 6,\n7, 8, 9"
+    assert inp.preprocess_inp(raw) == "WORD\n*KEYWORD\n123.4\n4, 5, 6, 7, 8, 9\n"
+    assert inp.keyword_arguments("*STEP , INC =  100")["INC"] == "100"
+    assert inp.positional_arguments("0.1, 1, 1E-05, 0.2") == ["0.1", "1", "1E-05", "0.2"]
+    assert "DIRECT" in inp.preprocess_inp("*Static, Solver=Spooles") and \
+        "ITERATIVE" in inp.preprocess_inp("*static, solver=iterative scaling")
+
+
+def test_c3d20_shape_functions():
+    # src/solver/mesh_lib/elements/c3d20.rs:243-266, plus derivative consistency
+    for p in [(0.0, 0.0, 0.0), (0.5, -0.3, 0.8)]:
+        n, _ = elem.shape_c3d20(*p)
+        assert abs(n.sum() - 1.0) < 1e-12
+    n, _ = elem.shape_c3d20(-1.0, -1.0, -1.0)
+    assert abs(n[0] - 1.0) < 1e-12 and np.all(np.abs(n[1:]) < 1e-12)
+    n, _ = elem.shape_c3d20(0.0, -1.0, -1.0)
+    assert abs(n[8] - 1.0) < 1e-12
+    rng = np.random.default_rng(0)
+    for _ in range(5):
+        p = rng.uniform(-1, 1, 3)
+        _, dn = elem.shape_c3d20(*p)
+        assert abs(dn.sum(axis=1)).max() < 1e-12
+        h = 1e-6
+        for d in range(3):
+            q1, q2 = p.copy(), p.copy(); q1[d] += h; q2[d] -= h
+            fd = (elem.shape_c3d20(*q1)[0] - elem.shape_c3d20(*q2)[0]) / (2 * h)
+            assert np.abs(fd - dn[d]).max() < 1e-8
+
+
+def test_gauss_rules():
+    pts, w = elem.gauss_points(20)
+    assert pts.shape == (27, 3) and abs(w.sum() - 8.0) < 1e-12
+    assert tuple(pts[1]) == (-0.774596669241483, -0.774596669241483, 0.0)  # zeta innermost
+    pts, w = elem.gauss_points(4)
+    assert pts.shape == (1, 3) and abs(w[0] - 1 / 6) < 1e-15
+
+
+MAT_DECK = """
+*MATERIAL, NAME=TestMat
+*DENSITY
+1000.0, 0.0
+900.0, 500.0
+*ELASTIC
+210000.0, 0.3, 0.0
+150000.0, 0.35, 500.0
+"""
+
+THERM_DECK = """
+*MATERIAL, NAME=ThermalMat
+*EXPANSION, ZERO=20.0
+1.2E-5, 0.0
+1.5E-5, 500.0
+*INITIAL CONDITIONS, TYPE=TEMPERATURE
+1, 100.0
+"""
+
+
+def test_material_parsing():
+    # tests/material_parsing.rs:5-36
+    p = inp.parse_inp_text(MAT_DECK)
+    assert len(p.materials) == 1 and p.materials[0].name == "TESTMAT"
+    m = p.materials[0]
+    assert [m.density.interpolate(t) for t in (0, 250, 500, 600)] == [1000.0, 950.0, 900.0, 900.0]
+    assert m.youngs_modulus.interpolate(250.0) == 180000.0
+    assert abs(m.poisson_ratio.interpolate(250.0) - 0.325) < 1e-12
+
+
+def test_thermal_parsing():
+    # tests/material_parsing.rs:38-60
+    p = inp.parse_inp_text(THERM_DECK)
+    m = p.materials[0]
+    assert m.reference_temperature == 20.0
+    assert m.thermal_expansion.interpolate(0.0) == 1.2e-5
+    assert m.thermal_expansion.interpolate(250.0) == 1.35e-5
+    assert m.thermal_expansion.interpolate(500.0) == 1.5e-5
+    assert p.initial_temperatures[1] == 100.0
+
+
+def test_parser_errors_and_quirks():
+    with pytest.raises(inp.FerrixError) as ei:
+        inp.parse_inp_text("*ORIENTATION, NAME=X\n")
+    assert ei.value.kind == "UnsupportedKeyword"
+    with pytest.raises(inp.FerrixError) as ei:
+        inp.parse_inp_text("*STEP\n*STATIC, SOLVER=MAGIC\n")
+    assert ei.value.kind == "UnknownSolver"
+    deck = ("*NODE\n1,0,0,0\n2,1,0,0\n*NSET, NSET=A\n1, 2\n*STEP\n*STATIC\n"
+            "*BOUNDARY\nA, 1, 6, 0\n2, 2, 2, 0\n*CLOAD\nA, 3, 5.0\n*NODE PRINT\nU\n*CLOAD\n2, 1, 1.0\n*END STEP\n")
+    p = inp.parse_inp_text(deck)
+    s = p.steps[0]
+    # only the first *BOUNDARY data line is read; DOFs 4-6 dropped
+    assert [(b.node_id, b.dof) for b in s.bcs] == [(1, 0), (1, 1), (1, 2), (2, 0), (2, 1), (2, 2)]
+    # nset CLOAD gives the full value to every node; second *CLOAD continues after *NODE PRINT
+    assert [(l.node_id, l.dof, l.value) for l in s.loads] == [(1, 2, 5.0), (2, 2, 5.0), (2, 0, 1.0)]
