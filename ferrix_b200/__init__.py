@@ -1,0 +1,321 @@
+"""ferrix_b200 — B200 (sm_100a) solver for FerriX's linear-static and NLGEOM
+*STATIC path (C3D4 / C3D20), behind the C ABI of include/ferrix_b200.h.
+
+The Python layer mirrors the reference's host interface so a FerriX test
+reads the same:
+
+    ctx = Context(0)
+    project = Project.from_jobname("tests/data/C3D4_staticstep", ctx)   # src/solver/project.rs:93-127
+    project.default_initial_temperature = 20.0                          # tests/calculix_parity.rs:29
+    state = SolutionState(project.num_dofs, project.num_nodes)          # src/solver/state.rs:32-42
+    state.initialize(project)                                           # src/solver/state.rs:47-79
+    timer = SolverTime()
+    for i, step in enumerate(project.steps):
+        step.solve(i + 1, project, state, writer, timer)                # src/solver/step/steps.rs:28-42
+    idx = project.mesh.get_index_for_node_id(17)
+    ux = state.displacements[idx * 3]
+
+Errors raise FerrixError with the reference's variant name in `.kind`.
+Everything numeric runs in libferrix_b200.so on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import weakref
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import PREC_FP64, PREC_FP64_CSR, PREC_MIXED, SolveOpts, StepStats
+
+__all__ = ["Context", "Project", "SolutionState", "SolverTime", "FerrixError", "SolveOptions", "solve_opts",
+           "batch_solve", "StepStats", "PREC_MIXED", "PREC_FP64", "PREC_FP64_CSR"]
+
+
+class FerrixError(Exception):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.kind = _lib.STATUS_NAMES.get(status, str(status))
+        self.message = message
+        super().__init__(f"{self.kind}: {message}")
+
+
+def _check(rc: int, ctx=None, what: str = ""):
+    if rc != 0:
+        msg = ""
+        if ctx is not None and ctx.handle:
+            msg = (_lib.load().fx_ctx_last_error(ctx.handle) or b"").decode(errors="replace")
+        raise FerrixError(rc, msg or what)
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One GPU and one CUDA stream (fx_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        _check(self.lib.fx_ctx_create(device, C.byref(h)), None, f"fx_ctx_create({device})")
+        self.handle = h
+        self._projects = weakref.WeakSet()  # models must be destroyed before their context
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.fx_ctx_kernel_launches(self.handle))
+
+    def close(self):
+        if self.handle:
+            for p in list(self._projects):
+                p.close()
+            self.lib.fx_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
+               reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
+               reference_iterative: bool = False) -> SolveOpts:
+    o = SolveOpts()
+    _lib.load().fx_default_solve_opts(C.byref(o))
+    o.precision = precision
+    o.rtol = rtol
+    o.max_iter = max_iter
+    o.poll_interval = poll_interval
+    o.reliable_delta = reliable_delta
+    o.use_graphs = int(use_graphs)
+    o.verbose = int(verbose)
+    o.reference_iterative = int(reference_iterative)
+    return o
+
+
+SolveOptions = solve_opts
+
+
+class SolverTime:
+    """Marker mirroring src/solver/time.rs; the running time lives in the model."""
+
+
+class _Mesh:
+    def __init__(self, project: "Project"):
+        self._p = project
+
+    def get_index_for_node_id(self, node_id: int) -> Optional[int]:
+        i = int(self._p.lib.fx_model_node_index(self._p.handle, int(node_id)))
+        return None if i < 0 else i
+
+    @property
+    def index_to_node_id(self) -> np.ndarray:
+        ids = np.empty(self._p.num_nodes, dtype=np.int64)
+        _check(self._p.lib.fx_model_node_ids(self._p.handle, _p(ids)), self._p.ctx)
+        return ids
+
+
+@dataclass
+class StepInfo:
+    nlgeom: bool
+    solver: str
+    increment: tuple
+    n_loads: int
+    n_bcs: int
+
+
+class Step:
+    def __init__(self, project: "Project", index: int):
+        self.project = project
+        self.index = index
+        nl = C.c_int()
+        sv = C.c_int()
+        inc = (C.c_double * 4)()
+        a = C.c_int64()
+        b = C.c_int64()
+        _check(project.lib.fx_model_step_info(project.handle, index, C.byref(nl), C.byref(sv), inc, C.byref(a),
+                                              C.byref(b)), project.ctx)
+        self.info = StepInfo(bool(nl.value), ["DEFAULT", "DIRECT", "ITERATIVE"][sv.value], tuple(inc), a.value,
+                             b.value)
+        self.last_stats: Optional[dict] = None
+
+    def solve(self, step_id: int, project: "Project", solution_state: "SolutionState", writer=None,
+              timer: Optional[SolverTime] = None, opts: Optional[SolveOpts] = None) -> dict:
+        """Step::solve (src/solver/step/steps.rs:28-42) for this step; step_id must be index + 1."""
+        if step_id != self.index + 1:
+            raise ValueError("step_id must be the 1-based position of the step")
+        st = StepStats()
+        o = opts if opts is not None else solve_opts()
+        _check(project.lib.fx_step_solve(project.handle, self.index, C.byref(o), C.byref(st)), project.ctx)
+        self.last_stats = st.as_dict()
+        if writer is not None and hasattr(writer, "write_increment"):
+            writer.write_increment(self.last_stats, timer)
+        return self.last_stats
+
+    def records(self, bcs: bool = False):
+        n = self.info.n_bcs if bcs else self.info.n_loads
+        ids = np.empty(n, dtype=np.int64)
+        dofs = np.empty(n, dtype=np.int32)
+        vals = np.empty(n, dtype=np.float64)
+        org = np.empty(n, dtype=np.int64)
+        tab = np.empty(n, dtype=np.int32)
+        _check(self.project.lib.fx_model_step_records(self.project.handle, self.index, int(bcs), _p(ids), _p(dofs),
+                                                      _p(vals), _p(org), _p(tab)), self.project.ctx)
+        return ids, dofs, vals, org, tab
+
+
+class Project:
+    """fx_model: the parsed deck plus its device-resident solution state."""
+
+    def __init__(self, handle, ctx: Optional[Context]):
+        self.lib = _lib.load()
+        self.handle = handle
+        self.ctx = ctx
+        nn = C.c_int64()
+        ne = C.c_int64()
+        ns = C.c_int()
+        nm = C.c_int()
+        _check(self.lib.fx_model_sizes(handle, C.byref(nn), C.byref(ne), C.byref(ns), C.byref(nm)), ctx)
+        self.num_nodes = nn.value
+        self.num_elements = ne.value
+        self.num_dofs = 3 * nn.value
+        self.num_materials = nm.value
+        self.mesh = _Mesh(self)
+        self.steps: List[Step] = [Step(self, k) for k in range(ns.value)]
+        self._default_t = 0.0
+        if ctx is not None:
+            ctx._projects.add(self)
+
+    @classmethod
+    def from_inp_text(cls, text: str, ctx: Optional[Context] = None) -> "Project":
+        lib = _lib.load()
+        raw = text.encode()
+        h = C.c_void_p()
+        _check(lib.fx_model_from_inp(ctx.handle if ctx else None, raw, len(raw), C.byref(h)), ctx)
+        return cls(h, ctx)
+
+    @classmethod
+    def from_jobname(cls, jobname: str, ctx: Optional[Context] = None) -> "Project":
+        path = jobname if jobname.lower().endswith(".inp") else jobname + ".inp"
+        try:
+            with open(path, "r") as fh:
+                text = fh.read()
+        except OSError as e:
+            raise FerrixError(1, f"IO error at {path}: {e}")
+        return cls.from_inp_text(text, ctx)
+
+    @property
+    def default_initial_temperature(self) -> float:
+        return self._default_t
+
+    @default_initial_temperature.setter
+    def default_initial_temperature(self, t: float) -> None:
+        self._default_t = float(t)
+        _check(self.lib.fx_model_set_default_temperature(self.handle, float(t)), self.ctx)
+
+    def export(self):
+        """Dense arrays: xyz (N,3), {4: (conn, mat), 20: (conn, mat)}."""
+        xyz = np.empty(3 * self.num_nodes)
+        n4 = C.c_int64()
+        n20 = C.c_int64()
+        _check(self.lib.fx_model_export(self.handle, None, C.byref(n4), None, None, C.byref(n20), None, None), self.ctx)
+        c4 = np.empty(4 * n4.value, dtype=np.int32)
+        m4 = np.empty(n4.value, dtype=np.int32)
+        c20 = np.empty(20 * n20.value, dtype=np.int32)
+        m20 = np.empty(n20.value, dtype=np.int32)
+        _check(self.lib.fx_model_export(self.handle, _p(xyz), C.byref(n4), _p(c4), _p(m4), C.byref(n20), _p(c20),
+                                        _p(m20)), self.ctx)
+        return xyz.reshape(-1, 3), {4: (c4.reshape(-1, 4), m4), 20: (c20.reshape(-1, 20), m20)}
+
+    def assemble_csr(self, u: Optional[np.ndarray] = None, precision: int = PREC_FP64):
+        """Assembler::assemble + to_csr on the GPU: (indptr, indices, data, maxdiag)."""
+        nnz = C.c_int64()
+        uu = None if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        _check(self.lib.fx_assemble_csr(self.handle, _p(uu), precision, C.byref(nnz), None, None, None, None),
+               self.ctx)
+        ip = np.empty(self.num_dofs + 1, dtype=np.int64)
+        ind = np.empty(nnz.value, dtype=np.int64)
+        dat = np.empty(nnz.value, dtype=np.float64)
+        md = C.c_double()
+        _check(self.lib.fx_assemble_csr(self.handle, _p(uu), precision, C.byref(nnz), _p(ip), _p(ind), _p(dat),
+                                        C.byref(md)), self.ctx)
+        return ip, ind, dat, md.value
+
+    def internal_force(self, u: np.ndarray, uconf: Optional[np.ndarray] = None) -> np.ndarray:
+        f = np.empty(self.num_dofs)
+        uu = np.ascontiguousarray(u, dtype=np.float64)
+        uc = None if uconf is None else np.ascontiguousarray(uconf, dtype=np.float64)
+        _check(self.lib.fx_internal_force(self.handle, _p(uu), _p(uc), _p(f)), self.ctx)
+        return f
+
+    def thermal_force(self) -> np.ndarray:
+        f = np.empty(self.num_dofs)
+        _check(self.lib.fx_thermal_force(self.handle, _p(f)), self.ctx)
+        return f
+
+    def close(self):
+        if self.handle:
+            self.lib.fx_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolutionState:
+    """SolutionState (src/solver/state.rs:16-79); the vectors stay on the GPU."""
+
+    def __init__(self, num_dofs: int = 0, num_nodes: int = 0):
+        self.num_dofs = num_dofs
+        self.num_nodes = num_nodes
+        self.project: Optional[Project] = None
+
+    def initialize(self, project: Project) -> None:
+        self.project = project
+        _check(project.lib.fx_state_initialize(project.handle), project.ctx)
+
+    @property
+    def displacements(self) -> np.ndarray:
+        u = np.empty(self.project.num_dofs)
+        _check(self.project.lib.fx_state_get_displacements(self.project.handle, _p(u)), self.project.ctx)
+        return u
+
+    @displacements.setter
+    def displacements(self, u: np.ndarray) -> None:
+        uu = np.ascontiguousarray(u, dtype=np.float64)
+        _check(self.project.lib.fx_state_set_displacements(self.project.handle, _p(uu)), self.project.ctx)
+
+    @property
+    def temperatures(self):
+        ti = np.empty(self.project.num_nodes)
+        tc = np.empty(self.project.num_nodes)
+        _check(self.project.lib.fx_state_get_temperatures(self.project.handle, _p(ti), _p(tc)), self.project.ctx)
+        return ti, tc
+
+    def set_temperatures(self, t_init: Optional[np.ndarray] = None, t_cur: Optional[np.ndarray] = None) -> None:
+        a = None if t_init is None else np.ascontiguousarray(t_init, dtype=np.float64)
+        b = None if t_cur is None else np.ascontiguousarray(t_cur, dtype=np.float64)
+        _check(self.project.lib.fx_state_set_temperatures(self.project.handle, _p(a), _p(b)), self.project.ctx)
+
+
+def batch_solve(ctx: Context, projects: Sequence[Project], opts: Optional[SolveOpts] = None):
+    """First step of every (initialized) project with the linear solves batched; returns (status, stats)."""
+    lib = _lib.load()
+    n = len(projects)
+    arr = (C.c_void_p * n)(*[p.handle for p in projects])
+    st = np.zeros(n, dtype=np.int32)
+    stats = (StepStats * n)()
+    o = opts if opts is not None else solve_opts()
+    rc = lib.fx_batch_solve(ctx.handle, C.cast(arr, C.c_void_p), n, C.byref(o), _p(st), C.cast(stats, C.c_void_p))
+    if rc != 0 and not np.any(st != 0):
+        _check(rc, ctx)
+    return st, [s.as_dict() for s in stats]

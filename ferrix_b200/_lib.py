@@ -1,0 +1,98 @@
+"""ctypes binding of libferrix_b200.so (declarations in include/ferrix_b200.h).
+
+The shared library is built in-tree by ferrix_b200/build.py. There is no
+fallback: if the library cannot be loaded, importing the solver API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libferrix_b200.so")
+
+STATUS_NAMES = {
+    0: "Ok", 1: "Io", 2: "GenericIo", 3: "ParseError", 4: "UnsupportedKeyword", 5: "UnknownSolver",
+    6: "NodeNotFound", 7: "ElementNotFound", 8: "MaterialNotFound", 9: "ElsetNotFound", 10: "NsetNotFound",
+    11: "NumericalError", 12: "ConvergenceError", 13: "InvalidModelState", 14: "Generic", 15: "Cancelled",
+    16: "Timeout", 17: "Cuda", 18: "InvalidArgument",
+}
+
+PREC_MIXED = 0
+PREC_FP64 = 1
+PREC_FP64_CSR = 2
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("rtol", C.c_double), ("max_iter", C.c_int), ("poll_interval", C.c_int),
+                ("reliable_delta", C.c_double), ("use_graphs", C.c_int), ("verbose", C.c_int),
+                ("reference_iterative", C.c_int)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("increments", C.c_int), ("newton_iterations", C.c_int), ("linear_solves", C.c_int),
+                ("pcg_iterations", C.c_longlong), ("reliable_updates", C.c_int),
+                ("last_rel_residual", C.c_double), ("last_linear_relres", C.c_double),
+                ("t_symbolic_ms", C.c_double), ("t_assembly_ms", C.c_double), ("t_forces_ms", C.c_double),
+                ("t_pcg_ms", C.c_double), ("t_total_ms", C.c_double), ("bsr_blocks", C.c_int64),
+                ("fp64_fallbacks", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# name -> (restype, argtypes); every symbol of include/ferrix_b200.h
+P = C.c_void_p
+I64P = C.POINTER(C.c_int64)
+SIGNATURES = {
+    "fx_default_solve_opts": (None, [C.POINTER(SolveOpts)]),
+    "fx_ctx_create": (C.c_int, [C.c_int, C.POINTER(P)]),
+    "fx_ctx_destroy": (None, [P]),
+    "fx_ctx_last_error": (C.c_char_p, [P]),
+    "fx_ctx_kernel_launches": (C.c_int64, [P]),
+    "fx_model_from_inp": (C.c_int, [P, C.c_char_p, C.c_size_t, C.POINTER(P)]),
+    "fx_model_destroy": (None, [P]),
+    "fx_model_sizes": (C.c_int, [P, I64P, I64P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "fx_model_node_ids": (C.c_int, [P, P]),
+    "fx_model_node_index": (C.c_int64, [P, C.c_int64]),
+    "fx_model_set_default_temperature": (C.c_int, [P, C.c_double]),
+    "fx_model_step_info": (C.c_int, [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), P, I64P, I64P]),
+    "fx_model_export": (C.c_int, [P, P, I64P, P, P, I64P, P, P]),
+    "fx_model_step_records": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P]),
+    "fx_state_initialize": (C.c_int, [P]),
+    "fx_state_get_displacements": (C.c_int, [P, P]),
+    "fx_state_set_displacements": (C.c_int, [P, P]),
+    "fx_state_get_temperatures": (C.c_int, [P, P, P]),
+    "fx_state_set_temperatures": (C.c_int, [P, P, P]),
+    "fx_step_solve": (C.c_int, [P, C.c_int, C.POINTER(SolveOpts), C.POINTER(StepStats)]),
+    "fx_assemble_csr": (C.c_int, [P, P, C.c_int, I64P, P, P, P, C.POINTER(C.c_double)]),
+    "fx_internal_force": (C.c_int, [P, P, P, P]),
+    "fx_thermal_force": (C.c_int, [P, P]),
+    "fx_solve_csr": (C.c_int, [P, C.c_int64, P, P, P, P, P, C.POINTER(SolveOpts), C.POINTER(StepStats)]),
+    "fx_batch_solve": (C.c_int, [P, P, C.c_int, C.POINTER(SolveOpts), P, P]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the library (once). Raises OSError when it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"{path} not built; run `python -m ferrix_b200.build`")
+        lib = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def header_symbols(header: str) -> list:
+    """Names of the functions declared in include/ferrix_b200.h."""
+    import re
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fx_[a-z0-9_]+)\s*\(", text)))

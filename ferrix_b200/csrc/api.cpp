@@ -1,0 +1,341 @@
+// extern "C" boundary (include/ferrix_b200.h). Every entry point converts
+// fx::Error / CUDA failures into an fx_status and keeps the message for
+// fx_ctx_last_error.
+#include <cstring>
+#include <new>
+
+#include "engine.hpp"
+
+using namespace fx;
+
+template <typename F>
+static int guarded(fx_ctx* ctx, F&& f) {
+    try {
+        return f();
+    } catch (const fx::Error& e) {
+        if (ctx) ctx->last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->last_error = "host allocation failed";
+        return FX_GENERIC;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->last_error = e.what();
+        return FX_GENERIC;
+    }
+}
+
+extern "C" {
+
+void fx_default_solve_opts(fx_solve_opts* o) {
+    if (!o) return;
+    o->precision = FX_PREC_MIXED;
+    o->rtol = 1e-8;
+    o->max_iter = 50000;
+    o->poll_interval = 32;
+    o->reliable_delta = 1e-2;
+    o->use_graphs = 1;
+    o->verbose = 0;
+    o->reference_iterative = 0;
+}
+
+int fx_ctx_create(int device, fx_ctx** out) {
+    if (!out) return FX_INVALID_ARGUMENT;
+    *out = nullptr;
+    fx_ctx* c = new (std::nothrow) fx_ctx();
+    if (!c) return FX_GENERIC;
+    int rc = guarded(c, [&] {
+        int n = 0;
+        FX_CUDA_CHECK(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) fail(FX_INVALID_ARGUMENT, "no such CUDA device");
+        c->device = device;
+        FX_CUDA_CHECK(cudaSetDevice(device));
+        FX_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->tables.init(c->stream);
+        return FX_OK;
+    });
+    if (rc != FX_OK) {
+        fx_ctx_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return FX_OK;
+}
+
+void fx_ctx_destroy(fx_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaStream_t s = ctx->stream;
+    ctx->stream = nullptr;
+    delete ctx;  // buffers free on their own streams
+    if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+}
+
+const char* fx_ctx_last_error(const fx_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int64_t fx_ctx_kernel_launches(const fx_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int fx_model_from_inp(fx_ctx* ctx, const char* text, size_t len, fx_model** out) {
+    if (!out || (!text && len)) return FX_INVALID_ARGUMENT;
+    *out = nullptr;
+    return guarded(ctx, [&] {
+        fx_model* m = new fx_model();
+        m->ctx = ctx;
+        try {
+            m->project = parse_inp(std::string(text ? text : "", len));
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+        return FX_OK;
+    });
+}
+
+int fx_model_export(fx_model* m, double* xyz, int64_t* n4, int32_t* conn4, int32_t* mat4, int64_t* n20,
+                    int32_t* conn20, int32_t* mat20) {
+    if (!m) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        ensure_dense(m);
+        const DenseModel& D = m->dense;
+        if (xyz) std::memcpy(xyz, D.xyz.data(), D.xyz.size() * sizeof(double));
+        if (n4) *n4 = D.g4.size();
+        if (n20) *n20 = D.g20.size();
+        if (conn4) std::memcpy(conn4, D.g4.conn.data(), D.g4.conn.size() * sizeof(int32_t));
+        if (mat4) std::memcpy(mat4, D.g4.mat.data(), D.g4.mat.size() * sizeof(int32_t));
+        if (conn20) std::memcpy(conn20, D.g20.conn.data(), D.g20.conn.size() * sizeof(int32_t));
+        if (mat20) std::memcpy(mat20, D.g20.mat.data(), D.g20.mat.size() * sizeof(int32_t));
+        return FX_OK;
+    });
+}
+
+int fx_model_step_records(const fx_model* m, int k, int is_bc, int64_t* ids, int32_t* dofs, double* vals,
+                          int64_t* origin, int32_t* tab) {
+    if (!m || k < 0 || k >= (int)m->project.steps.size()) return FX_INVALID_ARGUMENT;
+    const auto& recs = is_bc ? m->project.steps[k].bcs : m->project.steps[k].loads;
+    for (size_t i = 0; i < recs.size(); ++i) {
+        if (ids) ids[i] = recs[i].node_id;
+        if (dofs) dofs[i] = recs[i].dof;
+        if (vals) vals[i] = recs[i].value;
+        if (origin) origin[i] = recs[i].origin_step;
+        if (tab) tab[i] = recs[i].amp && recs[i].amp->has_data ? 1 : 0;
+    }
+    return FX_OK;
+}
+
+void fx_model_destroy(fx_model* m) {
+    if (!m) return;
+    if (m->ctx) {
+        cudaSetDevice(m->ctx->device);
+        cudaStreamSynchronize(m->ctx->stream);
+    }
+    delete m;
+}
+
+int fx_model_sizes(const fx_model* m, int64_t* nn, int64_t* ne, int* ns, int* nm) {
+    if (!m) return FX_INVALID_ARGUMENT;
+    if (nn) *nn = (int64_t)m->project.nodes.size();
+    if (ne) *ne = (int64_t)m->project.elements.size();
+    if (ns) *ns = (int)m->project.steps.size();
+    if (nm) *nm = (int)m->project.materials.size();
+    return FX_OK;
+}
+
+int fx_model_node_ids(const fx_model* m, int64_t* ids) {
+    if (!m || !ids) return FX_INVALID_ARGUMENT;
+    std::memcpy(ids, m->project.index_to_node_id.data(), m->project.index_to_node_id.size() * sizeof(int64_t));
+    return FX_OK;
+}
+
+int64_t fx_model_node_index(const fx_model* m, int64_t id) { return m ? m->project.index_of(id) : -1; }
+
+int fx_model_set_default_temperature(fx_model* m, double t) {
+    if (!m) return FX_INVALID_ARGUMENT;
+    m->project.default_initial_temperature = t;
+    return FX_OK;
+}
+
+int fx_model_step_info(const fx_model* m, int k, int* nlgeom, int* solver, double incr[4], int64_t* nl,
+                       int64_t* nb) {
+    if (!m || k < 0 || k >= (int)m->project.steps.size()) return FX_INVALID_ARGUMENT;
+    const StaticStep& s = m->project.steps[k];
+    if (nlgeom) *nlgeom = s.nlgeom ? 1 : 0;
+    if (solver) *solver = (int)s.solver;
+    if (incr) {
+        incr[0] = s.inc.initial;
+        incr[1] = s.inc.period;
+        incr[2] = s.inc.min_inc;
+        incr[3] = s.inc.max_inc;
+    }
+    if (nl) *nl = (int64_t)s.loads.size();
+    if (nb) *nb = (int64_t)s.bcs.size();
+    return FX_OK;
+}
+
+int fx_state_initialize(fx_model* m) {
+    if (!m || !m->ctx) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        state_initialize(m);
+        return FX_OK;
+    });
+}
+
+int fx_state_get_displacements(const fx_model* m, double* u) {
+    if (!m || !u) return FX_INVALID_ARGUMENT;
+    if (!m->state_ready) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        m->dev.u.download(u, 3 * (size_t)m->dense.n_nodes, m->ctx->stream);
+        FX_CUDA_CHECK(cudaStreamSynchronize(m->ctx->stream));
+        return FX_OK;
+    });
+}
+
+int fx_state_set_displacements(fx_model* m, const double* u) {
+    if (!m || !u || !m->state_ready) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        FX_CUDA_CHECK(cudaMemcpyAsync(m->dev.u.ptr, u, 3 * (size_t)m->dense.n_nodes * sizeof(double),
+                                      cudaMemcpyHostToDevice, m->ctx->stream));
+        FX_CUDA_CHECK(cudaStreamSynchronize(m->ctx->stream));
+        return FX_OK;
+    });
+}
+
+int fx_state_get_temperatures(const fx_model* m, double* ti, double* tc) {
+    if (!m || !m->state_ready) return FX_INVALID_ARGUMENT;
+    if (ti) std::memcpy(ti, m->t_init.data(), m->t_init.size() * sizeof(double));
+    if (tc) std::memcpy(tc, m->t_cur.data(), m->t_cur.size() * sizeof(double));
+    return FX_OK;
+}
+
+int fx_state_set_temperatures(fx_model* m, const double* ti, const double* tc) {
+    if (!m || !m->state_ready) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        const size_t n = (size_t)m->dense.n_nodes;
+        if (ti) m->t_init.assign(ti, ti + n);
+        if (tc) m->t_cur.assign(tc, tc + n);
+        m->dev.tinit.upload(m->t_init, m->ctx->stream);
+        m->dev.tcur.upload(m->t_cur, m->ctx->stream);
+        FX_CUDA_CHECK(cudaStreamSynchronize(m->ctx->stream));
+        return FX_OK;
+    });
+}
+
+int fx_step_solve(fx_model* m, int k, const fx_solve_opts* opts, fx_step_stats* st) {
+    if (!m || !m->ctx) return FX_INVALID_ARGUMENT;
+    fx_solve_opts o;
+    if (opts) o = *opts;
+    else fx_default_solve_opts(&o);
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        return step_solve(m, k, o, st);
+    });
+}
+
+int fx_assemble_csr(fx_model* m, const double* u, int precision, int64_t* nnz, int64_t* indptr, int64_t* indices,
+                    double* data, double* maxdiag) {
+    if (!m || !nnz) return FX_INVALID_ARGUMENT;
+    if (!m->state_ready) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        fx_ctx* ctx = m->ctx;
+        int64_t* saved = g_launch_counter;
+        g_launch_counter = &ctx->launches;
+        struct R {
+            int64_t* v;
+            ~R() { g_launch_counter = v; }
+        } r{saved};
+        ensure_dense(m);
+        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        ensure_structure(m);
+        ModelDev& d = m->dev;
+        cudaStream_t s = ctx->stream;
+        const int64_t nn = m->dense.n_nodes;
+        std::vector<int32_t> rp(nn + 1);
+        d.S.row_ptr.download(rp.data(), nn + 1, s);
+        FX_CUDA_CHECK(cudaStreamSynchronize(s));
+        std::vector<int64_t> ip(3 * nn + 1, 0);
+        for (int64_t i = 0; i < nn; ++i)
+            for (int rr = 0; rr < 3; ++rr) ip[3 * i + rr + 1] = ip[3 * i + rr] + 3 * (int64_t)(rp[i + 1] - rp[i]);
+        *nnz = ip[3 * nn];
+        if (!indptr || !indices || !data) return FX_OK;
+        DBuf<double> du;
+        const double* dptr = nullptr;
+        if (u) {
+            du.upload(u, 3 * (size_t)nn, s);
+            dptr = du.ptr;
+        }
+        double md = assemble(m, dptr, precision == FX_PREC_FP64);
+        if (maxdiag) *maxdiag = md;
+        DBuf<int64_t> dip, dind;
+        DBuf<double> ddat;
+        dip.upload(ip, s);
+        dind.alloc(*nnz, s);
+        ddat.alloc(*nnz, s);
+        if (precision == FX_PREC_FP64) launch_bsr_to_csr<double>(d.S, d.vals64.ptr, dip.ptr, dind.ptr, ddat.ptr, s);
+        else launch_bsr_to_csr<float>(d.S, d.vals32.ptr, dip.ptr, dind.ptr, ddat.ptr, s);
+        std::memcpy(indptr, ip.data(), ip.size() * sizeof(int64_t));
+        dind.download(indices, *nnz, s);
+        ddat.download(data, *nnz, s);
+        FX_CUDA_CHECK(cudaStreamSynchronize(s));
+        return FX_OK;
+    });
+}
+
+static int force_common(fx_model* m, const double* u, const double* uconf, double* f, bool thermal) {
+    if (!m || !f || (!thermal && !u) || !m->state_ready) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        fx_ctx* ctx = m->ctx;
+        int64_t* saved = g_launch_counter;
+        g_launch_counter = &ctx->launches;
+        struct R {
+            int64_t* v;
+            ~R() { g_launch_counter = v; }
+        } r{saved};
+        ensure_dense(m);
+        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        ensure_structure(m);
+        cudaStream_t s = ctx->stream;
+        const size_t n3 = 3 * (size_t)m->dense.n_nodes;
+        DBuf<double> du, duc, out;
+        out.alloc(n3, s);
+        if (thermal) {
+            compute_thermal_force(m, out.ptr);
+        } else {
+            du.upload(u, n3, s);
+            if (uconf) duc.upload(uconf, n3, s);
+            compute_internal_force(m, du.ptr, uconf ? duc.ptr : nullptr, out.ptr);
+        }
+        check_device_errors(m, thermal ? "thermal force" : "internal force");
+        out.download(f, n3, s);
+        FX_CUDA_CHECK(cudaStreamSynchronize(s));
+        return FX_OK;
+    });
+}
+
+int fx_internal_force(fx_model* m, const double* u, const double* uconf, double* f) {
+    return force_common(m, u, uconf, f, false);
+}
+
+int fx_thermal_force(fx_model* m, double* f) { return force_common(m, nullptr, nullptr, f, true); }
+
+int fx_batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts* opts, int* status,
+                   fx_step_stats* stats) {
+    if (!ctx || (!models && n)) return FX_INVALID_ARGUMENT;
+    fx_solve_opts o;
+    if (opts) o = *opts;
+    else fx_default_solve_opts(&o);
+    return guarded(ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(ctx->device));
+        return batch_solve(ctx, models, n, o, status, stats);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,94 @@
+// Context / model objects behind the C ABI and the device-resident static
+// step driver.
+#pragma once
+
+#include <memory>
+#include <string>
+
+#include "kernels.hpp"
+#include "model.hpp"
+#include "pcg.hpp"
+#include "pcg_csr.hpp"
+
+struct fx_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    fx::DeviceTables tables;
+    std::string last_error;
+    int64_t launches = 0;
+    fx::PcgBatch<float> pcg32;
+    fx::PcgBatch<double> pcg64;
+    fx::CsrPcg pcgcsr;
+};
+
+namespace fx {
+
+struct MatTableDev {
+    DBuf<int32_t> e_off, e_len, nu_off, nu_len, a_off, a_len;
+    DBuf<double> tref, t, v;
+    int n_mat = 0;
+    MatDev view() const {
+        return MatDev{e_off.ptr, e_len.ptr, nu_off.ptr, nu_len.ptr, a_off.ptr, a_len.ptr, tref.ptr, t.ptr, v.ptr,
+                      n_mat};
+    }
+};
+
+// Penalty / mask / load data of one step, merged per DOF on the host.
+struct StepBc {
+    std::vector<int32_t> dof;            // unique constrained DOFs, ascending
+    std::vector<double> cnt;             // records per DOF
+    std::vector<std::vector<int>> recs;  // record indices per DOF (for target sums)
+    DBuf<int32_t> d_dof;
+    DBuf<double> d_cnt, d_usum;
+    DBuf<uint8_t> d_mask;
+};
+
+struct ModelDev {
+    bool uploaded = false;
+    DBuf<double> xyz, tinit, tcur;
+    DBuf<int32_t> conn4, conn20, mat4, mat20;
+    MatTableDev mats;
+    bool have_structure = false;
+    BsrStructure S;
+    DBuf<float> ebuf32, vals32, minv32;
+    DBuf<double> ebuf64, vals64, minv64;
+    DBuf<double> fe, u, ustart, du, fext, ftmp, fint, R, r64, ax;
+    DBuf<unsigned long long> maxdiag;
+    DBuf<int> err;
+    DBuf<double> norm_part, norm_out;
+    DBuf<int32_t> load_dof;
+    DBuf<double> load_val;
+    ElemView g4() const { return ElemView{(int)conn4.n / 4, conn4.ptr, mat4.ptr}; }
+    ElemView g20() const { return ElemView{(int)conn20.n / 20, conn20.ptr, mat20.ptr}; }
+};
+
+}  // namespace fx
+
+struct fx_model {
+    fx_ctx* ctx = nullptr;
+    fx::Project project;
+    fx::DenseModel dense;
+    bool dense_built = false;
+    bool state_ready = false;
+    std::vector<double> t_init, t_cur;  // SolutionState temperatures
+    fx::SolverTime timer;
+    fx::ModelDev dev;
+};
+
+namespace fx {
+
+void ensure_dense(fx_model* m);
+void upload_model(fx_model* m);
+void ensure_structure(fx_model* m);
+void state_initialize(fx_model* m);
+// element loops
+void compute_internal_force(fx_model* m, const double* d_u, const double* d_uconf, double* d_out);
+void compute_thermal_force(fx_model* m, double* d_out);
+// assembles K (precision) at X (+d_u) into dev.vals32/vals64; returns maxdiag (host copy)
+double assemble(fx_model* m, const double* d_u, bool fp64);
+void check_device_errors(fx_model* m, const char* where);
+int step_solve(fx_model* m, int step_index, const fx_solve_opts& opts, fx_step_stats* stats);
+int batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts& opts, int* status,
+                fx_step_stats* stats);
+
+}  // namespace fx

@@ -1,0 +1,655 @@
+// `.inp` preprocessing and keyword parser with the semantics of FerriX's
+// src/solver/parser.rs (keyword state machine :111-482, data lines :484-876,
+// argument helpers :879-894, preprocessing :903-942), node / element line
+// parsing (mesh_lib/node.rs:25-35, mesh_lib/elements/element.rs:62-131) and
+// the node mapping of mesh_lib/mesh.rs:35-50.
+//
+// Reproduced behaviour: only the first data line after *BOUNDARY and
+// *AMPLITUDE is read; data following an ignored keyword is dropped; DOFs 4-6
+// are dropped; a *CLOAD on an nset gives the full value to every node; loads
+// and BCs carry over between steps unless OP=NEW; unknown keywords are an
+// error. Case folding is ASCII (decks are ASCII).
+#include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <unordered_set>
+
+#include "common.hpp"
+#include "model.hpp"
+
+namespace fx {
+
+// ------------------------------------------------------------------ helpers
+
+static inline bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n' || c == '\v' || c == '\f'; }
+
+static std::string trim(const std::string& s) {
+    size_t a = 0, b = s.size();
+    while (a < b && is_ws(s[a])) ++a;
+    while (b > a && is_ws(s[b - 1])) --b;
+    return s.substr(a, b - a);
+}
+
+static std::vector<std::string> split(const std::string& s, char sep) {
+    std::vector<std::string> out;
+    size_t start = 0;
+    for (size_t i = 0; i <= s.size(); ++i) {
+        if (i == s.size() || s[i] == sep) {
+            out.push_back(s.substr(start, i - start));
+            start = i + 1;
+        }
+    }
+    return out;
+}
+
+static bool starts_with(const std::string& s, const char* p) { return s.rfind(p, 0) == 0; }
+
+// f64::from_str: decimal / exponent forms, inf / infinity / nan; nothing else.
+static bool parse_f64(const std::string& s, double* out) {
+    if (s.empty()) return false;
+    std::string low;
+    for (char c : s) low.push_back((char)std::tolower((unsigned char)c));
+    size_t i = (low[0] == '+' || low[0] == '-') ? 1 : 0;
+    std::string body = low.substr(i);
+    if (body == "inf" || body == "infinity" || body == "nan") {
+        double v = body == "nan" ? NAN : INFINITY;
+        *out = low[0] == '-' ? -v : v;
+        return true;
+    }
+    bool digit = false;
+    for (size_t k = i; k < low.size(); ++k) {
+        char c = low[k];
+        if (std::isdigit((unsigned char)c)) digit = true;
+        else if (!(c == '.' || c == 'e' || c == '+' || c == '-')) return false;
+    }
+    if (!digit) return false;
+    char* end = nullptr;
+    errno = 0;
+    double v = std::strtod(s.c_str(), &end);
+    if (end != s.c_str() + s.size()) return false;
+    *out = v;
+    return true;
+}
+
+// usize::from_str: optional '+', ASCII digits, no overflow.
+static bool parse_usize(const std::string& s, int64_t* out) {
+    size_t i = 0;
+    if (!s.empty() && s[0] == '+') i = 1;
+    if (i >= s.size()) return false;
+    uint64_t v = 0;
+    for (; i < s.size(); ++i) {
+        if (!std::isdigit((unsigned char)s[i])) return false;
+        uint64_t d = (uint64_t)(s[i] - '0');
+        if (v > (UINT64_MAX - d) / 10) return false;
+        v = v * 10 + d;
+    }
+    if (v > (uint64_t)INT64_MAX) return false;
+    *out = (int64_t)v;
+    return true;
+}
+
+// get_keyword_arguments (parser.rs:879-890): later duplicates win.
+using KwArgs = std::unordered_map<std::string, std::pair<bool, std::string>>;  // key -> (has value, value)
+static KwArgs keyword_arguments(const std::string& line) {
+    KwArgs out;
+    auto parts = split(line, ',');
+    for (size_t i = 1; i < parts.size(); ++i) {
+        const std::string& s = parts[i];
+        size_t eq = s.find('=');
+        if (eq != std::string::npos) out[trim(s.substr(0, eq))] = {true, trim(s.substr(eq + 1))};
+        else out[trim(s)] = {false, std::string()};
+    }
+    return out;
+}
+static const std::string* kw_value(const KwArgs& a, const char* key) {
+    auto it = a.find(key);
+    if (it == a.end() || !it->second.first) return nullptr;
+    return &it->second.second;
+}
+
+// ------------------------------------------------------------------ model helpers
+
+void Lut::push(double t, double v) {
+    data.emplace_back(t, v);
+    std::stable_sort(data.begin(), data.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+}
+
+double Lut::interpolate(double temp) const {  // material.rs:36-68
+    if (data.size() == 1 || temp <= data[0].first) return data[0].second;
+    if (temp >= data.back().first) return data.back().second;
+    size_t lo = 0, hi = data.size() - 1;
+    while (hi - lo > 1) {
+        size_t mid = lo + (hi - lo) / 2;
+        if (data[mid].first <= temp) lo = mid;
+        else hi = mid;
+    }
+    double f = (temp - data[lo].first) / (data[hi].first - data[lo].first);
+    return data[lo].second + (data[hi].second - data[lo].second) * f;
+}
+
+double amplitude_interpolate(double t, const std::vector<double>& ts, const std::vector<double>& vs, double sx,
+                             double sy) {  // amplitude.rs:66-98
+    if (ts.empty()) return 0.0;
+    double tt = t - sx;
+    size_t idx = (size_t)(std::lower_bound(ts.begin(), ts.end(), tt) - ts.begin());
+    if (idx == 0) return vs.at(0) + sy;
+    if (idx >= ts.size()) return vs.at(vs.size() - 1) + sy;
+    double t0 = ts[idx - 1], t1 = ts[idx], v0 = vs.at(idx - 1), v1 = vs.at(idx);
+    return v0 + (v1 - v0) / (t1 - t0) * (tt - t0) + sy;
+}
+
+double Record::eval(const SolverTime& t, int64_t current_step) const {  // amplitude.rs:39-57
+    double y;
+    if (amp && amp->has_data) {
+        y = amplitude_interpolate(amp->total_time ? t.global : t.local, amp->t, amp->v, amp->shift_x, amp->shift_y);
+    } else if (current_step > origin_step) {
+        y = 1.0;
+    } else {
+        y = t.local / t.local_max;
+    }
+    return y * value;
+}
+
+// ------------------------------------------------------------------ preprocess
+
+std::string preprocess_inp(const std::string& text) {  // parser.rs:903-921
+    std::string out;
+    out.reserve(text.size());
+    size_t start = 0;
+    const size_t n = text.size();
+    while (start <= n) {
+        size_t nl = text.find('\n', start);
+        size_t end = nl == std::string::npos ? n : nl;
+        if (nl == std::string::npos && start == n) break;
+        size_t a = start, b = end;
+        while (a < b && is_ws(text[a])) ++a;
+        while (b > a && is_ws(text[b - 1])) --b;
+        if (a < b) {
+            bool comment = b - a >= 2 && text[a] == '*' && text[a + 1] == '*';
+            if (!comment) {
+                for (size_t k = a; k < b; ++k) out.push_back((char)std::toupper((unsigned char)text[k]));
+                out.push_back(text[b - 1] == ',' ? ' ' : '\n');
+            }
+        }
+        if (nl == std::string::npos) break;
+        start = nl + 1;
+    }
+    // substitute_ccx_solvers (parser.rs:930-942)
+    static const char* pats[] = {"ITERATIVE CHOLESKY", "ITERATIVE SCALING", "PASTIX", "PARDISO", "SPOOLES"};
+    static const char* reps[] = {"ITERATIVE", "ITERATIVE", "DIRECT", "DIRECT", "DIRECT"};
+    for (int k = 0; k < 5; ++k) {
+        std::string r;
+        r.reserve(out.size());
+        size_t pos = 0, plen = std::strlen(pats[k]);
+        while (true) {
+            size_t f = out.find(pats[k], pos);
+            if (f == std::string::npos) {
+                r.append(out, pos, std::string::npos);
+                break;
+            }
+            r.append(out, pos, f - pos);
+            r.append(reps[k]);
+            pos = f + plen;
+        }
+        out.swap(r);
+    }
+    return out;
+}
+
+// ------------------------------------------------------------------ parser
+
+namespace {
+
+const std::unordered_set<std::string>& keywords() {
+    static const std::unordered_set<std::string> k = {
+        "NODE", "ELEMENT", "NSET", "ELSET", "MATERIAL", "ELASTIC", "DENSITY", "SOLID_SECTION", "STEP", "STATIC",
+        "BOUNDARY", "CLOAD", "END_STEP", "HEADING", "NODE_FILE", "EL_FILE", "AMPLITUDE", "SURFACE", "DLOAD",
+        "DSLOAD", "NODE_PRINT", "EL_PRINT", "INCLUDE", "BEAM_SECTION", "EXPANSION", "SHELL_SECTION",
+        "CONDUCTIVITY", "SPECIFIC_HEAT", "INITIAL_CONDITIONS", "DEPVAR"};
+    return k;
+}
+
+struct Parser {
+    std::vector<std::string> lines;
+    size_t pos = 0;
+    Project p;
+    std::string kw;  // current keyword ("" = none)
+    int64_t line_nr = 0;
+    bool has_elem_type = false, has_elset = false, has_set = false, is_generate = false;
+    std::string elem_type, elset_name, set_name;
+    bool in_step = false;
+    StaticStep cur;
+    int64_t step_counter = 0;
+    std::vector<Record> step_loads, step_bcs;
+    bool has_ic = false;
+    std::string ic_type;
+
+    [[noreturn]] void perr(const std::string& msg) {
+        fail(FX_PARSE, "Parsing error at line " + std::to_string(line_nr) + ": " + msg);
+    }
+    const std::string* peek() const { return pos < lines.size() ? &lines[pos] : nullptr; }
+
+    void finish_step() {
+        cur.loads = step_loads;
+        cur.bcs = step_bcs;
+        p.steps.push_back(cur);
+        in_step = false;
+        cur = StaticStep();
+    }
+
+    std::vector<int64_t> targets(const std::string& t0) {
+        std::string t = trim(t0);
+        auto it = p.node_sets.find(t);
+        if (it != p.node_sets.end()) return it->second;
+        int64_t id;
+        if (parse_usize(t, &id)) return {id};
+        return {};
+    }
+
+    std::shared_ptr<const Amplitude> amp_for(const std::string* name) {
+        if (!name) return nullptr;
+        auto it = p.amplitudes.find(*name);
+        return it == p.amplitudes.end() ? nullptr : it->second;
+    }
+
+    int64_t origin() const { return in_step ? step_counter : 0; }
+
+    void run() {
+        while (pos < lines.size()) {
+            line_nr = (int64_t)pos + 1;
+            const std::string line = lines[pos++];
+            if (!line.empty() && line[0] == '*') {
+                keyword(line);
+                continue;
+            }
+            std::string t = trim(line);
+            if (t.empty()) continue;
+            if (!kw.empty()) data(t);
+        }
+        if (in_step) finish_step();
+        std::vector<int64_t> ids;
+        ids.reserve(p.nodes.size());
+        for (auto& kv : p.nodes) ids.push_back(kv.first);
+        std::sort(ids.begin(), ids.end());
+        p.index_to_node_id = ids;
+        p.node_id_to_index.reserve(ids.size());
+        for (size_t i = 0; i < ids.size(); ++i) p.node_id_to_index[ids[i]] = (int64_t)i;
+    }
+
+    void keyword(const std::string& line) {
+        auto parts = split(line, ',');
+        std::string k0 = trim(parts[0]);
+        std::string name = trim(k0.substr(1));
+        for (auto& c : name) c = (char)std::toupper((unsigned char)c);
+        std::string key = name;
+        std::replace(key.begin(), key.end(), ' ', '_');
+        if (!keywords().count(key))
+            fail(FX_UNSUPPORTED_KEYWORD, "Unsupported keyword at line " + std::to_string(line_nr) + ": " + name);
+        kw = key;
+        KwArgs ka = keyword_arguments(line);
+        if (key == "ELEMENT") {
+            const std::string* t = kw_value(ka, "TYPE");
+            has_elem_type = t != nullptr;
+            elem_type = t ? *t : "";
+            const std::string* es = kw_value(ka, "ELSET");
+            has_elset = es != nullptr;
+            elset_name = es ? *es : "";
+        } else if (key == "NSET" || key == "ELSET") {
+            const std::string* s = kw_value(ka, key.c_str());
+            has_set = s != nullptr;
+            set_name = s ? *s : "";
+            is_generate = ka.count("GENERATE") > 0;
+        } else if (key == "MATERIAL") {
+            const std::string* n = kw_value(ka, "NAME");
+            if (!n) perr("Material name not found");
+            Material m;
+            m.name = *n;
+            p.materials.push_back(m);
+        } else if (key == "EXPANSION") {
+            if (!p.materials.empty()) {
+                const std::string* z = kw_value(ka, "ZERO");
+                if (z) {
+                    double v;
+                    if (!parse_f64(*z, &v)) perr("Invalid ZERO value in *EXPANSION");
+                    p.materials.back().tref = v;
+                }
+            }
+        } else if (key == "INITIAL_CONDITIONS") {
+            const std::string* t = kw_value(ka, "TYPE");
+            has_ic = t != nullptr;
+            ic_type = t ? *t : "";
+            for (auto& c : ic_type) c = (char)std::toupper((unsigned char)c);
+        } else if (key == "SOLID_SECTION") {
+            const std::string* es = kw_value(ka, "ELSET");
+            if (!es) perr("Elset not found in *SOLID SECTION");
+            const std::string* mn = kw_value(ka, "MATERIAL");
+            if (!mn) perr("Material not found in *SOLID SECTION");
+            int midx = -1;
+            for (size_t i = 0; i < p.materials.size(); ++i)
+                if (p.materials[i].name == *mn) {
+                    midx = (int)i;
+                    break;
+                }
+            if (midx < 0) fail(FX_MATERIAL_NOT_FOUND, "Material " + *mn + " not found");
+            auto it = p.element_sets.find(*es);
+            if (it == p.element_sets.end()) fail(FX_ELSET_NOT_FOUND, "Elset " + *es + " not found");
+            for (int64_t eid : it->second) p.element_materials[eid] = midx;
+        } else if (key == "STEP") {
+            if (step_counter == 0) {
+                step_loads = p.initial_loads;
+                step_bcs = p.initial_bcs;
+            }
+            step_counter += 1;
+            if (in_step) finish_step();
+            bool nlgeom = ka.count("NLGEOM") > 0;
+            int64_t max_inc = 10000;
+            const std::string* inc = kw_value(ka, "INC");
+            if (inc) {
+                int64_t v;
+                if (parse_usize(*inc, &v)) max_inc = v;
+            }
+            const std::string* nxt = peek();
+            if (nxt && starts_with(*nxt, "*STATIC")) {
+                KwArgs ska = keyword_arguments(*nxt);
+                const std::string* sv = kw_value(ska, "SOLVER");
+                SolverType st = SolverType::Default;
+                if (sv) {
+                    if (*sv == "DIRECT") st = SolverType::Direct;
+                    else if (*sv == "ITERATIVE") st = SolverType::Iterative;
+                    else fail(FX_UNKNOWN_SOLVER, "Unknown solver type: " + *sv);
+                }
+                ++pos;  // consume *STATIC
+                IncrementData incd;
+                incd.max_increments = max_inc;
+                const std::string* dl = peek();
+                if (dl && !starts_with(*dl, "*")) {
+                    auto args = split(*dl, ',');
+                    for (auto& a : args) a = trim(a);
+                    if (args.size() >= 4) {
+                        if (!parse_f64(args[0], &incd.initial)) perr("Invalid initial time increment");
+                        if (!parse_f64(args[1], &incd.period)) perr("Invalid time period");
+                        if (!parse_f64(args[2], &incd.min_inc)) perr("Invalid min time increment");
+                        if (!parse_f64(args[3], &incd.max_inc)) perr("Invalid max time increment");
+                    }
+                    ++pos;  // consume the data line
+                }
+                cur = StaticStep();
+                cur.solver = st;
+                cur.inc = incd;
+                cur.nlgeom = nlgeom;
+                in_step = true;
+            }
+        } else if (key == "END_STEP") {
+            if (in_step) finish_step();
+        } else if (key == "AMPLITUDE") {
+            const std::string* n = kw_value(ka, "NAME");
+            if (!n) perr("Amplitude card is missing a Name= argument");
+            auto a = std::make_shared<Amplitude>();
+            const std::string* tt = kw_value(ka, "TIME");
+            a->total_time = tt && *tt == "TOTAL TIME";
+            double v;
+            const std::string* sx = kw_value(ka, "SHIFTX");
+            if (sx && parse_f64(*sx, &v)) a->shift_x = v;
+            const std::string* sy = kw_value(ka, "SHIFTY");
+            if (sy && parse_f64(*sy, &v)) a->shift_y = v;
+            const std::string* nxt = peek();
+            if (nxt) {
+                auto f = split(*nxt, ',');
+                for (size_t i = 0; i < f.size(); i += 2) {
+                    double x;
+                    if (parse_f64(trim(f[i]), &x)) a->t.push_back(x);
+                }
+                for (size_t i = 1; i < f.size(); i += 2) {
+                    double x;
+                    if (!parse_f64(trim(f[i]), &x)) perr("Invalid amplitude value");
+                    a->v.push_back(x);
+                }
+                a->has_data = true;
+                p.amplitudes[*n] = a;
+            }
+        } else if (key == "BOUNDARY") {
+            const std::string* an = kw_value(ka, "AMPLITUDE");
+            std::string amp_name = an ? *an : "";
+            const std::string* op = kw_value(ka, "OP");
+            if (op && *op == "NEW") {
+                if (in_step) step_bcs.clear();
+                else p.initial_bcs.clear();
+            }
+            const std::string* nxt = peek();
+            if (nxt && !starts_with(*nxt, "*")) boundary(*nxt, an ? &amp_name : nullptr);
+        } else if (key == "CLOAD") {
+            const std::string* an = kw_value(ka, "AMPLITUDE");
+            std::string amp_name = an ? *an : "";
+            const std::string* op = kw_value(ka, "OP");
+            if (op && *op == "NEW") {
+                if (in_step) step_loads.clear();
+                else p.initial_loads.clear();
+            }
+            while (const std::string* nxt = peek()) {
+                if (starts_with(*nxt, "*")) break;
+                std::string l = *nxt;
+                ++pos;
+                cload(l, an ? &amp_name : nullptr);
+            }
+        }
+    }
+
+    void cload(const std::string& line, const std::string* amp) {  // parser.rs:740-798
+        auto parts = split(line, ',');
+        for (auto& s : parts) s = trim(s);
+        if (parts.size() < 3) return;
+        int64_t dof;
+        if (!parse_usize(parts[1], &dof)) perr("Invalid DOF");
+        double val;
+        if (!parse_f64(parts[2], &val)) perr("Invalid load value");
+        auto nodes = targets(parts[0]);
+        if (dof >= 1 && dof <= 3) {
+            for (int64_t nid : nodes) {
+                Record r{nid, (int)(dof - 1), val, amp_for(amp), origin()};
+                (in_step ? step_loads : p.initial_loads).push_back(r);
+            }
+        }
+    }
+
+    void boundary(const std::string& line, const std::string* amp) {  // parser.rs:800-876
+        auto parts = split(line, ',');
+        for (auto& s : parts) s = trim(s);
+        if (parts.size() < 2) return;
+        int64_t first, last;
+        if (!parse_usize(parts[1], &first)) perr("Invalid first DOF");
+        if (parts.size() > 2 && !parts[2].empty()) {
+            if (!parse_usize(parts[2], &last)) perr("Invalid last DOF");
+        } else {
+            last = first;
+        }
+        double val = 0.0;
+        if (parts.size() > 3 && !parse_f64(parts[3], &val)) perr("Invalid boundary value");
+        for (int64_t nid : targets(parts[0]))
+            for (int64_t d = first; d <= last; ++d)
+                if (d >= 1 && d <= 3) {
+                    Record r{nid, (int)(d - 1), val, amp_for(amp), origin()};
+                    (in_step ? step_bcs : p.initial_bcs).push_back(r);
+                }
+    }
+
+    void data(const std::string& line) {
+        if (kw == "NODE") {
+            auto f = split(line, ',');
+            int64_t id;
+            std::array<double, 3> x;
+            if (f.size() != 4 || !parse_usize(trim(f[0]), &id) || !parse_f64(trim(f[1]), &x[0]) ||
+                !parse_f64(trim(f[2]), &x[1]) || !parse_f64(trim(f[3]), &x[2]))
+                perr("Invalid node definition: " + line);
+            p.nodes[id] = x;
+        } else if (kw == "ELEMENT") {
+            if (!has_elem_type) return;
+            auto f = split(line, ',');
+            std::vector<int64_t> nums;
+            nums.reserve(f.size());
+            for (auto& s : f) {
+                int64_t v;
+                if (!parse_usize(trim(s), &v)) fail(FX_PARSE, "Parsing error at line 0: Integer conversion failed");
+                nums.push_back(v);
+            }
+            int npe;
+            ElemType t;
+            if (elem_type == "C3D4") { npe = 4; t = ElemType::C3D4; }
+            else if (elem_type == "C3D20") { npe = 20; t = ElemType::C3D20; }
+            else fail(FX_PARSE, "Parsing error at line 0: Unknown element definition: " + elem_type);
+            if ((int)nums.size() - 1 != npe)
+                fail(FX_PARSE, "Parsing error at line 0: Wrong node count for " + elem_type);
+            int64_t eid = nums[0];
+            if (has_elset && !elset_name.empty()) p.element_sets[elset_name].push_back(eid);
+            ElementRec r;
+            r.type = t;
+            r.nodes.assign(nums.begin() + 1, nums.end());
+            p.elements[eid] = std::move(r);
+        } else if (kw == "NSET" || kw == "ELSET") {
+            if (!has_set || is_generate) return;
+            std::vector<int64_t> ids;
+            for (auto& s : split(line, ',')) {
+                std::string t = trim(s);
+                int64_t v;
+                if (!t.empty() && parse_usize(t, &v)) ids.push_back(v);
+            }
+            if (kw == "NSET") {
+                auto& dst = p.node_sets[set_name];
+                dst.insert(dst.end(), ids.begin(), ids.end());
+            } else if (line.find(',') == std::string::npos && ids.empty()) {
+                auto it = p.element_sets.find(trim(line));
+                if (it != p.element_sets.end()) {
+                    std::vector<int64_t> add = it->second;
+                    auto& dst = p.element_sets[set_name];
+                    dst.insert(dst.end(), add.begin(), add.end());
+                }
+            } else {
+                auto& dst = p.element_sets[set_name];
+                dst.insert(dst.end(), ids.begin(), ids.end());
+            }
+        } else if (kw == "ELASTIC" || kw == "DENSITY" || kw == "EXPANSION") {
+            if (p.materials.empty()) return;
+            std::vector<double> v;
+            for (auto& s : split(line, ',')) {
+                double x;
+                if (!parse_f64(trim(s), &x)) {
+                    if (kw == "ELASTIC") perr("Invalid elastic constant");
+                    if (kw == "DENSITY") perr("Invalid density value");
+                    perr("Invalid expansion constant");
+                }
+                v.push_back(x);
+            }
+            Material& m = p.materials.back();
+            if (kw == "ELASTIC") {
+                if (v.size() >= 2) {
+                    double t = v.size() >= 3 ? v[2] : 0.0;
+                    m.e.push(t, v[0]);
+                    m.has_e = true;
+                    m.nu.push(t, v[1]);
+                    m.has_nu = true;
+                }
+            } else if (!v.empty()) {
+                double t = v.size() >= 2 ? v[1] : 0.0;
+                if (kw == "DENSITY") { m.density.push(t, v[0]); m.has_density = true; }
+                else { m.alpha.push(t, v[0]); m.has_alpha = true; }
+            }
+        } else if (kw == "INITIAL_CONDITIONS") {
+            if (!has_ic || ic_type != "TEMPERATURE") return;
+            auto parts = split(line, ',');
+            for (auto& s : parts) s = trim(s);
+            if (parts.size() >= 2) {
+                double t;
+                if (!parse_f64(parts[1], &t)) perr("Invalid temperature value");
+                for (int64_t nid : targets(parts[0])) p.initial_temperatures[nid] = t;
+            }
+        } else if (kw == "DEPVAR") {
+            if (p.materials.empty()) return;
+            auto parts = split(line, ',');
+            int64_t n;
+            if (!parse_usize(trim(parts[0]), &n)) perr("Invalid DEPVAR value");
+            p.materials.back().depvars = n;
+        } else if (kw == "NODE_FILE" || kw == "EL_FILE") {
+            auto& dst = kw == "NODE_FILE" ? p.nodal_output : p.element_output;
+            for (auto& s : split(line, ',')) dst.push_back(trim(s));
+        }
+    }
+};
+
+}  // namespace
+
+Project parse_inp(const std::string& text) {
+    std::string pre = preprocess_inp(text);
+    Parser ps;
+    // str::lines semantics
+    size_t start = 0;
+    while (start < pre.size()) {
+        size_t nl = pre.find('\n', start);
+        size_t end = nl == std::string::npos ? pre.size() : nl;
+        std::string l = pre.substr(start, end - start);
+        if (!l.empty() && l.back() == '\r') l.pop_back();
+        ps.lines.push_back(std::move(l));
+        if (nl == std::string::npos) break;
+        start = nl + 1;
+    }
+    ps.run();
+    return std::move(ps.p);
+}
+
+DenseModel build_dense(const Project& p) {
+    DenseModel d;
+    d.n_nodes = (int64_t)p.index_to_node_id.size();
+    d.xyz.resize(3 * d.n_nodes);
+    for (int64_t i = 0; i < d.n_nodes; ++i) {
+        const auto& x = p.nodes.at(p.index_to_node_id[i]);
+        d.xyz[3 * i] = x[0];
+        d.xyz[3 * i + 1] = x[1];
+        d.xyz[3 * i + 2] = x[2];
+    }
+    std::vector<int64_t> ids;
+    ids.reserve(p.elements.size());
+    for (auto& kv : p.elements) ids.push_back(kv.first);
+    std::sort(ids.begin(), ids.end());
+    d.g4.npe = 4;
+    d.g20.npe = 20;
+    for (int64_t eid : ids) {
+        const ElementRec& r = p.elements.at(eid);
+        ElemGroup& g = r.type == ElemType::C3D4 ? d.g4 : d.g20;
+        g.elem_ids.push_back(eid);
+        for (int64_t nid : r.nodes) {
+            int64_t idx = p.index_of(nid);
+            if (idx < 0 && d.missing_node_id < 0) {
+                d.missing_node_id = nid;
+                d.missing_node_error = "Node " + std::to_string(nid) + " not found in mesh";
+            }
+            g.conn.push_back((int32_t)(idx < 0 ? 0 : idx));
+        }
+        auto it = p.element_materials.find(eid);
+        g.mat.push_back(it == p.element_materials.end() ? -1 : it->second);
+    }
+    MatTableHost& m = d.mats;
+    for (const Material& mat : p.materials) {
+        auto add = [&](bool has, const Lut& l, std::vector<int32_t>& off, std::vector<int32_t>& len) {
+            off.push_back((int32_t)m.t.size());
+            len.push_back(has ? (int32_t)l.data.size() : 0);
+            if (has)
+                for (auto& tv : l.data) {
+                    m.t.push_back(tv.first);
+                    m.v.push_back(tv.second);
+                }
+        };
+        add(mat.has_e, mat.e, m.e_off, m.e_len);
+        add(mat.has_nu, mat.nu, m.nu_off, m.nu_len);
+        add(mat.has_alpha, mat.alpha, m.a_off, m.a_len);
+        m.tref.push_back(mat.tref);
+        if (mat.has_alpha) d.any_expansion = true;
+    }
+    if (m.t.empty()) {
+        m.t.push_back(0.0);
+        m.v.push_back(0.0);
+    }
+    return d;
+}
+
+}  // namespace fx

@@ -1,0 +1,487 @@
+// Batched BSR3 PCG kernels and host loop (see pcg.hpp).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "pcg.hpp"
+
+namespace fx {
+
+constexpr int kChunkRows = 256;   // rows per CTA work item
+constexpr int kSpmvThreads = 512; // 64 rows in flight, 8 lanes per row
+constexpr int kUpdThreads = 256;  // one row per thread
+
+__device__ __forceinline__ void ld4(const float* p, int64_t i4, float o[4]) {
+    float4 v = __ldcs(reinterpret_cast<const float4*>(p) + i4);
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+}
+__device__ __forceinline__ void ld4(const double* p, int64_t i4, double o[4]) {
+    const double2* q = reinterpret_cast<const double2*>(p) + 2 * i4;
+    double2 a = __ldcs(q), b = __ldcs(q + 1);
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
+}
+
+// Fixed-order block reduction of NV doubles; result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(double v[NV], double* sh /* [NV][32] */) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if (l == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k * 32 + w] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = 0.0;
+            for (int j = 0; j < nw; ++j) t += sh[k * 32 + j];
+            v[k] = t;
+        }
+}
+
+// Publish this CTA's partials; returns true in every thread of the CTA that
+// completes the system (then `tot` holds the fixed-order totals in thread 0).
+template <int NV>
+__device__ __forceinline__ bool last_cta_reduce(double v[NV], double* part, int chunk_id, int chunk0, int nchunks,
+                                                int* counter, double* sh, double tot[NV]) {
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) part[(int64_t)chunk_id * 4 + k] = v[k];
+        __threadfence();
+        int t = atomicAdd(counter, 1);
+        s_last = (t == nchunks - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int c = threadIdx.x; c < nchunks; c += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(part + (int64_t)(chunk0 + c) * 4 + k);
+    __syncthreads();
+    block_sum<NV>(acc, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) tot[k] = acc[k];
+        *counter = 0;
+    }
+    return true;
+}
+
+// Status read once per CTA and broadcast, so every thread of a CTA takes the same path.
+__device__ __forceinline__ bool cta_running(const int* status) {
+    __shared__ int s_st;
+    if (threadIdx.x == 0) s_st = *(volatile const int*)status;
+    __syncthreads();
+    return s_st == kRun;
+}
+
+// (A) q = K p_new, p_new = z + beta p_old (fused), partial p_new . q
+template <typename T>
+__global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __restrict__ chunks,
+                                                           const InstDev<T>* __restrict__ insts, int parity) {
+    __shared__ double sh[4 * 32];
+    const ChunkDev ck = chunks[blockIdx.x];
+    const InstDev<T> I = insts[ck.inst];
+    if (!cta_running(I.status)) return;
+    const T beta = (T)I.scal[kBeta];
+    const T* __restrict__ pold = parity ? I.p1 : I.p0;
+    T* __restrict__ pnew = parity ? I.p0 : I.p1;
+    const T* __restrict__ z = I.z;
+    const int sub = threadIdx.x & 7, grp = threadIdx.x >> 3;
+    double dot = 0.0;
+    const int nrows = ck.row1 - ck.row0;
+    // The trip count is uniform across the CTA so that every lane reaches the
+    // full-warp shuffles below; lanes past the chunk end carry zeros.
+    for (int base = 0; base < nrows; base += kSpmvThreads / 8) {
+        const bool valid = base + grp < nrows;
+        const int row = ck.row0 + (valid ? base + grp : 0);
+        const int g0 = valid ? I.goff[row] : 0;
+        const int ng = valid ? I.goff[row + 1] - g0 : 0;
+        T a0 = 0, a1 = 0, a2 = 0;
+        for (int g = sub; g < ng; g += 8) {
+            int4 cc = __ldcs(reinterpret_cast<const int4*>(I.cols) + g0 + g);
+            T v[9][4];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) ld4(I.vals, (int64_t)g0 * 9 + (int64_t)e * ng + g, v[e]);
+            const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c3 = 3 * cj[j];
+                T q0 = z[c3] + beta * pold[c3];
+                T q1 = z[c3 + 1] + beta * pold[c3 + 1];
+                T q2 = z[c3 + 2] + beta * pold[c3 + 2];
+                a0 += v[0][j] * q0 + v[1][j] * q1 + v[2][j] * q2;
+                a1 += v[3][j] * q0 + v[4][j] * q1 + v[5][j] * q2;
+                a2 += v[6][j] * q0 + v[7][j] * q1 + v[8][j] * q2;
+            }
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (valid && sub == 0) {
+            const int r3 = 3 * row;
+            T p0 = z[r3] + beta * pold[r3];
+            T p1 = z[r3 + 1] + beta * pold[r3 + 1];
+            T p2 = z[r3 + 2] + beta * pold[r3 + 2];
+            I.q[r3] = a0;
+            I.q[r3 + 1] = a1;
+            I.q[r3 + 2] = a2;
+            pnew[r3] = p0;
+            pnew[r3 + 1] = p1;
+            pnew[r3 + 2] = p2;
+            dot += (double)p0 * (double)a0 + (double)p1 * (double)a1 + (double)p2 * (double)a2;
+        }
+    }
+    double v[1] = {dot}, tot[1];
+    block_sum<1>(v, sh);
+    __syncthreads();
+    if (last_cta_reduce<1>(v, I.part, ck.pad, I.chunk0, I.nchunks, I.counter, sh, tot) && threadIdx.x == 0) {
+        double pq = tot[0];
+        I.scal[kPq] = pq;
+        if (!(pq > 0.0) || !isfinite(pq)) {
+            *I.status = kBreak;
+            I.scal[kAlpha] = 0.0;
+        } else {
+            I.scal[kAlpha] = I.scal[kRz] / pq;
+        }
+    }
+}
+
+// (B) x += alpha p, r -= alpha q, z = M r, partial r.z and r.r
+template <typename T>
+__global__ void __launch_bounds__(kUpdThreads) k_pcg_update(const ChunkDev* __restrict__ chunks,
+                                                            const InstDev<T>* __restrict__ insts, int parity) {
+    __shared__ double sh[4 * 32];
+    const ChunkDev ck = chunks[blockIdx.x];
+    const InstDev<T> I = insts[ck.inst];
+    if (!cta_running(I.status)) return;
+    const double alpha = I.scal[kAlpha];
+    const T* __restrict__ p = parity ? I.p0 : I.p1;
+    double rz = 0.0, rr = 0.0;
+    for (int row = ck.row0 + threadIdx.x; row < ck.row1; row += blockDim.x) {
+        const int r3 = 3 * row;
+        T r[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            T pc = p[r3 + c];
+            I.x[r3 + c] += alpha * (double)pc;
+            r[c] = I.r[r3 + c] - (T)alpha * I.q[r3 + c];
+            I.r[r3 + c] = r[c];
+        }
+        const T* m = I.minv + 9 * (int64_t)row;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            T zc = m[3 * c] * r[0] + m[3 * c + 1] * r[1] + m[3 * c + 2] * r[2];
+            I.z[r3 + c] = zc;
+            rz += (double)r[c] * (double)zc;
+            rr += (double)r[c] * (double)r[c];
+        }
+    }
+    double v[2] = {rz, rr}, tot[2];
+    block_sum<2>(v, sh);
+    __syncthreads();
+    if (last_cta_reduce<2>(v, I.part, ck.pad, I.chunk0, I.nchunks, I.counter + 1, sh, tot) && threadIdx.x == 0) {
+        double rzn = tot[0];
+        double rzo = I.scal[kRz];
+        I.scal[kRzOld] = rzo;
+        I.scal[kRz] = rzn;
+        I.scal[kRr] = tot[1];
+        I.scal[kBeta] = rzo > 0.0 ? rzn / rzo : 0.0;
+        I.scal[kIters] += 1.0;
+        if (!isfinite(rzn) || rzn < 0.0) *I.status = kBreak;
+        else if (rzn <= I.scal[kThresh]) *I.status = kConv;
+    }
+}
+
+// Residual (re)placement: r = (T) r64, z = M r, r.z; FP64 r64 . M r64.
+// first != 0: start of a solve (beta = 0, ||b||_M^2 and the stop threshold recorded).
+template <typename T>
+__global__ void __launch_bounds__(kUpdThreads) k_pcg_replace(const ChunkDev* __restrict__ chunks,
+                                                             const InstDev<T>* __restrict__ insts, int first,
+                                                             double rtol2) {
+    __shared__ double sh[4 * 32];
+    const ChunkDev ck = chunks[blockIdx.x];
+    const InstDev<T> I = insts[ck.inst];
+    double rz = 0.0, rz64 = 0.0;
+    for (int row = ck.row0 + threadIdx.x; row < ck.row1; row += blockDim.x) {
+        const int r3 = 3 * row;
+        double r64[3];
+        T r[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            r64[c] = I.r64[r3 + c];
+            r[c] = (T)r64[c];
+            I.r[r3 + c] = r[c];
+        }
+        const T* m = I.minv + 9 * (int64_t)row;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            T zc = m[3 * c] * r[0] + m[3 * c + 1] * r[1] + m[3 * c + 2] * r[2];
+            I.z[r3 + c] = zc;
+            rz += (double)r[c] * (double)zc;
+            double z64 = (double)m[3 * c] * r64[0] + (double)m[3 * c + 1] * r64[1] + (double)m[3 * c + 2] * r64[2];
+            rz64 += r64[c] * z64;
+        }
+    }
+    double v[2] = {rz, rz64}, tot[2];
+    block_sum<2>(v, sh);
+    __syncthreads();
+    if (last_cta_reduce<2>(v, I.part, ck.pad, I.chunk0, I.nchunks, I.counter + 2, sh, tot) && threadIdx.x == 0) {
+        double rzn = tot[0];
+        I.scal[kRz64] = tot[1];
+        if (first) {
+            I.scal[kBnorm] = tot[1];
+            I.scal[kThresh] = rtol2 * tot[1];
+            I.scal[kBeta] = 0.0;
+            I.scal[kIters] = 0.0;
+        } else {
+            double rzo = I.scal[kRzOld];
+            I.scal[kBeta] = rzo > 0.0 ? rzn / rzo : 0.0;
+        }
+        I.scal[kRz] = rzn;
+        I.scal[kRzRef] = rzn;
+        *I.status = kRun;
+    }
+}
+
+// ------------------------------------------------------------------ host loop
+
+template <typename T>
+int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, cudaStream_t s,
+                       int64_t* launches) {
+    const int n = (int)sys.size();
+    if (n == 0) return FX_OK;
+    work_.resize(n);
+    std::vector<InstDev<T>> hi(n);
+    std::vector<ChunkDev> all_chunks;
+    d_scal_.alloc((size_t)n * kNScal, s);
+    d_scal_.zero(s);
+    d_status_.alloc(n, s);
+    d_status_.zero(s);
+    d_counter_.alloc((size_t)n * 4, s);
+    d_counter_.zero(s);
+    std::vector<int> chunk0(n), nch(n);
+    for (int i = 0; i < n; ++i) {
+        const int rows = sys[i]->S->n_rows;
+        chunk0[i] = (int)all_chunks.size();
+        for (int r0 = 0; r0 < rows; r0 += kChunkRows)
+            all_chunks.push_back(ChunkDev{i, r0, std::min(rows, r0 + kChunkRows), (int)all_chunks.size()});
+        nch[i] = (int)all_chunks.size() - chunk0[i];
+    }
+    d_part_.alloc(all_chunks.size() * 4 + 4, s);
+    for (int i = 0; i < n; ++i) {
+        PcgSystem<T>& S = *sys[i];
+        Work& w = work_[i];
+        const size_t m = 3 * (size_t)S.S->n_rows;
+        w.r.alloc(m, s);
+        w.z.alloc(m, s);
+        w.p0.alloc(m, s);
+        w.p1.alloc(m, s);
+        w.q.alloc(m, s);
+        w.r64.alloc(m, s);
+        w.p0.zero(s);
+        w.p1.zero(s);
+        if (S.warm_start) {
+            S.residual64(S.x, S.b, w.r64.ptr, s);
+        } else {
+            FX_CUDA_CHECK(cudaMemsetAsync(S.x, 0, m * sizeof(double), s));
+            FX_CUDA_CHECK(cudaMemcpyAsync(w.r64.ptr, S.b, m * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        }
+        InstDev<T>& d = hi[i];
+        d.n_rows = S.S->n_rows;
+        d.chunk0 = chunk0[i];
+        d.nchunks = nch[i];
+        d.goff = S.S->goff.ptr;
+        d.cols = S.S->cols.ptr;
+        d.vals = S.vals;
+        d.minv = S.minv;
+        d.r = w.r.ptr;
+        d.z = w.z.ptr;
+        d.p0 = w.p0.ptr;
+        d.p1 = w.p1.ptr;
+        d.q = w.q.ptr;
+        d.x = S.x;
+        d.r64 = w.r64.ptr;
+        d.scal = d_scal_.ptr + (size_t)i * kNScal;
+        d.status = d_status_.ptr + i;
+        d.counter = d_counter_.ptr + 4 * i;
+        d.part = d_part_.ptr;
+        S.status = FX_OK;
+        S.iterations = 0;
+        S.replacements = 0;
+    }
+    d_inst_.upload(hi, s);
+    d_chunks_.upload(all_chunks, s);
+    const double rtol2 = opt.rtol * opt.rtol;
+    const bool trace = std::getenv("FX_DEBUG") != nullptr;
+    FX_LAUNCH(k_pcg_replace<T>, (unsigned)all_chunks.size(), kUpdThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, 1,
+              rtol2);
+    if (launches) ++*launches;
+
+    std::vector<double> h_scal((size_t)n * kNScal);
+    std::vector<int> h_status(n);
+    auto pull = [&]() {
+        FX_CUDA_CHECK(cudaMemcpyAsync(h_scal.data(), d_scal_.ptr, h_scal.size() * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s));
+        FX_CUDA_CHECK(cudaMemcpyAsync(h_status.data(), d_status_.ptr, n * sizeof(int), cudaMemcpyDeviceToHost, s));
+        stream_wait(s, "pcg poll");
+    };
+    pull();
+    std::vector<char> done(n, 0);
+    std::vector<double> best(n, 1e300);
+    std::vector<int> stall(n, 0);
+    for (int i = 0; i < n; ++i) {
+        if (!(h_scal[i * kNScal + kBnorm] > 0.0)) {  // b = 0: x = 0 is exact
+            done[i] = 1;
+            sys[i]->relres = 0.0;
+        }
+    }
+    const int poll = std::max(2, opt.poll & ~1);
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<ChunkDev> act;
+    DBuf<ChunkDev> d_act;
+    bool rebuild = true;
+    int result = FX_OK;
+    auto set_status = [&](int i, int st) {
+        FX_CUDA_CHECK(cudaMemcpyAsync(d_status_.ptr + i, &st, sizeof(int), cudaMemcpyHostToDevice, s));
+    };
+    for (int i = 0; i < n; ++i)
+        if (done[i]) set_status(i, kIdle);
+    while (true) {
+        if (rebuild) {
+            act.clear();
+            for (auto& c : all_chunks)
+                if (!done[c.inst]) act.push_back(c);
+            if (act.empty()) break;
+            d_act.upload(act, s);
+            if (gexec) {
+                cudaGraphExecDestroy(gexec);
+                gexec = nullptr;
+            }
+            if (opt.graphs && !debug_sync()) {
+                cudaGraph_t g;
+                int64_t* saved = g_launch_counter;
+                g_launch_counter = nullptr;
+                FX_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                for (int k = 0; k < poll; ++k) {
+                    FX_LAUNCH(k_pcg_spmv<T>, (unsigned)act.size(), kSpmvThreads, 0, s, d_act.ptr, d_inst_.ptr, k & 1);
+                    FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr,
+                              k & 1);
+                }
+                FX_CUDA_CHECK(cudaStreamEndCapture(s, &g));
+                g_launch_counter = saved;
+                FX_CUDA_CHECK(cudaGraphInstantiate(&gexec, g, 0));
+                cudaGraphDestroy(g);
+            }
+            rebuild = false;
+        }
+        if (gexec) {
+            FX_CUDA_CHECK(cudaGraphLaunch(gexec, s));
+        } else {
+            int64_t* saved = g_launch_counter;
+            g_launch_counter = nullptr;
+            for (int k = 0; k < poll; ++k) {
+                FX_LAUNCH(k_pcg_spmv<T>, (unsigned)act.size(), kSpmvThreads, 0, s, d_act.ptr, d_inst_.ptr, k & 1);
+                FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr, k & 1);
+            }
+            g_launch_counter = saved;
+        }
+        if (launches) *launches += 2 * (int64_t)poll;
+        pull();
+        if (trace)
+            for (int i = 0; i < n; ++i)
+                std::fprintf(stderr, "[pcg] sys %d status %d iters %.0f rz %.3e rzref %.3e thresh %.3e pq %.3e\n", i,
+                             h_status[i], h_scal[i * kNScal + kIters], h_scal[i * kNScal + kRz],
+                             h_scal[i * kNScal + kRzRef], h_scal[i * kNScal + kThresh], h_scal[i * kNScal + kPq]);
+        // decide per system
+        std::vector<int> replace;
+        for (int i = 0; i < n; ++i) {
+            if (done[i]) continue;
+            const double* sc = &h_scal[(size_t)i * kNScal];
+            const int st = h_status[i];
+            sys[i]->iterations = (long long)sc[kIters];
+            if (st == kBreak) {
+                // r.z == 0 exactly means an exact solution; anything else is a breakdown
+                done[i] = 1;
+                sys[i]->status = FX_NUMERICAL;
+                if (result == FX_OK) result = FX_NUMERICAL;
+                rebuild = true;
+                continue;
+            }
+            bool reached = st == kConv;
+            bool drop = sizeof(T) == 4 && sc[kRzRef] > 0.0 && sc[kRz] < opt.reliable_delta * opt.reliable_delta * sc[kRzRef];
+            if (reached || drop) replace.push_back(i);
+            else if (sc[kIters] >= opt.max_iter) {
+                done[i] = 1;
+                sys[i]->status = FX_CONVERGENCE;
+                if (result == FX_OK) result = FX_CONVERGENCE;
+                rebuild = true;
+            }
+        }
+        if (!replace.empty()) {
+            std::vector<ChunkDev> rc;
+            for (int i : replace) {
+                PcgSystem<T>& S = *sys[i];
+                S.residual64(S.x, S.b, work_[i].r64.ptr, s);
+                for (int c = 0; c < nch[i]; ++c) rc.push_back(all_chunks[chunk0[i] + c]);
+                S.replacements++;
+            }
+            DBuf<ChunkDev> d_rc;
+            d_rc.upload(rc, s);
+            FX_LAUNCH(k_pcg_replace<T>, (unsigned)rc.size(), kUpdThreads, 0, s, d_rc.ptr, d_inst_.ptr, 0, rtol2);
+            pull();
+            for (int i : replace) {
+                const double* sc = &h_scal[(size_t)i * kNScal];
+                double rel = std::sqrt(std::max(0.0, sc[kRz64]) / sc[kBnorm]);
+                if (trace) std::fprintf(stderr, "[pcg] replace sys %d relres %.3e\n", i, rel);
+                sys[i]->relres = rel;
+                if (rel < 0.5 * best[i]) {
+                    best[i] = rel;
+                    stall[i] = 0;
+                } else {
+                    ++stall[i];
+                }
+                if (rel <= opt.rtol) {
+                    done[i] = 1;
+                    set_status(i, kIdle);
+                    rebuild = true;
+                } else if (sizeof(T) == 4 && stall[i] >= opt.stall_limit) {
+                    done[i] = 1;
+                    set_status(i, kIdle);
+                    sys[i]->status = FX_CONVERGENCE;
+                    sys[i]->stagnated = true;
+                    rebuild = true;
+                } else if (sc[kIters] >= opt.max_iter) {
+                    done[i] = 1;
+                    set_status(i, kIdle);
+                    sys[i]->status = FX_CONVERGENCE;
+                    if (result == FX_OK) result = FX_CONVERGENCE;
+                    rebuild = true;
+                }
+            }
+        }
+    }
+    if (gexec) cudaGraphExecDestroy(gexec);
+    stream_wait(s, "stream");
+    return result;
+}
+
+template class PcgBatch<float>;
+template class PcgBatch<double>;
+
+}  // namespace fx

@@ -1,0 +1,108 @@
+// Batched preconditioned conjugate gradient over BSR(3x3) systems.
+//
+// Stands in for the reference's DirectSolver (src/solver/solvers/direct.rs:19-55,
+// an FP64 sparse Cholesky) and IterativeSolver (src/solver/solvers/iterative.rs:82-177,
+// a Jacobi-PCG): both solve K du = R; this solver returns du to a stated
+// tolerance on the FP64 true residual.
+//
+// Mixed precision (T = float): the SpMV, the 3x3 block-Jacobi and the vector
+// recurrences run in FP32 while the solution is accumulated in FP64 and the
+// residual is periodically replaced by the FP64 true residual b - A x
+// (residual replacement / "reliable updates", van der Vorst & Ye 2000),
+// computed by a caller-supplied FP64 operator. This is the FP64
+// iterative-refinement loop around the FP32 Krylov iteration, without
+// discarding the search direction at each refinement.
+// FP64 (T = double): the same kernels on FP64 data; the true residual is
+// checked once at the end.
+//
+// Per iteration two kernels run per batch: (A) q = K p with the direction
+// update p = z + beta p fused into the gather and the p.q partial sum, (B)
+// x += alpha p, r -= alpha q, z = M r and the r.z partial sum. Scalars are
+// reduced by the last CTA of each system in a fixed order (deterministic).
+// A block of `poll_interval` iterations is captured in a CUDA graph and
+// replayed between host checks.
+#pragma once
+
+#include <functional>
+#include <vector>
+
+#include "kernels.hpp"
+
+namespace fx {
+
+enum PcgStatus : int { kRun = 0, kConv = 1, kBreak = 2, kIdle = 3 };
+
+// scalars per system
+enum PcgScal : int {
+    kRz = 0, kPq = 1, kAlpha = 2, kBeta = 3, kRzOld = 4, kRr = 5, kRzRef = 6, kIters = 7, kThresh = 8,
+    kRz64 = 9, kBnorm = 10, kNScal = 16
+};
+
+template <typename T>
+struct InstDev {
+    int n_rows;
+    int chunk0, nchunks;
+    const int32_t* goff;
+    const int32_t* cols;
+    const T* vals;
+    const T* minv;
+    T *r, *z, *p0, *p1, *q;
+    double* x;
+    const double* r64;
+    double* scal;
+    int* status;
+    int* counter;
+    double* part;
+};
+
+struct ChunkDev {
+    int inst, row0, row1, pad;
+};
+
+// One linear system of a batch.
+template <typename T>
+struct PcgSystem {
+    const BsrStructure* S = nullptr;
+    const T* vals = nullptr;
+    const T* minv = nullptr;
+    const double* b = nullptr;  // FP64 right-hand side (device)
+    double* x = nullptr;        // FP64 solution (device), overwritten
+    // r64 = b - A x in FP64 (device pointers); the FP64 operator of this system
+    std::function<void(const double* x, const double* b, double* r64, cudaStream_t)> residual64;
+    bool warm_start = false;    // start from the given x (r0 = b - A x by residual64) instead of x = 0
+    // outputs
+    int status = 0;
+    bool stagnated = false;     // mixed: FP64 residual stopped improving across replacements
+    long long iterations = 0;
+    int replacements = 0;
+    double relres = 0.0;  // final ||b - A x||_M / ||b||_M
+};
+
+struct PcgOptions {
+    double rtol = 1e-10;
+    int max_iter = 20000;
+    int poll = 32;
+    double reliable_delta = 1e-2;
+    bool graphs = true;
+    int stall_limit = 4;  // replacements without halving the best FP64 residual before giving up (mixed)
+};
+
+template <typename T>
+class PcgBatch {
+   public:
+    // Solves all systems; returns FX_OK or the first failing status (per-system status in sys[i].status).
+    int solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, cudaStream_t s, int64_t* launches);
+
+   private:
+    struct Work {
+        DBuf<T> r, z, p0, p1, q;
+        DBuf<double> r64;
+    };
+    std::vector<Work> work_;
+    DBuf<InstDev<T>> d_inst_;
+    DBuf<ChunkDev> d_chunks_;
+    DBuf<double> d_scal_, d_part_;
+    DBuf<int> d_status_, d_counter_;
+};
+
+}  // namespace fx

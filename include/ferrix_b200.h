@@ -1,0 +1,174 @@
+/*
+ * ferrix_b200 — C ABI of the B200 (sm_100a) solver for FerriX's linear-static
+ * and NLGEOM *STATIC path (C3D4 / C3D20 solids).
+ *
+ * Plain C types only: opaque handles, host pointers and sizes. The caller owns
+ * every host buffer; the library owns all device memory behind the handles.
+ * One context = one GPU + one CUDA stream; a context and its models must be
+ * used from one thread at a time.
+ *
+ * Reference seams each entry point replaces (paths relative to the FerriX
+ * crate root):
+ *   fx_model_from_inp            Project::from_jobname / Parser::parse
+ *                                (src/solver/project.rs:93-127, src/solver/parser.rs:111-147)
+ *   fx_state_initialize          SolutionState::new + initialize (src/solver/state.rs:32-79)
+ *                                and SolverTime::new (src/solver/time.rs:27-33)
+ *   fx_step_solve                Step::solve -> StaticStep::solve
+ *                                (src/solver/step/steps.rs:28-42, src/solver/step/static_step.rs:47-267)
+ *   fx_assemble_csr              Assembler::assemble + TriMat::to_csr
+ *                                (src/solver/assembler.rs:37-151, src/solver/step/static_step.rs:198)
+ *   fx_internal_force            Assembler::assemble_internal_force (src/solver/assembler.rs:157-241)
+ *   fx_thermal_force             Assembler::assemble_thermal_force (src/solver/assembler.rs:247-299)
+ *   fx_solve_csr                 Solver::solve (src/solver/solvers/mod.rs:18-43), the seam behind
+ *                                DirectSolver (direct.rs:19-55) and IterativeSolver (iterative.rs:82-177)
+ *   fx_batch_solve               no reference counterpart (one deck per process there): many
+ *                                independent decks' first *STATIC step in one batched launch sequence
+ *   fx_server_*                  no reference counterpart: continuous-batching request loop
+ */
+#ifndef FERRIX_B200_H
+#define FERRIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: the FerrixError variants (src/solver/error.rs:12-72) plus
+ * device-side conditions. 0 is success. */
+typedef enum {
+    FX_OK = 0,
+    FX_IO = 1,
+    FX_GENERIC_IO = 2,
+    FX_PARSE = 3,
+    FX_UNSUPPORTED_KEYWORD = 4,
+    FX_UNKNOWN_SOLVER = 5,
+    FX_NODE_NOT_FOUND = 6,
+    FX_ELEMENT_NOT_FOUND = 7,
+    FX_MATERIAL_NOT_FOUND = 8,
+    FX_ELSET_NOT_FOUND = 9,
+    FX_NSET_NOT_FOUND = 10,
+    FX_NUMERICAL = 11,        /* singular Jacobian, PCG breakdown, indefinite system */
+    FX_CONVERGENCE = 12,      /* increment / Newton / PCG iteration limits */
+    FX_INVALID_MODEL = 13,
+    FX_GENERIC = 14,
+    FX_CANCELLED = 15,
+    FX_TIMEOUT = 16,
+    FX_CUDA = 17,
+    FX_INVALID_ARGUMENT = 18
+} fx_status;
+
+typedef struct fx_ctx fx_ctx;
+typedef struct fx_model fx_model;
+typedef struct fx_server fx_server;
+
+/* Arithmetic of the PCG that stands in for the reference's FP64 Cholesky. */
+typedef enum {
+    FX_PREC_MIXED = 0, /* FP32 BSR3 SpMV + 3x3 block-Jacobi, FP64 residual replacement and accumulation */
+    FX_PREC_FP64 = 1,  /* FP64 BSR3 SpMV + 3x3 block-Jacobi throughout */
+    FX_PREC_FP64_CSR = 2 /* plain FP64 PCG: scalar CSR SpMV + Jacobi (the reference IterativeSolver's algorithm) */
+} fx_precision;
+
+typedef struct {
+    int precision;          /* fx_precision */
+    double rtol;            /* stop when ||b - A x||_M / ||b||_M <= rtol (FP64 true residual, M = block-Jacobi) */
+    int max_iter;           /* PCG iteration cap per linear solve (FX_CONVERGENCE beyond) */
+    int poll_interval;      /* PCG iterations per CUDA-graph replay between host checks (even) */
+    double reliable_delta;  /* mixed: FP64 residual replacement once the residual fell by this factor */
+    int use_graphs;         /* capture the PCG iteration block in a CUDA graph */
+    int verbose;            /* print the reference's per-iteration |R| lines to stdout */
+    int reference_iterative; /* SOLVER=ITERATIVE steps: reference semantics (Jacobi PCG, absolute
+                                sqrt(r.z) < 1e-8, at most 1000 iterations; iterative.rs:82-177) */
+} fx_solve_opts;
+
+typedef struct {
+    int increments;            /* increments attempted (converged or cut back) */
+    int newton_iterations;
+    int linear_solves;
+    long long pcg_iterations;
+    int reliable_updates;
+    double last_rel_residual;  /* |R|/|F_ext| of the last converged Newton iteration */
+    double last_linear_relres; /* ||b - A x||_M / ||b||_M of the last linear solve */
+    double t_symbolic_ms, t_assembly_ms, t_forces_ms, t_pcg_ms, t_total_ms;  /* device event times */
+    int64_t bsr_blocks;        /* 3x3 blocks of the assembled stiffness */
+    int fp64_fallbacks;        /* mixed solves that stalled and were finished in FP64 */
+} fx_step_stats;
+
+void fx_default_solve_opts(fx_solve_opts* opts);
+
+/* ---- context ---------------------------------------------------------- */
+int fx_ctx_create(int device, fx_ctx** out);
+void fx_ctx_destroy(fx_ctx* ctx);
+const char* fx_ctx_last_error(const fx_ctx* ctx);
+/* Number of kernel launches issued by this context so far (all entry points). */
+int64_t fx_ctx_kernel_launches(const fx_ctx* ctx);
+
+/* ---- model (Project) -------------------------------------------------- */
+/* Preprocess + parse `.inp` text with the reference parser's semantics.
+ * ctx may be NULL: the model can then be inspected but not solved. */
+int fx_model_from_inp(fx_ctx* ctx, const char* text, size_t len, fx_model** out);
+void fx_model_destroy(fx_model* model);
+/* Counts: nodes, elements (all types), steps, materials. */
+int fx_model_sizes(const fx_model* model, int64_t* n_nodes, int64_t* n_elements, int* n_steps, int* n_materials);
+/* Mesh::index_to_node_id: ids[i] = node id of matrix index i (ascending ids). */
+int fx_model_node_ids(const fx_model* model, int64_t* ids);
+/* Mesh::get_index_for_node_id: -1 when absent. */
+int64_t fx_model_node_index(const fx_model* model, int64_t node_id);
+/* Project.default_initial_temperature (applied by fx_state_initialize). */
+int fx_model_set_default_temperature(fx_model* model, double temperature);
+/* Step description: nlgeom flag, solver (0 default, 1 direct, 2 iterative),
+ * increment data (initial, period, min, max), counts of loads and BCs. */
+int fx_model_step_info(const fx_model* model, int step_index, int* nlgeom, int* solver, double incr[4],
+                       int64_t* n_loads, int64_t* n_bcs);
+
+/* Dense model arrays (node index = rank of node id; elements of each type in
+ * ascending id order): xyz[3N], conn[n*npe] node indices, mat[n] material
+ * index (-1 = none). Pass NULL for arrays not wanted; counts always written. */
+int fx_model_export(fx_model* model, double* xyz, int64_t* n4, int32_t* conn4, int32_t* mat4, int64_t* n20,
+                    int32_t* conn20, int32_t* mat20);
+/* Loads (is_bc = 0) or BCs (is_bc = 1) of a step in record order: node id,
+ * dof (0..2), value, origin step, amplitude flag (1 = tabular amplitude). */
+int fx_model_step_records(const fx_model* model, int step_index, int is_bc, int64_t* node_ids, int32_t* dofs,
+                          double* values, int64_t* origin, int32_t* tabular);
+
+/* ---- solution state (SolutionState + SolverTime) --------------------- */
+int fx_state_initialize(fx_model* model);
+int fx_state_get_displacements(const fx_model* model, double* u /* 3N */);
+int fx_state_set_displacements(fx_model* model, const double* u /* 3N */);
+int fx_state_get_temperatures(const fx_model* model, double* t_init /* N */, double* t_cur /* N */);
+/* SolutionState.initial_temperatures / .temperatures are public fields in the
+ * reference (src/solver/state.rs:20-24); NULL leaves a vector unchanged. */
+int fx_state_set_temperatures(fx_model* model, const double* t_init /* N */, const double* t_cur /* N */);
+
+/* ---- the static step -------------------------------------------------- */
+/* Step::solve for project.steps[step_index] with step_id = step_index + 1.
+ * stats may be NULL; opts NULL = fx_default_solve_opts. */
+int fx_step_solve(fx_model* model, int step_index, const fx_solve_opts* opts, fx_step_stats* stats);
+
+/* ---- lower-level seams (parity tests, Rust shims) -------------------- */
+/* Stiffness on X (+u when u != NULL) with the current temperatures, as the
+ * expanded CSR of the 3x3 block structure (explicit zeros kept), FP64 values
+ * of the `precision` assembly. Call with indptr/indices/data NULL to get *nnz. */
+int fx_assemble_csr(fx_model* model, const double* u_or_null, int precision, int64_t* nnz, int64_t* indptr,
+                    int64_t* indices, double* data, double* maxdiag);
+/* f_int(u) on X (+uconf when != NULL), current temperatures; f is 3N. */
+int fx_internal_force(fx_model* model, const double* u, const double* uconf_or_null, double* f);
+int fx_thermal_force(fx_model* model, double* f);
+/* Solver::solve seam: solve K x = b for a host CSR matrix (square, symmetric
+ * positive definite, n rows) with the GPU PCG; tol / max_iter as the caller's
+ * Solver::solve arguments are mapped by `opts`. */
+int fx_solve_csr(fx_ctx* ctx, int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
+                 const double* b, double* x, const fx_solve_opts* opts, fx_step_stats* stats);
+
+/* ---- batched decks ---------------------------------------------------- */
+/* Runs the first step of every model (each fx_state_initialize'd) with all
+ * linear solves of the batch advanced together; per-model status in status[]. */
+int fx_batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts* opts, int* status,
+                   fx_step_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FERRIX_B200_H */

@@ -1,0 +1,153 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol the
+header declares, and its `.inp` parser builds the same model as the oracle's
+restatement of src/solver/parser.rs (no compute call is made)."""
+import gzip
+import os
+
+import numpy as np
+import pytest
+
+from ferrix_b200 import _lib, decks
+import ferrix_b200 as fx
+from oracle import inp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "ferrix_b200.h")
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    declared = _lib.header_symbols(HEADER)
+    assert len(declared) >= 20
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(declared) == set(_lib.SIGNATURES), set(declared) ^ set(_lib.SIGNATURES)
+
+
+def _compare(text):
+    o = inp.parse_inp_text(text)
+    m = inp.model_arrays(o) if o.nodes else None
+    p = fx.Project.from_inp_text(text)
+    assert p.num_nodes == len(o.nodes)
+    assert p.num_elements == len(o.elements)
+    assert len(p.steps) == len(o.steps)
+    assert p.num_materials == len(o.materials)
+    if m is not None:
+        assert np.array_equal(p.mesh.index_to_node_id, m.node_ids)
+        xyz, groups = p.export()
+        assert np.array_equal(xyz, m.xyz)
+        for npe in (4, 20):
+            conn, mat = groups[npe]
+            if npe in m.groups:
+                assert np.array_equal(conn, m.groups[npe][1]) and np.array_equal(mat, m.groups[npe][2])
+            else:
+                assert conn.size == 0
+    for k, (ps, os_) in enumerate(zip(p.steps, o.steps)):
+        assert ps.info.nlgeom == os_.nlgeom and ps.info.solver == os_.solver
+        inc = os_.increment
+        assert ps.info.increment == (inc.initial_time_increment, inc.time_period, inc.min_time_increment,
+                                     inc.max_time_increment)
+        for is_bc, recs in ((False, os_.loads), (True, os_.bcs)):
+            ids, dofs, vals, org, tab = ps.records(is_bc)
+            assert len(ids) == len(recs)
+            for i, r in enumerate(recs):
+                assert (ids[i], dofs[i], vals[i], org[i], bool(tab[i])) == \
+                    (r.node_id, r.dof, r.value, r.origin_step, r.amplitude.times is not None)
+    return p, o
+
+
+@pytest.mark.parametrize("name", ["C3D4_staticstep", "C3D4_2staticstep", "C3D20", "NLGEOM_test"])
+def test_parser_matches_oracle_on_reference_decks(golden_dir, name):
+    with gzip.open(os.path.join(golden_dir, "decks", name + ".inp.gz"), "rt") as fh:
+        _compare(fh.read())
+
+
+def test_parser_matches_oracle_on_synthetic_decks():
+    _compare(decks.c3d4_cantilever(2, 2, 4))
+    _compare(decks.c3d20_box(2, 2, 3))
+    _compare(decks.c3d4_nlgeom_beam(4, 2, 2))
+
+
+QUIRKS = """** comment
+*Heading
+title line
+*Node
+1, 0, 0, 0
+2, 1.0, 0, 0
+3, 0, 1.0, 0
+4, 0, 0, 1.0
+5, 1E0, 1e0, +1.0
+*Element, type=C3D4, elset=E1
+1, 1, 2, 3, 4
+2, 2, 3, 4,
+5
+*Nset, nset=ALL
+1, 2, 3,
+4, 5
+*Elset, elset=E2
+E1
+*Material, name=Steel
+*Elastic
+210000, 0.3, 20
+190000, 0.3, 300
+*Expansion, zero=20
+1.2e-5
+*Solid section, elset=E2, material=STEEL
+*Amplitude, name=A1, shiftx=0.5
+0, 0, 1, 2
+*Initial conditions, type=temperature
+ALL, 50
+3, 70
+*Boundary
+1, 1, 3
+2, 4, 6
+*Step, nlgeom, inc=50
+*Static, solver=pardiso
+0.25, 1.0, 1e-4, 0.5
+*Boundary, op=new
+1, 1, 3, 0.0
+2, 2
+*Cload, amplitude=A1
+ALL, 2, 10.0
+5, 3, -1.5
+*Node print, nset=ALL
+U
+*Cload
+4, 1, 99.0
+*End step
+*Step
+*Static, Solver=Iterative Scaling
+*Cload, op=NEW
+3, 3, 2.5
+*Dload
+*End step
+"""
+
+
+def test_parser_quirks_match_oracle():
+    p, o = _compare(QUIRKS)
+    assert p.steps[0].info.nlgeom and p.steps[0].info.solver == "DIRECT"
+    assert p.steps[1].info.solver == "ITERATIVE"
+    assert o.initial_temperatures[3] == 70.0
+
+
+@pytest.mark.parametrize("text,kind", [
+    ("*ORIENTATION, NAME=X\n", "UnsupportedKeyword"),
+    ("*STEP\n*STATIC, SOLVER=MAGIC\n", "UnknownSolver"),
+    ("*NODE\n1, 0, 0\n", "ParseError"),
+    ("*MATERIAL\n", "ParseError"),
+    ("*SOLID SECTION, MATERIAL=M\n", "ParseError"),
+    ("*SOLID SECTION, ELSET=A, MATERIAL=M\n", "MaterialNotFound"),
+    ("*MATERIAL, NAME=M\n*SOLID SECTION, ELSET=A, MATERIAL=M\n", "ElsetNotFound"),
+    ("*MATERIAL, NAME=M\n*SOLID SECTION, ELSET=A, MATERIAL=Q\n", "MaterialNotFound"),
+    ("*ELEMENT, TYPE=C3D8\n1, 1, 2, 3, 4, 5, 6, 7, 8\n", "ParseError"),
+    ("*ELEMENT, TYPE=C3D4\n1, 1, 2, 3\n", "ParseError"),
+    ("*AMPLITUDE\n0, 1\n", "ParseError"),
+])
+def test_parser_errors(text, kind):
+    with pytest.raises(inp.FerrixError) as eo:
+        inp.parse_inp_text(text)
+    assert eo.value.kind == kind
+    with pytest.raises(fx.FerrixError) as eg:
+        fx.Project.from_inp_text(text)
+    assert eg.value.kind == kind

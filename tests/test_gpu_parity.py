@@ -1,0 +1,260 @@
+"""GPU parity: every result of libferrix_b200.so (through the C ABI) against the
+oracle's FP64 restatement of the FerriX path on the same inputs.
+
+Tolerances (relative, stated per check):
+  * FP64 stiffness entries / maxdiag: 1e-12 of the largest entry
+  * FP32 stiffness entries: 2e-6 of the largest entry (FP32 element kernels)
+  * FP64 internal / thermal force: 1e-11 of the largest entry
+  * displacement after a linear step, both precisions: 1e-8 in the 2-norm
+  * NLGEOM displacement: 1e-6 in the 2-norm (each Newton iterate carries the
+    1e-8-accurate linear solve forward through 4 iterations)
+"""
+import ctypes as C
+import gzip
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import ferrix_b200 as fx
+from ferrix_b200 import decks
+from oracle import elem, inp, static_step
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = fx.Context(0)
+    yield c
+    c.close()
+
+
+def _deck(golden_dir, name):
+    with gzip.open(os.path.join(golden_dir, "decks", name + ".inp.gz"), "rt") as fh:
+        return fh.read()
+
+
+def _project(ctx, text, t_default=20.0):
+    p = fx.Project.from_inp_text(text, ctx)
+    p.default_initial_temperature = t_default
+    st = fx.SolutionState(p.num_dofs, p.num_nodes)
+    st.initialize(p)
+    return p, st
+
+
+def _oracle(text, t_default=20.0):
+    o = inp.parse_inp_text(text)
+    o.default_initial_temperature = t_default
+    return o, inp.model_arrays(o)
+
+
+def _csr(p, u, prec):
+    ip, ind, dat, md = p.assemble_csr(u, prec)
+    return sp.csr_matrix((dat, ind, ip), shape=(p.num_dofs, p.num_dofs)), md
+
+
+SMALL = {
+    "one_c3d4": lambda: decks.c3d4_cantilever(1, 1, 1),
+    "one_c3d20": lambda: decks.c3d20_box(1, 1, 1),
+    "c3d4_box": lambda: decks.c3d4_cantilever(3, 4, 5),
+    "c3d20_box": lambda: decks.c3d20_box(2, 3, 4),
+    "tdep_beam": lambda: decks.c3d4_nlgeom_beam(6, 2, 2),
+}
+
+
+@pytest.mark.parametrize("case", list(SMALL))
+@pytest.mark.parametrize("with_u", [False, True])
+def test_stiffness_matches_oracle(ctx, case, with_u):
+    text = SMALL[case]()
+    p, st = _project(ctx, text)
+    o, m = _oracle(text)
+    t = inp.initial_temperatures(o)
+    u = np.random.default_rng(1).normal(scale=1e-2, size=p.num_dofs) if with_u else None
+    K_or, md_or = elem.assemble(m, u, t)
+    scale = abs(K_or).max()
+    for prec, tol in ((fx.PREC_FP64, 1e-12), (fx.PREC_MIXED, 2e-6)):
+        K, md = _csr(p, u, prec)
+        assert abs(K - K_or).max() <= tol * scale, (case, prec)
+        assert abs(md - md_or) <= tol * md_or
+
+
+@pytest.mark.parametrize("case", list(SMALL))
+def test_internal_and_thermal_force_match_oracle(ctx, case):
+    text = SMALL[case]()
+    p, st = _project(ctx, text)
+    o, m = _oracle(text)
+    rng = np.random.default_rng(2)
+    t0 = inp.initial_temperatures(o)
+    t1 = t0 + rng.uniform(0, 150, size=t0.shape)   # T_cur != T_init exercises eps_th
+    st.set_temperatures(t0, t1)
+    u = rng.normal(scale=1e-2, size=p.num_dofs)
+    for uconf in (None, u):
+        f = p.internal_force(u, uconf)
+        f_or = elem.internal_force(m, u, uconf, t0, t1)
+        assert np.abs(f - f_or).max() <= 1e-11 * np.abs(f_or).max()
+    fth = p.thermal_force()
+    fth_or = elem.thermal_force(m, t0, t1)
+    if np.abs(fth_or).max() > 0:
+        assert np.abs(fth - fth_or).max() <= 1e-11 * np.abs(fth_or).max()
+    else:
+        assert np.abs(fth).max() == 0.0
+
+
+@pytest.mark.parametrize("name", ["C3D4_staticstep", "C3D4_2staticstep", "C3D20", "NLGEOM_test"])
+@pytest.mark.parametrize("prec", [fx.PREC_MIXED, fx.PREC_FP64])
+def test_reference_decks(ctx, golden_dir, name, prec):
+    gold = json.load(open(os.path.join(golden_dir, "calculix.json")))[name]
+    fix = np.load(os.path.join(golden_dir, f"oracle_{name}.npz"))
+    p, st = _project(ctx, _deck(golden_dir, name))
+    idx = p.mesh.get_index_for_node_id(gold["node"])
+    tol = 1e-6 if name.startswith("NLGEOM") else 1e-8
+    for k, want in enumerate(gold["steps"]):
+        stats = p.steps[k].solve(k + 1, p, st, opts=fx.solve_opts(precision=prec))
+        u = st.displacements
+        ref = fix[f"step{k + 1}"]
+        err = np.linalg.norm(u - ref) / np.linalg.norm(ref)
+        assert err <= tol, (name, k, err, stats)
+        assert np.all(np.abs(u[3 * idx:3 * idx + 3] - np.array(want)) < gold["tol"])
+
+
+def _oracle_run(text, t_default=20.0):
+    o = inp.parse_inp_text(text)
+    o.default_initial_temperature = t_default
+    r = static_step.Runner(o)
+    s = r.run()
+    return s.displacements, r
+
+
+@pytest.mark.parametrize("prec", [fx.PREC_MIXED, fx.PREC_FP64])
+def test_c3d4_cantilever_full_size(ctx, prec):
+    text = decks.c3d4_cantilever()   # 24,000 C3D4, 14,883 DOF
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    p.steps[0].solve(1, p, st, opts=fx.solve_opts(precision=prec))
+    u = st.displacements
+    assert np.linalg.norm(u - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("prec", [fx.PREC_MIXED, fx.PREC_FP64])
+def test_c3d20_jittered_box(ctx, prec):
+    text = decks.c3d20_box(4, 4, 16, lengths=(20.0, 20.0, 80.0))
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    p.steps[0].solve(1, p, st, opts=fx.solve_opts(precision=prec))
+    assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
+def test_nlgeom_thermal_beam(ctx):
+    # E(T) table, initial temperature gradient, *AMPLITUDE ramp, 4 increments, NLGEOM
+    text = decks.c3d4_nlgeom_beam(12, 3, 3, tip_load=2.0e3, increments=4)
+    ref, r = _oracle_run(text)
+    p, st = _project(ctx, text)
+    stats = p.steps[0].solve(1, p, st, opts=fx.solve_opts(precision=fx.PREC_MIXED))
+    assert stats["increments"] == sum(1 for l in r.log)
+    assert np.linalg.norm(st.displacements - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+def test_batch_matches_single(ctx):
+    pop = decks.batch_population(6, seed=11, dof_lo=500, dof_hi=6000, c3d20_fraction=0.3)
+    singles = []
+    for text, _ in pop:
+        p, st = _project(ctx, text)
+        p.steps[0].solve(1, p, st)
+        singles.append(st.displacements)
+    projs = [_project(ctx, text)[0] for text, _ in pop]
+    status, stats = fx.batch_solve(ctx, projs)
+    assert np.all(status == 0)
+    for p, u1, (text, _) in zip(projs, singles, pop):
+        st = fx.SolutionState(p.num_dofs, p.num_nodes)
+        st.project = p
+        u = st.displacements
+        assert np.array_equal(u, u1)  # same per-system arithmetic alone and in the batch
+        ref, _ = _oracle_run(text)
+        assert np.linalg.norm(u - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
+def test_solve_csr_seam(ctx):
+    text = decks.c3d4_cantilever(4, 4, 12)
+    o = inp.parse_inp_text(text)
+    r = static_step.Runner(o)
+    r.run()
+    K, R, du = r.last_K.tocsr(), r.last_R, r.last_du
+    K.sort_indices()
+    ip = K.indptr.astype(np.int64)
+    ind = K.indices.astype(np.int64)
+    lib = fx._lib.load()
+    for prec in (fx.PREC_MIXED, fx.PREC_FP64):
+        x = np.empty_like(R)
+        st = fx.StepStats()
+        o_ = fx.solve_opts(precision=prec)
+        rc = lib.fx_solve_csr(ctx.handle, K.shape[0], fx._p(ip), fx._p(ind), fx._p(K.data), fx._p(R), fx._p(x),
+                              C.byref(o_), C.byref(st))
+        assert rc == 0, lib.fx_ctx_last_error(ctx.handle)
+        assert np.linalg.norm(x - du) <= 1e-8 * np.linalg.norm(du)
+
+
+@pytest.mark.parametrize("prec", [fx.PREC_FP64_CSR])
+def test_plain_fp64_csr_jacobi(ctx, prec):
+    text = decks.c3d20_box(2, 2, 6)
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    p.steps[0].solve(1, p, st, opts=fx.solve_opts(precision=prec))
+    assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
+def test_iterative_solver_reference_semantics(ctx):
+    # *STATIC, SOLVER=ITERATIVE SCALING: Jacobi PCG with absolute sqrt(r.z) < 1e-8 and 1000 iterations
+    text = decks.c3d4_cantilever(2, 2, 3).replace("*Static, Solver=Spooles", "*Static, Solver=Iterative scaling")
+    ref, r = _oracle_run(text)
+    p, st = _project(ctx, text)
+    assert p.steps[0].info.solver == "ITERATIVE"
+    p.steps[0].solve(1, p, st, opts=fx.solve_opts(reference_iterative=True))
+    assert np.linalg.norm(st.displacements - ref) <= 1e-6 * np.linalg.norm(ref)
+    # the reference's 1000-iteration cap surfaces as ConvergenceError
+    big = decks.c3d4_cantilever(6, 6, 24).replace("*Static, Solver=Spooles", "*Static, Solver=Iterative scaling")
+    p, st = _project(ctx, big)
+    with pytest.raises(fx.FerrixError) as e:
+        p.steps[0].solve(1, p, st, opts=fx.solve_opts(reference_iterative=True))
+    assert e.value.kind == "ConvergenceError"
+
+
+def test_determinism(ctx):
+    text = decks.c3d20_box(2, 2, 6)
+    outs = []
+    for _ in range(2):
+        p, st = _project(ctx, text)
+        p.steps[0].solve(1, p, st)
+        outs.append(st.displacements)
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_errors_are_reported(ctx):
+    # element without material: SolutionState::initialize panics in the reference
+    bad = decks.c3d4_cantilever(1, 1, 1).replace("*Solid section, Elset=Vol, Material=Mat\n", "")
+    p = fx.Project.from_inp_text(bad, ctx)
+    with pytest.raises(fx.FerrixError) as e:
+        fx.SolutionState().initialize(p)
+    assert e.value.kind == "InvalidModelState"
+    # degenerate (flat) tet: singular Jacobian
+    flat = ("*NODE\n1,0,0,0\n2,1,0,0\n3,0,1,0\n4,1,1,0\n*ELEMENT, TYPE=C3D4, ELSET=E\n1,1,2,3,4\n"
+            "*MATERIAL, NAME=M\n*ELASTIC\n1000,0.3\n*SOLID SECTION, ELSET=E, MATERIAL=M\n"
+            "*STEP\n*STATIC\n*BOUNDARY\n1,1,3\n*CLOAD\n4,3,1.0\n*END STEP\n")
+    p, st = _project(ctx, flat)
+    with pytest.raises(fx.FerrixError) as e:
+        p.steps[0].solve(1, p, st)
+    assert e.value.kind == "NumericalError"
+    # PCG iteration cap
+    p, st = _project(ctx, decks.c3d4_cantilever(2, 2, 6))
+    with pytest.raises(fx.FerrixError) as e:
+        p.steps[0].solve(1, p, st, opts=fx.solve_opts(max_iter=2, poll_interval=2))
+    assert e.value.kind == "ConvergenceError"
+    # unknown node in an element: NodeNotFound at the first element loop
+    orphan = decks.c3d4_cantilever(1, 1, 1).replace("*Element, Type=C3D4, Elset=Solid\n",
+                                                    "*Element, Type=C3D4, Elset=Solid\n99, 1, 2, 3, 12345\n")
+    p, st = _project(ctx, orphan)
+    with pytest.raises(fx.FerrixError) as e:
+        p.steps[0].solve(1, p, st)
+    assert e.value.kind == "NodeNotFound"
