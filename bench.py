@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark of the linear-static C3D20 solve (the north-star workload).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp64|mixed|fp64_csr]
+
+Workload: C3D20 box 20x20x80 mm, 20x20x80 serendipity bricks (32,000 elements,
+139,041 nodes, 417,123 DOF), interior nodes jittered U(+-10% h) with a fixed
+seed, E=70000 MPa, nu=0.33, z=0 face clamped (*BOUNDARY 1..6), 5000 N in -x
+spread over the z=80 face nodes; written as `.inp` text and parsed like any deck.
+
+One step = one StaticStep::solve of that deck to a displacement accurate to
+1e-8 against the FP64 direct solution: residual, symbolic pattern (rebuilt every
+step), element stiffness + BSR3 assembly, penalty BCs, PCG to the stated
+tolerance, update, convergence re-check. `value` is solves/s over all ranks with
+the model already resident on the device; `e2e` is the same through the public
+API from host text and host buffers (parse, upload, solve, download).
+With N GPUs each rank solves its own replica (no collective: a single deck is
+not sharded); value = N*K / max-over-ranks time.
+
+The oracle (FP64 multifrontal Cholesky restatement of the reference's CPU path)
+runs in a separate process on the host cores during the GPU timing; it supplies
+the rel. error of the GPU solution and the `cpu_baseline` entry.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "C3D20 time-to-1e-8 (mixed vs FP64 GPU PCG); solves/s; serving p50/p99 latency"
+WORKLOAD = "C3D20 box 20x20x80 cells, 417,123 DOF, linear *STATIC, clamped z=0, 5000 N on z=80, tol 1e-8 vs FP64 direct"
+
+
+def _deck():
+    from ferrix_b200 import decks
+    return decks.c3d20_box()
+
+
+def _oracle_job(out_path: str, q) -> None:
+    """CPU reference path (oracle restatement): parse, serial assembly, CSR, FP64 Cholesky, Newton check."""
+    import numpy as np
+    from oracle import inp, static_step
+    text = _deck()
+    t0 = time.perf_counter()
+    p = inp.parse_inp_text(text)
+    r = static_step.Runner(p)
+    st = r.run()
+    dt = time.perf_counter() - t0
+    np.save(out_path, st.displacements)
+    q.put({"seconds": dt, "phases": {k: round(v, 3) for k, v in vars(r.t).items()},
+           "cores": os.cpu_count(), "blas_threads": os.environ.get("OPENBLAS_NUM_THREADS", "all")})
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for k, name in enumerate(names):
+                    if r[4 + k].lower().startswith("active"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    """--impl reference: the reference's CPU path (oracle port) on this host's cores, rank 0 only."""
+    if rank != 0:
+        return
+    q = mp.get_context("spawn").Queue()
+    t0 = time.perf_counter()
+    _oracle_job(os.path.join("/tmp", f"u_oracle_ref_{os.getpid()}.npy"), q)
+    res = q.get()
+    sec = res["seconds"]
+    line = {
+        "metric": METRIC, "impl": "reference", "value": 1.0 / sec, "unit": "solves/s", "n_gpus": world,
+        "steps": 1, "warmup": 0, "requested_steps": args.steps, "requested_warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded deck generator)",
+        "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": 1.0 / sec, "unit": "solves/s", "cores": res["cores"], "kind": "port",
+                         "sample": "one full-size solve (the step is ~minutes on the CPU, so 1 step regardless of K)",
+                         "phases_s": res["phases"]},
+        "e2e": {"value": 1.0 / sec, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp64_csr"])
+    ap.add_argument("--no-oracle", action="store_true", help="skip the CPU oracle (accuracy / cpu_baseline)")
+    ap.add_argument("--no-arms", action="store_true", help="skip the comparison arms")
+    ap.add_argument("--mode", default="solve", choices=["solve", "spmv"],
+                    help="spmv: only assemble and time REPS standalone SpMV launches (profiling case)")
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if args.mode == "spmv":
+        import ferrix_b200 as fx
+        ctx = fx.Context(local)
+        p = fx.Project.from_inp_text(_deck(), ctx)
+        st = fx.SolutionState(p.num_dofs, p.num_nodes)
+        st.initialize(p)
+        prec = {"fp64": fx.PREC_FP64, "mixed": fx.PREC_MIXED, "fp64_csr": fx.PREC_FP64}[args.precision]
+        ms, by = p.profile_spmv(prec, args.reps)
+        print(json.dumps({"mode": "spmv", "precision": args.precision, "ms_per_launch": ms, "bytes": by,
+                          "GBps": by / ms / 1e6}), flush=True)
+        p.close()
+        ctx.close()
+        return
+
+    # the oracle process starts before any CUDA initialisation (spawn)
+    oracle_q = oracle_p = None
+    oracle_out = os.path.join("/tmp", f"u_oracle_{os.getpid()}.npy")
+    if rank == 0 and not args.no_oracle:
+        ctxmp = mp.get_context("spawn")
+        oracle_q = ctxmp.Queue()
+        oracle_p = ctxmp.Process(target=_oracle_job, args=(oracle_out, oracle_q), daemon=True)
+        oracle_p.start()
+
+    import numpy as np
+    import torch
+    import ferrix_b200 as fx
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    prec = {"fp64": fx.PREC_FP64, "mixed": fx.PREC_MIXED, "fp64_csr": fx.PREC_FP64_CSR}[args.precision]
+    opts = fx.solve_opts(precision=prec, rtol=1e-8)
+    text = _deck()
+    ctx = fx.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    project = fx.Project.from_inp_text(text, ctx)
+    state = fx.SolutionState(project.num_dofs, project.num_nodes)
+
+    def one_step():
+        state.initialize(project)
+        project.drop_cache()
+        return project.steps[0].solve(1, project, state, opts=opts)
+
+    for _ in range(max(3, args.warmup)):
+        one_step()
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    clocks.start()
+    ev0.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        stats.append(one_step())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    launches = ctx.kernel_launches - launches0
+    u_gpu = state.displacements
+    if dist:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        dist.barrier()
+
+    # dominant kernel: the fused SpMV, timed standalone with CUDA events
+    spmv_ms, spmv_bytes = project.profile_spmv(prec if prec != fx.PREC_FP64_CSR else fx.PREC_FP64, 30)
+
+    # e2e through the public API from host text and host buffers
+    h2d = d2h = 0
+    e2e_elapsed = None
+    if rank == 0 or True:
+        def e2e_step():
+            p = fx.Project.from_inp_text(text, ctx)
+            s = fx.SolutionState(p.num_dofs, p.num_nodes)
+            s.initialize(p)
+            p.steps[0].solve(1, p, s, opts=opts)
+            u = s.displacements
+            p.close()
+            return u
+        e2e_step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ke = max(1, min(args.steps, 3))
+        for _ in range(ke):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_elapsed = e0.elapsed_time(e1) / 1e3 / ke
+        xyz, groups = project.export()
+        n_el = sum(len(g[1]) for g in groups.values())
+        h2d = (xyz.size * 8 + sum(g[0].size * 4 + g[1].size * 4 for g in groups.values())
+               + 2 * project.num_nodes * 8)
+        d2h = project.num_dofs * 8
+
+    arms = {}
+    if rank == 0 and not args.no_arms:
+        for name, pr in (("fp64_bsr_blockjacobi", fx.PREC_FP64), ("plain_fp64_csr_jacobi", fx.PREC_FP64_CSR),
+                         ("mixed_fp32_bsr", fx.PREC_MIXED)):
+            if pr == prec:
+                arms[name] = {"ms": elapsed / args.steps * 1e3, "pcg_iterations": stats[-1]["pcg_iterations"]}
+                continue
+            o2 = fx.solve_opts(precision=pr, rtol=1e-8)
+            state.initialize(project)
+            project.drop_cache()
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            try:
+                st = project.steps[0].solve(1, project, state, opts=o2)
+                a1.record(stream)
+                torch.cuda.synchronize()
+                arms[name] = {"ms": a0.elapsed_time(a1), "pcg_iterations": st["pcg_iterations"],
+                              "fp64_fallbacks": st["fp64_fallbacks"], "u": state.displacements}
+            except fx.FerrixError as e:
+                arms[name] = {"error": str(e)}
+
+    cpu = None
+    rel_err = None
+    if oracle_p is not None:
+        res = oracle_q.get(timeout=3600)
+        oracle_p.join(timeout=60)
+        u_ref = np.load(oracle_out)
+        rel_err = float(np.linalg.norm(u_gpu - u_ref) / np.linalg.norm(u_ref))
+        for a in arms.values():
+            if "u" in a:
+                a["rel_err_vs_oracle"] = float(np.linalg.norm(a["u"] - u_ref) / np.linalg.norm(u_ref))
+        cpu = {"value": 1.0 / res["seconds"], "unit": "solves/s", "cores": res["cores"], "kind": "port",
+               "sample": "one full-size solve of the same deck (parse, serial assembly, CSR, FP64 multifrontal "
+                         "Cholesky, Newton re-check), in a spawned process during the GPU timing",
+               "phases_s": res["phases"]}
+        try:
+            os.remove(oracle_out)
+        except OSError:
+            pass
+    for a in arms.values():
+        a.pop("u", None)
+
+    if rank == 0:
+        import json as _j
+        peaks = {}
+        try:
+            peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+        traffic = None  # DRAM read+write per launch from the committed ncu capture of the same kernel / workload
+        try:
+            import re
+            prof = open(os.path.join(ROOT, "profiles", "k_pcg_spmv_c3d20_box.md")).read()
+            m = re.search(r"traffic_bytes_per_launch[^|]*\|\s*([\d,]+)\s*\|\s*([\d,]+)", prof)
+            if m:
+                traffic = int((m.group(2) if prec == fx.PREC_MIXED else m.group(1)).replace(",", ""))
+        except OSError:
+            pass
+        s0 = stats[-1]
+        line = {
+            "metric": METRIC, "value": world * args.steps / elapsed, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": elapsed / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp64": "f64", "mixed": "f32 matrix / f64 residual", "fp64_csr": "f64"}[args.precision],
+            "data": "synthetic (seeded .inp deck generator; inputs exceed L2: BSR3 FP64 matrix ~600 MB)",
+            "config": {"workload": WORKLOAD, "precision": args.precision, "solver": "PCG + 3x3 block-Jacobi, BSR3",
+                       "rtol_M": 1e-8, "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+            "time_to_1e8_ms": elapsed / args.steps * 1e3,
+            "rel_err_vs_oracle": rel_err,
+            "pcg_iterations": s0["pcg_iterations"],
+            "phase_ms": {k: round(s0[k], 3) for k in ("t_assembly_ms", "t_pcg_ms", "t_total_ms")},
+            "arms": arms,
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "k_pcg_spmv (fused BSR3 SpMV + direction update + p.q)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else
+                         "fallback 6650 GB/s", "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms,
+                         "traffic": traffic, "traffic_source": "profiles/k_pcg_spmv_c3d20_box.md (ncu)"},
+            "clocks": clk,
+            "e2e": {"value": 1.0 / e2e_elapsed if e2e_elapsed else None, "unit": "solves/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": e2e_elapsed * 1e3 if e2e_elapsed else None},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    project.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -69,6 +69,11 @@ class Context:
     def kernel_launches(self) -> int:
         return int(self.lib.fx_ctx_kernel_launches(self.handle))
 
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the context (for CUDA events recorded by the caller)."""
+        return int(self.lib.fx_ctx_stream(self.handle) or 0)
+
     def close(self):
         if self.handle:
             for p in list(self._projects):
@@ -83,7 +88,7 @@ class Context:
             pass
 
 
-def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
+def solve_opts(precision: int = PREC_FP64, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
                reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
                reference_iterative: bool = False) -> SolveOpts:
     o = SolveOpts()
@@ -253,6 +258,16 @@ class Project:
         uc = None if uconf is None else np.ascontiguousarray(uconf, dtype=np.float64)
         _check(self.lib.fx_internal_force(self.handle, _p(uu), _p(uc), _p(f)), self.ctx)
         return f
+
+    def drop_cache(self) -> None:
+        _check(self.lib.fx_model_drop_cache(self.handle), self.ctx)
+
+    def profile_spmv(self, precision: int = PREC_FP64, reps: int = 20):
+        """(mean ms of one standalone SpMV launch, algorithmic bytes per launch)."""
+        ms = C.c_double()
+        by = C.c_double()
+        _check(self.lib.fx_profile_spmv(self.handle, precision, reps, C.byref(ms), C.byref(by)), self.ctx)
+        return ms.value, by.value
 
     def thermal_force(self) -> np.ndarray:
         f = np.empty(self.num_dofs)

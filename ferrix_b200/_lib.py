@@ -50,6 +50,7 @@ SIGNATURES = {
     "fx_ctx_destroy": (None, [P]),
     "fx_ctx_last_error": (C.c_char_p, [P]),
     "fx_ctx_kernel_launches": (C.c_int64, [P]),
+    "fx_ctx_stream": (C.c_void_p, [P]),
     "fx_model_from_inp": (C.c_int, [P, C.c_char_p, C.c_size_t, C.POINTER(P)]),
     "fx_model_destroy": (None, [P]),
     "fx_model_sizes": (C.c_int, [P, I64P, I64P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -69,6 +70,8 @@ SIGNATURES = {
     "fx_internal_force": (C.c_int, [P, P, P, P]),
     "fx_thermal_force": (C.c_int, [P, P]),
     "fx_solve_csr": (C.c_int, [P, C.c_int64, P, P, P, P, P, C.POINTER(SolveOpts), C.POINTER(StepStats)]),
+    "fx_model_drop_cache": (C.c_int, [P]),
+    "fx_profile_spmv": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_batch_solve": (C.c_int, [P, P, C.c_int, C.POINTER(SolveOpts), P, P]),
 }
 

@@ -24,11 +24,40 @@ static int guarded(fx_ctx* ctx, F&& f) {
     }
 }
 
+namespace {
+template <typename T>
+static double profile_t(fx_model* m, int reps, double* bytes) {
+    ModelDev& d = m->dev;
+    cudaStream_t s = m->ctx->stream;
+    const bool is64 = sizeof(T) == 8;
+    assemble(m, nullptr, is64);
+    const int64_t nn = m->dense.n_nodes;
+    DBuf<T> minv;
+    minv.alloc((size_t)nn * 9, s);
+    const T* vals = is64 ? (const T*)d.vals64.ptr : (const T*)d.vals32.ptr;
+    launch_block_jacobi<T>(d.S, vals, minv.ptr, s);
+    std::vector<double> ones(3 * (size_t)nn, 1.0);
+    d.R.upload(ones, s);
+    PcgSystem<T> sys;
+    sys.S = &d.S;
+    sys.vals = vals;
+    sys.minv = minv.ptr;
+    sys.b = d.R.ptr;
+    sys.x = d.du.ptr;
+    PcgBatch<T> batch;
+    double ms = batch.profile_spmv(sys, reps, s);
+    const double nb = (double)d.S.n_blocks, n3 = 3.0 * (double)nn;
+    *bytes = nb * (9.0 * sizeof(T) + 4.0) + 4.0 * (nn + 1) + 4.0 * sizeof(T) * n3;
+    return ms;
+}
+
+}  // namespace
+
 extern "C" {
 
 void fx_default_solve_opts(fx_solve_opts* o) {
     if (!o) return;
-    o->precision = FX_PREC_MIXED;
+    o->precision = FX_PREC_FP64;
     o->rtol = 1e-8;
     o->max_iter = 50000;
     o->poll_interval = 32;
@@ -77,6 +106,8 @@ void fx_ctx_destroy(fx_ctx* ctx) {
 const char* fx_ctx_last_error(const fx_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 
 int64_t fx_ctx_kernel_launches(const fx_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+void* fx_ctx_stream(const fx_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int fx_model_from_inp(fx_ctx* ctx, const char* text, size_t len, fx_model** out) {
     if (!out || (!text && len)) return FX_INVALID_ARGUMENT;
@@ -325,6 +356,42 @@ int fx_internal_force(fx_model* m, const double* u, const double* uconf, double*
 }
 
 int fx_thermal_force(fx_model* m, double* f) { return force_common(m, nullptr, nullptr, f, true); }
+
+int fx_model_drop_cache(fx_model* m) {
+    if (!m || !m->ctx) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        ModelDev& d = m->dev;
+        d.have_structure = false;
+        d.S = BsrStructure();
+        d.ebuf32.release();
+        d.vals32.release();
+        d.minv32.release();
+        d.ebuf64.release();
+        d.vals64.release();
+        d.minv64.release();
+        stream_wait(m->ctx->stream, "drop cache");
+        return FX_OK;
+    });
+}
+
+int fx_profile_spmv(fx_model* m, int precision, int reps, double* ms, double* bytes) {
+    if (!m || !m->ctx || !ms || !bytes || reps <= 0 || !m->state_ready) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        int64_t* saved = g_launch_counter;
+        g_launch_counter = &m->ctx->launches;
+        struct R {
+            int64_t* v;
+            ~R() { g_launch_counter = v; }
+        } r{saved};
+        ensure_dense(m);
+        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        ensure_structure(m);
+        *ms = precision == FX_PREC_MIXED ? profile_t<float>(m, reps, bytes) : profile_t<double>(m, reps, bytes);
+        return FX_OK;
+    });
+}
 
 int fx_batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts* opts, int* status,
                    fx_step_stats* stats) {

@@ -262,20 +262,20 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_replace(const ChunkDev* __r
 // ------------------------------------------------------------------ host loop
 
 template <typename T>
-int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, cudaStream_t s,
-                       int64_t* launches) {
+void PcgBatch<T>::prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::vector<ChunkDev>& all_chunks,
+                          std::vector<int>& chunk0, std::vector<int>& nch) {
     const int n = (int)sys.size();
-    if (n == 0) return FX_OK;
     work_.resize(n);
     std::vector<InstDev<T>> hi(n);
-    std::vector<ChunkDev> all_chunks;
+    all_chunks.clear();
     d_scal_.alloc((size_t)n * kNScal, s);
     d_scal_.zero(s);
     d_status_.alloc(n, s);
     d_status_.zero(s);
     d_counter_.alloc((size_t)n * 4, s);
     d_counter_.zero(s);
-    std::vector<int> chunk0(n), nch(n);
+    chunk0.assign(n, 0);
+    nch.assign(n, 0);
     for (int i = 0; i < n; ++i) {
         const int rows = sys[i]->S->n_rows;
         chunk0[i] = (int)all_chunks.size();
@@ -324,9 +324,37 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
         S.status = FX_OK;
         S.iterations = 0;
         S.replacements = 0;
+        S.stagnated = false;
     }
     d_inst_.upload(hi, s);
     d_chunks_.upload(all_chunks, s);
+}
+
+template <typename T>
+double PcgBatch<T>::profile_spmv(PcgSystem<T>& sys, int reps, cudaStream_t s) {
+    std::vector<PcgSystem<T>*> v{&sys};
+    std::vector<ChunkDev> chunks;
+    std::vector<int> c0, nc;
+    sys.warm_start = false;
+    prepare(v, s, chunks, c0, nc);
+    FX_LAUNCH(k_pcg_replace<T>, (unsigned)chunks.size(), kUpdThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, 1, 0.0);
+    for (int k = 0; k < 3; ++k)  // warm-up
+        FX_LAUNCH(k_pcg_spmv<T>, (unsigned)chunks.size(), kSpmvThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, k & 1);
+    EventTimer t;
+    t.start(s);
+    for (int k = 0; k < reps; ++k)
+        FX_LAUNCH(k_pcg_spmv<T>, (unsigned)chunks.size(), kSpmvThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, k & 1);
+    return t.stop_ms(s) / reps;
+}
+
+template <typename T>
+int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, cudaStream_t s,
+                       int64_t* launches) {
+    const int n = (int)sys.size();
+    if (n == 0) return FX_OK;
+    std::vector<ChunkDev> all_chunks;
+    std::vector<int> chunk0, nch;
+    prepare(sys, s, all_chunks, chunk0, nch);
     const double rtol2 = opt.rtol * opt.rtol;
     const bool trace = std::getenv("FX_DEBUG") != nullptr;
     FX_LAUNCH(k_pcg_replace<T>, (unsigned)all_chunks.size(), kUpdThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, 1,
@@ -345,6 +373,7 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
     std::vector<char> done(n, 0);
     std::vector<double> best(n, 1e300);
     std::vector<int> stall(n, 0);
+    std::vector<double> last_rep(n, 0.0);  // iteration of the last FP64 residual replacement
     for (int i = 0; i < n; ++i) {
         if (!(h_scal[i * kNScal + kBnorm] > 0.0)) {  // b = 0: x = 0 is exact
             done[i] = 1;
@@ -425,7 +454,12 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
             }
             bool reached = st == kConv;
             bool drop = sizeof(T) == 4 && sc[kRzRef] > 0.0 && sc[kRz] < opt.reliable_delta * opt.reliable_delta * sc[kRzRef];
-            if (reached || drop) replace.push_back(i);
+            // FP32 recurrences can stall above the replacement trigger: replace periodically too
+            bool periodic = sizeof(T) == 4 && sc[kIters] - last_rep[i] >= opt.replace_every;
+            if (reached || drop || periodic) {
+                replace.push_back(i);
+                last_rep[i] = sc[kIters];
+            }
             else if (sc[kIters] >= opt.max_iter) {
                 done[i] = 1;
                 sys[i]->status = FX_CONVERGENCE;

@@ -85,6 +85,7 @@ struct PcgOptions {
     double reliable_delta = 1e-2;
     bool graphs = true;
     int stall_limit = 4;  // replacements without halving the best FP64 residual before giving up (mixed)
+    int replace_every = 256;  // mixed: FP64 residual replacement at least this often (iterations)
 };
 
 template <typename T>
@@ -92,8 +93,12 @@ class PcgBatch {
    public:
     // Solves all systems; returns FX_OK or the first failing status (per-system status in sys[i].status).
     int solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, cudaStream_t s, int64_t* launches);
+    // Mean duration (ms) of one standalone launch of the fused SpMV kernel on this system.
+    double profile_spmv(PcgSystem<T>& sys, int reps, cudaStream_t s);
 
    private:
+    void prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::vector<ChunkDev>& chunks,
+                 std::vector<int>& chunk0, std::vector<int>& nch);
     struct Work {
         DBuf<T> r, z, p0, p1, q;
         DBuf<double> r64;

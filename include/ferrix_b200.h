@@ -103,6 +103,8 @@ void fx_ctx_destroy(fx_ctx* ctx);
 const char* fx_ctx_last_error(const fx_ctx* ctx);
 /* Number of kernel launches issued by this context so far (all entry points). */
 int64_t fx_ctx_kernel_launches(const fx_ctx* ctx);
+/* The context's cudaStream_t (as void*), for callers that time or order work on it. */
+void* fx_ctx_stream(const fx_ctx* ctx);
 
 /* ---- model (Project) -------------------------------------------------- */
 /* Preprocess + parse `.inp` text with the reference parser's semantics.
@@ -160,6 +162,16 @@ int fx_thermal_force(fx_model* model, double* f);
  * Solver::solve arguments are mapped by `opts`. */
 int fx_solve_csr(fx_ctx* ctx, int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
                  const double* b, double* x, const fx_solve_opts* opts, fx_step_stats* stats);
+
+/* Drops the cached sparsity pattern and assembled matrices of a model; the
+ * next solve rebuilds them (the symbolic phase then counts in its time). */
+int fx_model_drop_cache(fx_model* model);
+/* Measurement: assembles K (precision, X only, penalty applied) and times
+ * `reps` standalone launches of the PCG SpMV kernel with CUDA events on the
+ * context stream; *ms = mean duration of one launch, *bytes = algorithmic
+ * bytes of one launch (matrix values + column indices + row offsets + the
+ * two gathered vectors + the two written vectors, padding excluded). */
+int fx_profile_spmv(fx_model* model, int precision, int reps, double* ms, double* bytes);
 
 /* ---- batched decks ---------------------------------------------------- */
 /* Runs the first step of every model (each fx_state_initialize'd) with all
