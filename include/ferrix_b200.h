@@ -179,6 +179,21 @@ int fx_profile_spmv(fx_model* model, int precision, int reps, double* ms, double
 int fx_batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts* opts, int* status,
                    fx_step_stats* stats);
 
+/* ---- allocation-free SpMV with fused dot -------------------------------
+ * No counterpart in the reference. y = A x and *dot = x . y for an FP64 CSR
+ * matrix of n rows, all pointers on `device`, work queued on `stream`
+ * (cudaStream_t as void*, NULL = default stream); results are ready when the
+ * stream reaches them. For callers that may not allocate device memory (a
+ * loop being captured into a CUDA graph, a layer that only sees memory owned
+ * by the host application's own allocator, a real-time path): it calls no
+ * cudaMalloc / cudaFree and uses only a fixed ~513 KiB scratch array compiled
+ * into the library, held by every GPU that loads it until exit. Limit: at most
+ * 524,288 rows (FX_INVALID_ARGUMENT beyond). The first call on a device looks
+ * up the scratch address — make it before any stream capture. Calls share the
+ * scratch: calls that overlap on the GPU race and must be ordered. */
+int fx_spmv_dot_noalloc(int device, int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
+                        const double* x, double* y, double* dot, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
