@@ -373,7 +373,8 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
     std::vector<char> done(n, 0);
     std::vector<double> best(n, 1e300);
     std::vector<int> stall(n, 0);
-    std::vector<double> last_rep(n, 0.0);  // iteration of the last FP64 residual replacement
+    std::vector<double> last_rep(n, 0.0);      // iteration of the last FP64 residual replacement
+    std::vector<double> last_improve(n, 0.0);  // iteration at which the best FP64 residual last halved
     for (int i = 0; i < n; ++i) {
         if (!(h_scal[i * kNScal + kBnorm] > 0.0)) {  // b = 0: x = 0 is exact
             done[i] = 1;
@@ -487,14 +488,16 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
                 if (rel < 0.5 * best[i]) {
                     best[i] = rel;
                     stall[i] = 0;
+                    last_improve[i] = sc[kIters];
                 } else {
                     ++stall[i];
                 }
+                const bool slow = sc[kIters] - last_improve[i] >= opt.stall_iters || sc[kIters] >= 0.25 * opt.max_iter;
                 if (rel <= opt.rtol) {
                     done[i] = 1;
                     set_status(i, kIdle);
                     rebuild = true;
-                } else if (sizeof(T) == 4 && stall[i] >= opt.stall_limit) {
+                } else if (sizeof(T) == 4 && (stall[i] >= opt.stall_limit || slow)) {
                     done[i] = 1;
                     set_status(i, kIdle);
                     sys[i]->status = FX_CONVERGENCE;

@@ -85,7 +85,8 @@ struct PcgOptions {
     double reliable_delta = 1e-2;
     bool graphs = true;
     int stall_limit = 4;  // replacements without halving the best FP64 residual before giving up (mixed)
-    int replace_every = 256;  // mixed: FP64 residual replacement at least this often (iterations)
+    int replace_every = 512;  // mixed: FP64 residual replacement at least this often (iterations)
+    int stall_iters = 2048;   // mixed: give up on FP32 when the FP64 residual has not halved for this long
 };
 
 template <typename T>
