@@ -22,17 +22,17 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-import weakref
 from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
 import numpy as np
 
 from . import _lib
-from ._lib import PREC_FP64, PREC_FP64_CSR, PREC_MIXED, SolveOpts, StepStats
+from ._lib import PRECOND_AMG, PRECOND_BLOCK_JACOBI, PREC_FP64, PREC_FP64_CSR, PREC_MIXED, SolveOpts, StepStats
 
 __all__ = ["Context", "Project", "SolutionState", "SolverTime", "FerrixError", "SolveOptions", "solve_opts",
-           "batch_solve", "StepStats", "PREC_MIXED", "PREC_FP64", "PREC_FP64_CSR"]
+           "batch_solve", "StepStats", "PREC_MIXED", "PREC_FP64", "PREC_FP64_CSR", "PRECOND_AMG",
+           "PRECOND_BLOCK_JACOBI"]
 
 
 class FerrixError(Exception):
@@ -63,7 +63,10 @@ class Context:
         h = C.c_void_p()
         _check(self.lib.fx_ctx_create(device, C.byref(h)), None, f"fx_ctx_create({device})")
         self.handle = h
-        self._projects = weakref.WeakSet()  # models must be destroyed before their context
+        # raw handles of the live models bound to this context: models must be
+        # destroyed before their context, also when the garbage collector
+        # finalizes a context and its projects in arbitrary order
+        self._models = {}
 
     @property
     def kernel_launches(self) -> int:
@@ -76,8 +79,9 @@ class Context:
 
     def close(self):
         if self.handle:
-            for p in list(self._projects):
-                p.close()
+            for h in list(self._models.values()):
+                self.lib.fx_model_destroy(h)
+            self._models.clear()
             self.lib.fx_ctx_destroy(self.handle)
             self.handle = None
 
@@ -90,7 +94,7 @@ class Context:
 
 def solve_opts(precision: int = PREC_FP64, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
                reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
-               reference_iterative: bool = False) -> SolveOpts:
+               reference_iterative: bool = False, preconditioner: int = PRECOND_BLOCK_JACOBI) -> SolveOpts:
     o = SolveOpts()
     _lib.load().fx_default_solve_opts(C.byref(o))
     o.precision = precision
@@ -101,6 +105,7 @@ def solve_opts(precision: int = PREC_FP64, rtol: float = 1e-8, max_iter: int = 5
     o.use_graphs = int(use_graphs)
     o.verbose = int(verbose)
     o.reference_iterative = int(reference_iterative)
+    o.preconditioner = int(preconditioner)
     return o
 
 
@@ -195,7 +200,7 @@ class Project:
         self.steps: List[Step] = [Step(self, k) for k in range(ns.value)]
         self._default_t = 0.0
         if ctx is not None:
-            ctx._projects.add(self)
+            ctx._models[id(self)] = handle
 
     @classmethod
     def from_inp_text(cls, text: str, ctx: Optional[Context] = None) -> "Project":
@@ -276,7 +281,11 @@ class Project:
 
     def close(self):
         if self.handle:
-            self.lib.fx_model_destroy(self.handle)
+            if self.ctx is None:
+                self.lib.fx_model_destroy(self.handle)
+            elif self.ctx._models.pop(id(self), None) is not None:
+                self.lib.fx_model_destroy(self.handle)
+            # else: the context was closed first and destroyed this model with it
             self.handle = None
 
     def __del__(self):

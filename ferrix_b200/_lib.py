@@ -21,12 +21,14 @@ STATUS_NAMES = {
 PREC_MIXED = 0
 PREC_FP64 = 1
 PREC_FP64_CSR = 2
+PRECOND_BLOCK_JACOBI = 0
+PRECOND_AMG = 1
 
 
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("rtol", C.c_double), ("max_iter", C.c_int), ("poll_interval", C.c_int),
                 ("reliable_delta", C.c_double), ("use_graphs", C.c_int), ("verbose", C.c_int),
-                ("reference_iterative", C.c_int)]
+                ("reference_iterative", C.c_int), ("preconditioner", C.c_int)]
 
 
 class StepStats(C.Structure):
@@ -35,7 +37,7 @@ class StepStats(C.Structure):
                 ("last_rel_residual", C.c_double), ("last_linear_relres", C.c_double),
                 ("t_symbolic_ms", C.c_double), ("t_assembly_ms", C.c_double), ("t_forces_ms", C.c_double),
                 ("t_pcg_ms", C.c_double), ("t_total_ms", C.c_double), ("bsr_blocks", C.c_int64),
-                ("fp64_fallbacks", C.c_int)]
+                ("fp64_fallbacks", C.c_int), ("amg_levels", C.c_int), ("amg_setup_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

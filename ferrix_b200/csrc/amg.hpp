@@ -1,0 +1,87 @@
+// Aggregation multigrid preconditioner for the stiffness systems (3 DOF per
+// node), used inside PCG in place of the 3x3 block-Jacobi preconditioner.
+//
+// Hierarchy (setup, all on the GPU, deterministic):
+//   * aggregation by spatial binning of the level's points (nodes, then
+//     aggregate centroids) into cubic cells;
+//   * tentative prolongator from the six rigid-body modes (three translations,
+//     three rotations about the aggregate centroid): per aggregate a QR of the
+//     stacked near-null-space rows (one warp per aggregate, modified
+//     Gram-Schmidt applied twice); Q gives the prolongator rows, R the next
+//     level's near-null-space (Vanek, Mandel & Brezina 1996, without the
+//     prolongator smoothing step);
+//   * Galerkin coarse matrix A_c = Q^T A Q: fine blocks are sorted by their
+//     (aggregate, aggregate) key and every coarse 6x6 block sums Q_i^T A_ij Q_j
+//     over its fine blocks in a fixed order (no atomics);
+//   * Chebyshev smoothing of degree 2 on D^-1 A (D = block diagonal) with the
+//     largest eigenvalue from power iteration; dense inverse at the coarsest
+//     level.
+// Application: one V-cycle per PCG iteration.
+#pragma once
+
+#include <vector>
+
+#include "kernels.hpp"
+#include "pcg.hpp"
+
+namespace fx {
+
+struct AmgLevel {
+    int n = 0;   // block rows (nodes at level 0, aggregates above)
+    int bs = 3;  // block size
+    // level 0 matrix: the planar BSR3 of the fine system
+    const BsrStructure* S0 = nullptr;
+    const double* vals0 = nullptr;
+    const double* dinv0 = nullptr;  // 3x3 block inverses of the fine diagonal (block-Jacobi)
+    // coarse levels: row-major block CSR, blocks of bs x bs
+    DBuf<int32_t> row_ptr, cols;
+    DBuf<double> vals, dinv;
+    int64_t nblocks = 0;
+    double lmax = 0.0;
+    // transfer to the next level
+    DBuf<int32_t> agg;                 // aggregate of each block row
+    DBuf<double> Q;                    // n * bs * 6 prolongator rows
+    DBuf<int32_t> agg_ptr, agg_nodes;  // members of each aggregate
+    int n_agg = 0;
+    // work vectors (n * bs)
+    DBuf<double> x, b, r, d, t;
+    // coarsest level: dense inverse (n*bs)^2
+    bool coarsest = false;
+    DBuf<double> dense_inv;
+    const double* dinv_ptr() const { return S0 ? dinv0 : dinv.ptr; }
+};
+
+struct AmgStats {
+    int levels = 0;
+    std::vector<int> sizes;   // DOF per level
+    double setup_ms = 0.0;
+};
+
+class Amg {
+   public:
+    // xyz: FP64 node coordinates (device, 3 per node); dinv0: fine 3x3 block inverses.
+    void setup(const BsrStructure& S0, const double* vals0, const double* dinv0, const double* xyz, int n_nodes,
+               double cell0, cudaStream_t s, AmgStats* st);
+    // z = V-cycle(r), FP64 vectors of 3 * n_nodes.
+    void apply(const double* r, double* z, cudaStream_t s);
+    std::vector<AmgLevel> L;
+
+   private:
+    void vcycle(int l, cudaStream_t s);
+    DBuf<uint8_t> tmp_;
+    DBuf<double> red_;  // reduction scratch
+};
+
+// CG on the FP64 BSR3 system preconditioned by one V-cycle per iteration.
+class AmgPcg {
+   public:
+    int solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz, double cell0,
+              const double* b, double* x, const PcgOptions& opt, cudaStream_t s, int64_t* launches, long long* iters,
+              double* relres, AmgStats* st);
+    Amg amg;
+
+   private:
+    DBuf<double> r_, z_, p_, q_, part_, sc_;
+};
+
+}  // namespace fx

@@ -65,6 +65,7 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->use_graphs = 1;
     o->verbose = 0;
     o->reference_iterative = 0;
+    o->preconditioner = FX_PRECOND_BLOCK_JACOBI;
 }
 
 int fx_ctx_create(int device, fx_ctx** out) {

@@ -20,6 +20,7 @@
 
 #include "engine.hpp"
 #include "pcg_csr.hpp"
+#include "amg.hpp"
 
 namespace fx {
 
@@ -235,6 +236,10 @@ struct StepRunner {
     int csr_status = FX_OK;
     long long csr_iters = 0;
     double csr_relres = 0.0;
+    // aggregation-multigrid preconditioned FP64 CG (FX_PRECOND_AMG)
+    bool amg = false;
+    double amg_cell = 0.0;
+    DBuf<double> amg_xyz;
 
     void begin(fx_model* mm, int kk, const fx_solve_opts& oo) {
         m = mm;
@@ -249,7 +254,12 @@ struct StepRunner {
         step_id = k + 1;
         csr_reference = o.reference_iterative && step->solver == SolverType::Iterative;
         csr = o.precision == FX_PREC_FP64_CSR || csr_reference;
-        fp64 = o.precision == FX_PREC_FP64 || csr;
+        amg = !csr && o.preconditioner == FX_PRECOND_AMG;
+        fp64 = o.precision == FX_PREC_FP64 || csr || amg;
+        if (amg) {  // aggregate cells holding ~40 nodes on average
+            const double vol = m->dense.volume > 0.0 ? m->dense.volume : 1.0;
+            amg_cell = std::cbrt(40.0 * vol / (double)std::max<int64_t>(1, m->dense.n_nodes));
+        }
         cudaStream_t s = m->ctx->stream;
         ModelDev& d = m->dev;
         const size_t n3 = 3 * (size_t)m->dense.n_nodes;
@@ -386,6 +396,14 @@ struct StepRunner {
         if (csr) {
             launch_penalty<double>(d.S, d.vals64.ptr, bcv, d.maxdiag.ptr, d.R.ptr, ucur.ptr, s);
             csr_sys.from_bsr(d.S, d.vals64.ptr, s);
+        } else if (amg) {
+            launch_penalty<double>(d.S, d.vals64.ptr, bcv, d.maxdiag.ptr, d.R.ptr, ucur.ptr, s);
+            d.minv64.alloc((size_t)nn * 9, s);
+            launch_block_jacobi<double>(d.S, d.vals64.ptr, d.minv64.ptr, s);
+            amg_xyz.alloc(3 * (size_t)nn, s);
+            // aggregation and rigid-body modes on the configuration the tangent is taken at
+            launch_axpby(3 * nn, 1.0, d.xyz.ptr, step->nlgeom ? 1.0 : 0.0, step->nlgeom ? ucur.ptr : nullptr,
+                         amg_xyz.ptr, s);
         } else if (fp64) {
             launch_penalty<double>(d.S, d.vals64.ptr, bcv, d.maxdiag.ptr, d.R.ptr, ucur.ptr, s);
             d.minv64.alloc((size_t)nn * 9, s);
@@ -459,13 +477,14 @@ struct StepRunner {
     // u += du (static_step.rs:207-209); cut-back after 15 solves (:251-259)
     void after_solve() {
         const bool use64 = fp64 || fallback;
-        long long iters = csr ? csr_iters : use64 ? sys64.iterations : sys32.iterations;
-        int st = csr ? csr_status : use64 ? sys64.status : sys32.status;
+        const bool scalar = csr || amg;  // solved outside the batched BSR3 PCG
+        long long iters = scalar ? csr_iters : use64 ? sys64.iterations : sys32.iterations;
+        int st = scalar ? csr_status : use64 ? sys64.status : sys32.status;
         fallback = false;
         S.linear_solves++;
         S.pcg_iterations += iters;
-        S.reliable_updates += csr ? 0 : use64 ? sys64.replacements : sys32.replacements;
-        S.last_linear_relres = csr ? csr_relres : use64 ? sys64.relres : sys32.relres;
+        S.reliable_updates += scalar ? 0 : use64 ? sys64.replacements : sys32.replacements;
+        S.last_linear_relres = scalar ? csr_relres : use64 ? sys64.relres : sys32.relres;
         if (st == FX_NUMERICAL)
             fail(FX_NUMERICAL,
                  "Mathematical error: PCG breakdown (system not positive definite). Check for rigid body modes!");
@@ -547,9 +566,18 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         EventTimer ph;
         ph.start(s);
         std::vector<size_t> csr_ids, bsr_ids;
-        for (size_t i : solve) (rs[i]->csr ? csr_ids : bsr_ids).push_back(i);
+        for (size_t i : solve) (rs[i]->csr || rs[i]->amg ? csr_ids : bsr_ids).push_back(i);
         for (size_t i : csr_ids) {
             StepRunner& r = *rs[i];
+            if (r.amg) {
+                AmgStats ast;
+                r.csr_status = ctx->amgpcg.solve(r.m->dev.S, r.m->dev.vals64.ptr, r.m->dev.minv64.ptr,
+                                                 r.amg_xyz.ptr, r.amg_cell, r.m->dev.R.ptr, r.m->dev.du.ptr, po, s,
+                                                 &ctx->launches, &r.csr_iters, &r.csr_relres, &ast);
+                r.S.amg_levels = ast.levels;
+                r.S.amg_setup_ms += ast.setup_ms;
+                continue;
+            }
             PcgOptions pc = po;
             if (r.csr_reference) {  // iterative.rs:26-122 called with tol 1e-8, max_iter 1000 (static_step.rs:204)
                 pc.rtol = 1e-8;

@@ -9,6 +9,7 @@
 #include "model.hpp"
 #include "pcg.hpp"
 #include "pcg_csr.hpp"
+#include "amg.hpp"
 
 struct fx_ctx {
     int device = 0;
@@ -19,6 +20,7 @@ struct fx_ctx {
     fx::PcgBatch<float> pcg32;
     fx::PcgBatch<double> pcg64;
     fx::CsrPcg pcgcsr;
+    fx::AmgPcg amgpcg;
 };
 
 namespace fx {

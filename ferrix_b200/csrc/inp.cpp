@@ -628,6 +628,30 @@ DenseModel build_dense(const Project& p) {
         auto it = p.element_materials.find(eid);
         g.mat.push_back(it == p.element_materials.end() ? -1 : it->second);
     }
+    // mesh volume: tets exactly; bricks as 6 Kuhn tets of their 8 corner nodes
+    auto tet_vol = [&](int a, int b, int c, int e) {
+        const double* A = &d.xyz[3 * (size_t)a];
+        const double* B = &d.xyz[3 * (size_t)b];
+        const double* Cc = &d.xyz[3 * (size_t)c];
+        const double* E = &d.xyz[3 * (size_t)e];
+        double u[3], v[3], w[3];
+        for (int k = 0; k < 3; ++k) {
+            u[k] = B[k] - A[k];
+            v[k] = Cc[k] - A[k];
+            w[k] = E[k] - A[k];
+        }
+        return std::fabs(u[0] * (v[1] * w[2] - v[2] * w[1]) - u[1] * (v[0] * w[2] - v[2] * w[0]) +
+                         u[2] * (v[0] * w[1] - v[1] * w[0])) / 6.0;
+    };
+    for (int64_t e = 0; e < d.g4.size(); ++e) {
+        const int32_t* c = &d.g4.conn[4 * (size_t)e];
+        d.volume += tet_vol(c[0], c[1], c[2], c[3]);
+    }
+    static const int kuhn[6][4] = {{0, 1, 2, 6}, {0, 2, 3, 6}, {0, 3, 7, 6}, {0, 7, 4, 6}, {0, 4, 5, 6}, {0, 5, 1, 6}};
+    for (int64_t e = 0; e < d.g20.size(); ++e) {
+        const int32_t* c = &d.g20.conn[20 * (size_t)e];
+        for (auto& t : kuhn) d.volume += tet_vol(c[t[0]], c[t[1]], c[t[2]], c[t[3]]);
+    }
     MatTableHost& m = d.mats;
     for (const Material& mat : p.materials) {
         auto add = [&](bool has, const Lut& l, std::vector<int32_t>& off, std::vector<int32_t>& len) {

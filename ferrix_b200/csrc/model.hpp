@@ -122,6 +122,7 @@ struct DenseModel {
     ElemGroup g4, g20;
     MatTableHost mats;
     bool any_expansion = false;
+    double volume = 0.0;              // mesh volume (tets exact, bricks from their corner hexahedron)
     std::string missing_node_error;  // NodeNotFound deferred to the first element loop
     int64_t missing_node_id = -1;
 };

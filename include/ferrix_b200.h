@@ -80,7 +80,14 @@ typedef struct {
     int verbose;            /* print the reference's per-iteration |R| lines to stdout */
     int reference_iterative; /* SOLVER=ITERATIVE steps: reference semantics (Jacobi PCG, absolute
                                 sqrt(r.z) < 1e-8, at most 1000 iterations; iterative.rs:82-177) */
+    int preconditioner;     /* fx_preconditioner */
 } fx_solve_opts;
+
+/* Preconditioner of the BSR3 PCG. */
+typedef enum {
+    FX_PRECOND_BLOCK_JACOBI = 0, /* 3x3 block-Jacobi */
+    FX_PRECOND_AMG = 1           /* aggregation multigrid V-cycle (rigid-body near-null-space), FP64 CG */
+} fx_preconditioner;
 
 typedef struct {
     int increments;            /* increments attempted (converged or cut back) */
@@ -93,6 +100,8 @@ typedef struct {
     double t_symbolic_ms, t_assembly_ms, t_forces_ms, t_pcg_ms, t_total_ms;  /* device event times */
     int64_t bsr_blocks;        /* 3x3 blocks of the assembled stiffness */
     int fp64_fallbacks;        /* mixed solves that stalled and were finished in FP64 */
+    int amg_levels;            /* multigrid levels of the last AMG-preconditioned solve */
+    double amg_setup_ms;       /* multigrid setup time, summed over the step */
 } fx_step_stats;
 
 void fx_default_solve_opts(fx_solve_opts* opts);

@@ -221,6 +221,37 @@ def test_iterative_solver_reference_semantics(ctx, golden_dir):
     assert e.value.kind == "ConvergenceError"
 
 
+AMG_CASES = {
+    "c3d4_cantilever": lambda: decks.c3d4_cantilever(),
+    "c3d20_box": lambda: decks.c3d20_box(4, 4, 16, lengths=(20.0, 20.0, 80.0)),
+    "small_c3d20": lambda: decks.c3d20_box(2, 2, 3),
+    "c3d20_box_3_levels": lambda: decks.c3d20_box(8, 8, 32),
+}
+
+
+@pytest.mark.parametrize("case", list(AMG_CASES))
+def test_amg_preconditioned_solve(ctx, case):
+    text = AMG_CASES[case]()
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    stats = p.steps[0].solve(1, p, st, opts=fx.solve_opts(preconditioner=fx.PRECOND_AMG))
+    assert stats["amg_levels"] >= (3 if case.endswith("3_levels") else 2)
+    assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref), stats
+
+
+@pytest.mark.parametrize("name", ["C3D4_staticstep", "C3D20", "NLGEOM_test"])
+def test_amg_reference_decks(ctx, golden_dir, name):
+    gold = json.load(open(os.path.join(golden_dir, "calculix.json")))[name]
+    fix = np.load(os.path.join(golden_dir, f"oracle_{name}.npz"))
+    p, st = _project(ctx, _deck(golden_dir, name))
+    tol = 1e-6 if name.startswith("NLGEOM") else 1e-8
+    for k, want in enumerate(gold["steps"]):
+        stats = p.steps[k].solve(k + 1, p, st, opts=fx.solve_opts(preconditioner=fx.PRECOND_AMG))
+        ref = fix[f"step{k + 1}"]
+        err = np.linalg.norm(st.displacements - ref) / np.linalg.norm(ref)
+        assert err <= tol, (name, k, err, stats)
+
+
 def test_determinism(ctx):
     text = decks.c3d20_box(2, 2, 6)
     outs = []
