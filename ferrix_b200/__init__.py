@@ -94,7 +94,8 @@ class Context:
 
 def solve_opts(precision: int = PREC_FP64, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
                reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
-               reference_iterative: bool = False, preconditioner: int = PRECOND_BLOCK_JACOBI) -> SolveOpts:
+               reference_iterative: bool = False, preconditioner: int = PRECOND_BLOCK_JACOBI,
+               amg_aggregate_nodes: int = 40, amg_smoother_degree: int = 2) -> SolveOpts:
     o = SolveOpts()
     _lib.load().fx_default_solve_opts(C.byref(o))
     o.precision = precision
@@ -106,6 +107,8 @@ def solve_opts(precision: int = PREC_FP64, rtol: float = 1e-8, max_iter: int = 5
     o.verbose = int(verbose)
     o.reference_iterative = int(reference_iterative)
     o.preconditioner = int(preconditioner)
+    o.amg_aggregate_nodes = int(amg_aggregate_nodes)
+    o.amg_smoother_degree = int(amg_smoother_degree)
     return o
 
 

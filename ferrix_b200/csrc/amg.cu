@@ -163,6 +163,20 @@ struct FineView {
         int ng = goff[i + 1] - (int)g0;
         return vals[(g0 * 9 + (int64_t)(3 * r + c) * ng + k / 4) * 4 + (k & 3)];
     }
+    template <int BS>
+    __device__ __forceinline__ void load(int64_t b, int i, double* v) const {
+        if (BS == 6) {
+#pragma unroll
+            for (int k = 0; k < 36; ++k) v[k] = vals[b * 36 + k];
+        } else {
+            const int k = (int)(b - row_ptr[i]);
+            const int64_t g0 = goff[i];
+            const int ng = goff[i + 1] - (int)g0;
+            const double* base = vals + (g0 * 9 + k / 4) * 4 + (k & 3);
+#pragma unroll
+            for (int t = 0; t < 9; ++t) v[t] = base[(int64_t)t * ng * 4];
+        }
+    }
 };
 
 __global__ void k_coarse_keys(int64_t nb, FineView F, const int32_t* __restrict__ agg, int nbits,
@@ -195,35 +209,69 @@ __global__ void k_coarse_blocks(int64_t n, const uint64_t* __restrict__ keys, co
     }
 }
 
-// coarse block = sum over its fine blocks of Q_i^T A_ij Q_j (fixed order)
-__global__ void k_galerkin(int64_t ncb, const int64_t* __restrict__ seg, const int64_t* __restrict__ sorted_b,
-                           FineView F, const double* __restrict__ Q, double* __restrict__ cvals) {
-    int64_t cb = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (cb >= ncb) return;
-    const int bs = F.bs;
+// Coarse block = sum over its fine blocks of Q_i^T A_ij Q_j. One warp per coarse
+// block; lane k takes the k-th contiguous slice of the block's sorted fine blocks
+// (row-major within a key, so each row's blocks are adjacent): T = sum_j A_ij Q_j
+// is accumulated per row and Q_i^T T added when the row changes. The 36 sums are
+// combined by a fixed butterfly: no atomics, the result does not depend on timing.
+template <int BS>
+__global__ void __launch_bounds__(128) k_galerkin(int64_t ncb, const int64_t* __restrict__ seg,
+                                                  const int64_t* __restrict__ sorted_b, FineView F,
+                                                  const double* __restrict__ Q, double* __restrict__ cvals) {
+    const int64_t cb = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (cb >= ncb) return;  // warp-uniform
+    const int64_t s0 = seg[cb], len = seg[cb + 1] - s0;
+    const int64_t per = (len + 31) / 32;
+    const int64_t a = s0 + lane * per, e = min(a + per, s0 + len);
     double acc[36];
+#pragma unroll
     for (int k = 0; k < 36; ++k) acc[k] = 0.0;
-    for (int64_t s = seg[cb]; s < seg[cb + 1]; ++s) {
-        int64_t b = sorted_b[s];
-        int i = F.blk_row[b];
-        int j = F.col(b, i);
-        const double* Qi = Q + (size_t)i * bs * 6;
-        const double* Qj = Q + (size_t)j * bs * 6;
-        double T[6 * 6];  // A_ij Q_j (bs x 6)
-        for (int r = 0; r < bs; ++r)
-            for (int c = 0; c < 6; ++c) {
-                double t = 0.0;
-                for (int k = 0; k < bs; ++k) t += F.val(b, i, r, k) * Qj[k * 6 + c];
-                T[r * 6 + c] = t;
-            }
-        for (int r = 0; r < 6; ++r)
-            for (int c = 0; c < 6; ++c) {
-                double t = 0.0;
-                for (int k = 0; k < bs; ++k) t += Qi[k * 6 + r] * T[k * 6 + c];
-                acc[r * 6 + c] += t;
-            }
+    double T[BS * 6];
+    int cur = -1;
+    auto flush = [&]() {
+        const double* Qi = Q + (size_t)cur * BS * 6;
+#pragma unroll
+        for (int k = 0; k < BS; ++k) {
+            double q[6];
+#pragma unroll
+            for (int r = 0; r < 6; ++r) q[r] = Qi[k * 6 + r];
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+#pragma unroll
+                for (int c = 0; c < 6; ++c) acc[r * 6 + c] += q[r] * T[k * 6 + c];
+        }
+    };
+    for (int64_t s = a; s < e; ++s) {
+        const int64_t b = sorted_b[s];
+        const int i = F.blk_row[b];
+        const int j = F.col(b, i);
+        if (i != cur) {
+            if (cur >= 0) flush();
+            cur = i;
+#pragma unroll
+            for (int k = 0; k < BS * 6; ++k) T[k] = 0.0;
+        }
+        const double* Qj = Q + (size_t)j * BS * 6;
+        double v[BS * BS];
+        F.load<BS>(b, i, v);
+#pragma unroll
+        for (int k = 0; k < BS; ++k) {
+            double q[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) q[c] = Qj[k * 6 + c];
+#pragma unroll
+            for (int r = 0; r < BS; ++r)
+#pragma unroll
+                for (int c = 0; c < 6; ++c) T[r * 6 + c] += v[r * BS + k] * q[c];
+        }
     }
-    for (int k = 0; k < 36; ++k) cvals[cb * 36 + k] = acc[k];
+    if (cur >= 0) flush();
+#pragma unroll
+    for (int k = 0; k < 36; ++k) {
+        const double t = warp_sum(acc[k]);
+        if (lane == 0) cvals[cb * 36 + k] = t;
+    }
 }
 
 __global__ void k_expand_rows(int n, const int32_t* __restrict__ row_ptr, int32_t* __restrict__ blk_row) {
@@ -282,54 +330,6 @@ __global__ void k_block_inv6(int n, const int32_t* __restrict__ row_ptr, const i
 }
 
 // ------------------------------------------------------------------ level operators
-
-// y = A x (b == null) or y = b - A x, level 0 planar BSR3, 8 lanes per row
-__global__ void __launch_bounds__(256) k_l0_spmv(int n, const int32_t* __restrict__ goff,
-                                                 const int32_t* __restrict__ cols, const double* __restrict__ vals,
-                                                 const double* __restrict__ x, const double* __restrict__ b,
-                                                 double* __restrict__ y) {
-    const int sub = threadIdx.x & 7;
-    const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const int rows_per_grid = (gridDim.x * blockDim.x) >> 3;
-    const int nb = ((n + 3) / 4) * 4;  // uniform trip count per warp (4 rows per warp)
-    for (int base = row0 - (row0 & 3); base < nb; base += rows_per_grid) {
-        const int row = base + (row0 & 3);
-        const bool valid = row < n;
-        const int g0 = valid ? goff[row] : 0;
-        const int ng = valid ? goff[row + 1] - g0 : 0;
-        double a0 = 0, a1 = 0, a2 = 0;
-        for (int g = sub; g < ng; g += 8) {
-            const int4 cc = __ldg(reinterpret_cast<const int4*>(cols) + g0 + g);
-            const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
-            const double* vb = vals + ((int64_t)g0 * 9 + g) * 4;
-            const int64_t pl = (int64_t)ng * 4;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double x0 = x[3 * cj[q]], x1 = x[3 * cj[q] + 1], x2 = x[3 * cj[q] + 2];
-                a0 += vb[0 * pl + q] * x0 + vb[1 * pl + q] * x1 + vb[2 * pl + q] * x2;
-                a1 += vb[3 * pl + q] * x0 + vb[4 * pl + q] * x1 + vb[5 * pl + q] * x2;
-                a2 += vb[6 * pl + q] * x0 + vb[7 * pl + q] * x1 + vb[8 * pl + q] * x2;
-            }
-        }
-#pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
-            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-        }
-        if (valid && sub == 0) {
-            if (b) {
-                y[3 * row] = b[3 * row] - a0;
-                y[3 * row + 1] = b[3 * row + 1] - a1;
-                y[3 * row + 2] = b[3 * row + 2] - a2;
-            } else {
-                y[3 * row] = a0;
-                y[3 * row + 1] = a1;
-                y[3 * row + 2] = a2;
-            }
-        }
-    }
-}
 
 // coarse levels: row-major 6x6 blocks, one warp per block row
 __global__ void __launch_bounds__(256) k_ln_spmv(int n, const int32_t* __restrict__ row_ptr,
@@ -397,20 +397,26 @@ __global__ void k_cheb_step(int n, int bs, const double* __restrict__ dinv, doub
     }
 }
 
+// bc = Q^T rf per aggregate: one warp per aggregate, lanes over member rows
 __global__ void k_restrict(int na, const int32_t* __restrict__ ptr, const int32_t* __restrict__ nodes, int bs,
                            const double* __restrict__ Q, const double* __restrict__ rf, double* __restrict__ bc) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= na) return;
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (a >= na) return;  // warp-uniform
+    const int p0 = ptr[a], rows = (ptr[a + 1] - p0) * bs;
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int p = ptr[a]; p < ptr[a + 1]; ++p) {
-        int j = nodes[p];
-        for (int d = 0; d < bs; ++d) {
-            double rv = rf[(int64_t)j * bs + d];
-            const double* q = Q + ((int64_t)j * bs + d) * 6;
-            for (int c = 0; c < 6; ++c) acc[c] += q[c] * rv;
-        }
+    for (int r = lane; r < rows; r += 32) {
+        const int j = nodes[p0 + r / bs];
+        const int64_t row = (int64_t)j * bs + r % bs;
+        const double rv = rf[row];
+        const double* q = Q + row * 6;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc[c] += q[c] * rv;
     }
-    for (int c = 0; c < 6; ++c) bc[(int64_t)a * 6 + c] = acc[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        const double t = warp_sum(acc[c]);
+        if (lane == 0) bc[(int64_t)a * 6 + c] = t;
+    }
 }
 
 __global__ void k_prolong(int ndof, int bs, const int32_t* __restrict__ agg, const double* __restrict__ Q,
@@ -438,45 +444,108 @@ __global__ void k_dense_from_bsr(int n, const int32_t* __restrict__ row_ptr, con
                 A[(int64_t)(6 * i + r) * nd + 6 * cols[b] + c] = vals[(int64_t)b * 36 + r * 6 + c];
 }
 
-// In-place Gauss-Jordan inverse of an SPD matrix (one CTA); DOFs with a vanishing
-// diagonal are decoupled first and get zero rows/columns in the inverse.
-__global__ void __launch_bounds__(1024) k_dense_inverse(int nd, double* __restrict__ A, uint8_t* __restrict__ dead) {
-    __shared__ double s_dmax;
-    if (threadIdx.x == 0) {
-        double m = 0.0;
-        for (int k = 0; k < nd; ++k) m = fmax(m, fabs(A[(int64_t)k * nd + k]));
-        s_dmax = m;
-    }
+// Coarsest level: in-place blocked Gauss-Jordan inverse of the dense SPD matrix
+// (no pivoting), panels of kPanel pivots. Per panel K: the pivot block is
+// inverted by one CTA (P), the panel rows become P A[K, j], every other row i
+// gets A[i, j] -= A[i, K] (P A[K, j]) and A[i, K] = -A[i, K] P. DOFs with a
+// vanishing diagonal are decoupled first and get zero rows/columns in the inverse.
+constexpr int kPanel = 32;
+
+__global__ void __launch_bounds__(1024) k_dense_decouple(int nd, double* __restrict__ A, uint8_t* __restrict__ dead) {
+    __shared__ double s_red[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double m = 0.0;
+    for (int k = threadIdx.x; k < nd; k += blockDim.x) m = fmax(m, fabs(A[(int64_t)k * nd + k]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) s_red[warp] = m;
     __syncthreads();
-    for (int k = threadIdx.x; k < nd; k += blockDim.x) dead[k] = !(fabs(A[(int64_t)k * nd + k]) > 1e-12 * s_dmax);
+    double dmax = 0.0;
+    for (int w = 0; w < nw; ++w) dmax = fmax(dmax, s_red[w]);
+    for (int k = threadIdx.x; k < nd; k += blockDim.x) dead[k] = !(fabs(A[(int64_t)k * nd + k]) > 1e-12 * dmax);
     __syncthreads();
-    for (int64_t e = threadIdx.x; e < (int64_t)nd * nd; e += blockDim.x) {
-        int r = (int)(e / nd), c = (int)(e % nd);
-        if (dead[r] || dead[c]) A[e] = (r == c) ? 1.0 : 0.0;
-    }
+    for (int r = warp; r < nd; r += nw)
+        for (int c = lane; c < nd; c += 32)
+            if (dead[r] || dead[c]) A[(int64_t)r * nd + c] = (r == c) ? 1.0 : 0.0;
+}
+
+// P = inverse of the pivot block A[k0:k0+b, k0:k0+b], written in place (one CTA, 32 warps)
+__global__ void __launch_bounds__(1024) k_panel_inverse(int nd, int k0, int b, double* __restrict__ A) {
+    __shared__ double S[kPanel][kPanel + 1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    S[w][lane] = (w < b && lane < b) ? A[(int64_t)(k0 + w) * nd + k0 + lane] : (w == lane ? 1.0 : 0.0);
     __syncthreads();
-    for (int k = 0; k < nd; ++k) {
-        const double ip = 1.0 / A[(int64_t)k * nd + k];
+    for (int t = 0; t < b; ++t) {
+        const double ip = 1.0 / S[t][t];
         __syncthreads();
-        for (int c = threadIdx.x; c < nd; c += blockDim.x)
-            if (c != k) A[(int64_t)k * nd + c] *= ip;
+        if (w == t && lane != t) S[t][lane] *= ip;
         __syncthreads();
-        for (int64_t e = threadIdx.x; e < (int64_t)nd * nd; e += blockDim.x) {
-            int r = (int)(e / nd), c = (int)(e % nd);
-            if (r == k || c == k) continue;
-            A[e] -= A[(int64_t)r * nd + k] * A[(int64_t)k * nd + c];
+        const double f = S[w][t];
+        __syncthreads();
+        if (w != t) {
+            if (lane != t) S[w][lane] -= f * S[t][lane];
+            else S[w][t] = -f * ip;
         }
         __syncthreads();
-        for (int r = threadIdx.x; r < nd; r += blockDim.x)
-            if (r != k) A[(int64_t)r * nd + k] *= -ip;
-        __syncthreads();
-        if (threadIdx.x == 0) A[(int64_t)k * nd + k] = ip;
+        if (threadIdx.x == 0) S[t][t] = ip;
         __syncthreads();
     }
-    for (int64_t e = threadIdx.x; e < (int64_t)nd * nd; e += blockDim.x) {
-        int r = (int)(e / nd), c = (int)(e % nd);
-        if (dead[r] || dead[c]) A[e] = 0.0;
+    if (w < b && lane < b) A[(int64_t)(k0 + w) * nd + k0 + lane] = S[w][lane];
+}
+
+__device__ __forceinline__ void load_panel(int nd, int k0, int b, const double* A, double (*P)[kPanel]) {
+    for (int e = threadIdx.x; e < kPanel * kPanel; e += blockDim.x) {
+        const int r = e / kPanel, c = e % kPanel;
+        P[r][c] = (r < b && c < b) ? A[(int64_t)(k0 + r) * nd + k0 + c] : 0.0;
     }
+    __syncthreads();
+}
+
+// panel rows: A[K, j] = P A[K, j] for every column j outside K (one thread per column)
+__global__ void __launch_bounds__(128) k_panel_rows(int nd, int k0, int b, double* __restrict__ A) {
+    __shared__ double P[kPanel][kPanel];
+    load_panel(nd, k0, b, A, P);
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nd || (j >= k0 && j < k0 + b)) return;
+    double col[kPanel];
+#pragma unroll
+    for (int t = 0; t < kPanel; ++t) col[t] = t < b ? A[(int64_t)(k0 + t) * nd + j] : 0.0;
+    for (int r = 0; r < b; ++r) {
+        double s = 0.0;
+#pragma unroll
+        for (int t = 0; t < kPanel; ++t) s += P[r][t] * col[t];
+        A[(int64_t)(k0 + r) * nd + j] = s;
+    }
+}
+
+// every row i outside K (one warp per row): A[i, j] -= A[i, K] A[K, j], then A[i, K] = -A[i, K] P
+__global__ void __launch_bounds__(256) k_panel_trailing(int nd, int k0, int b, double* __restrict__ A) {
+    __shared__ double P[kPanel][kPanel];
+    load_panel(nd, k0, b, A, P);
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= nd || (i >= k0 && i < k0 + b)) return;  // warp-uniform
+    double* Ai = A + (int64_t)i * nd;
+    const double a = lane < b ? Ai[k0 + lane] : 0.0;
+    for (int j0 = 0; j0 < nd; j0 += 32) {  // uniform trip count: all lanes reach the shuffles
+        const int j = j0 + lane;
+        const bool valid = j < nd && !(j >= k0 && j < k0 + b);
+        double acc = 0.0;
+        for (int t = 0; t < b; ++t) {
+            const double at = __shfl_sync(0xffffffffu, a, t);
+            if (valid) acc += at * A[(int64_t)(k0 + t) * nd + j];
+        }
+        if (valid) Ai[j] -= acc;
+    }
+    double acc = 0.0;
+    for (int s = 0; s < b; ++s) acc += __shfl_sync(0xffffffffu, a, s) * P[s][lane];
+    if (lane < b) Ai[k0 + lane] = -acc;
+}
+
+__global__ void __launch_bounds__(256) k_dense_zero_dead(int nd, double* __restrict__ A,
+                                                         const uint8_t* __restrict__ dead) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (r >= nd) return;
+    for (int c = lane; c < nd; c += 32)
+        if (dead[r] || dead[c]) A[(int64_t)r * nd + c] = 0.0;
 }
 
 __global__ void k_dense_matvec(int nd, const double* __restrict__ A, const double* __restrict__ x,
@@ -507,11 +576,19 @@ __global__ void k_dot_part(int64_t n, const double* __restrict__ a, const double
 }
 
 __global__ void k_sum_part(int nb, const double* __restrict__ part, double* __restrict__ out) {
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int k = 0; k < nb; ++k) s += part[k];
-        *out = s;
-    }
+    double t = 0.0;
+    for (int k = threadIdx.x; k < nb; k += 32) t += part[k];
+    t = warp_sum(t);
+    if (threadIdx.x == 0) *out = t;
+}
+
+// x = d / sqrt(*nrm2), the norm read on the device
+__global__ void k_normalize(int64_t n, const double* __restrict__ nrm2, const double* __restrict__ d,
+                            double* __restrict__ x) {
+    const double v = *nrm2;
+    const double inv = v > 0.0 ? 1.0 / sqrt(v) : 1.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = d[i] * inv;
 }
 
 __global__ void k_fill_hash(int64_t n, double* __restrict__ v) {
@@ -531,9 +608,10 @@ unsigned grid_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); 
 
 // ---- outer PCG scalars: S[0] r.z, S[1] p.q, S[2] r.D^-1 r, S[3] b.D^-1 b, S[4] beta, S[5] alpha, S[6] breakdown
 __global__ void k_fin(int nb, const double* __restrict__ part, double* __restrict__ S, int what) {
+    double t = 0.0;  // fixed lane assignment and tree: deterministic
+    for (int k = threadIdx.x; k < nb; k += 32) t += part[k];
+    t = warp_sum(t);
     if (threadIdx.x != 0) return;
-    double t = 0.0;
-    for (int k = 0; k < nb; ++k) t += part[k];
     if (what == 0) {  // p.q -> alpha
         S[1] = t;
         if (!(t > 0.0) || !isfinite(t)) {
@@ -550,33 +628,6 @@ __global__ void k_fin(int nb, const double* __restrict__ part, double* __restric
     } else if (what == 3) {  // initial: r.z and b.D^-1 b
         S[0] = t;
         S[4] = 0.0;
-    }
-}
-
-// x += alpha p, r -= alpha q, partial r . D^-1 r (3x3 blocks)
-__global__ void k_amg_update(int n, const double* __restrict__ S, const double* __restrict__ p,
-                             const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r,
-                             const double* __restrict__ dinv, double* __restrict__ part) {
-    __shared__ double sh[8];
-    const double alpha = S[5];
-    double acc = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double rv[3];
-        for (int c = 0; c < 3; ++c) {
-            x[3 * i + c] += alpha * p[3 * i + c];
-            rv[c] = r[3 * i + c] - alpha * q[3 * i + c];
-            r[3 * i + c] = rv[c];
-        }
-        const double* D = dinv + 9 * (int64_t)i;
-        for (int c = 0; c < 3; ++c) acc += rv[c] * (D[3 * c] * rv[0] + D[3 * c + 1] * rv[1] + D[3 * c + 2] * rv[2]);
-    }
-    acc = warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w];
-        part[blockIdx.x] = s;
     }
 }
 
@@ -606,46 +657,307 @@ __global__ void k_xpby(int64_t n, const double* __restrict__ z, const double* __
         p[i] = z[i] + beta * p[i];
 }
 
+
+// ------------------------------------------------------------------ level 0: fused operators
+// One pass over the planar BSR3 matrix (8 lanes per block row, FP64 accumulation,
+// values in VT = double or float) followed by a row-local epilogue:
+//   kL0Resid  y = b - A v (y = A v without b)
+//   kL0RUpd   r -= A v
+//   kL0Cheb0  r = b - A v; d = c2 D^-1 r; xo = v + d             (first Chebyshev step from v = x)
+//   kL0ChebK  r -= A v; d = c1 v + c2 D^-1 r; xo += d            (later steps, v = previous direction)
+//   kL0Apply  y = A v
+// With dot = 1 the CTA partials of v.y give alpha = r.z / p.q; with dot = 2 the
+// partials of b.xo give r.z and beta (the last V-cycle step of the outer CG).
+// The last CTA to finish sums the partials in a fixed order.
+enum : int { kL0Resid = 0, kL0RUpd = 1, kL0Cheb0 = 2, kL0ChebK = 3, kL0Apply = 4 };
+
+template <typename VT>
+struct L0Op {
+    int n;
+    const int32_t* goff;
+    const int32_t* cols;
+    const VT* vals;
+    const double* v;
+    const double* b;
+    double* y;
+    double* r;
+    double* d_out;
+    double* xo;
+    const double* dinv;
+    double c1, c2;
+    int dot;
+    double* part;
+    int* counter;
+    double* S;
+};
+
+__device__ __forceinline__ void ld4v(const float* p, float o[4]) {
+    const float4 v = __ldcs(reinterpret_cast<const float4*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+}
+__device__ __forceinline__ void ld4v(const double* p, double o[4]) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
+}
+
+// Fixed-order CTA sum, then the last CTA to arrive reduces all CTA partials and
+// finalises the outer CG scalars.
+__device__ __forceinline__ void cta_dot_finalize(double v, int mode, double* part, int* counter, double* S) {
+    __shared__ double sh[32];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < nw; ++k) t += sh[k];
+        part[blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last || w != 0) return;
+    __threadfence();
+    double t = 0.0;
+    for (int k = lane; k < (int)gridDim.x; k += 32) t += __ldcg(part + k);
+    t = warp_sum(t);
+    if (lane != 0) return;
+    *counter = 0;
+    if (mode == 1) {  // p.q -> alpha
+        S[1] = t;
+        if (!(t > 0.0) || !isfinite(t)) {
+            S[6] = 1.0;
+            S[5] = 0.0;
+        } else {
+            S[5] = S[0] / t;
+        }
+    } else {  // new r.z -> beta
+        S[4] = S[0] > 0.0 ? t / S[0] : 0.0;
+        S[0] = t;
+    }
+}
+
+constexpr int kL0MinBlocks = 4;  // 256-thread CTAs resident per SM (caps registers at 64)
+
+template <typename VT, int MODE>
+__global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
+    const int sub = threadIdx.x & 7;
+    const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const int rows_per_grid = (gridDim.x * blockDim.x) >> 3;
+    const int nb = ((o.n + 3) / 4) * 4;  // uniform trip count per warp (4 rows per warp)
+    const double* __restrict__ v = o.v;
+    double dsum = 0.0;
+    for (int base = row0 - (row0 & 3); base < nb; base += rows_per_grid) {
+        const int row = base + (row0 & 3);
+        const bool valid = row < o.n;
+        const int g0 = valid ? o.goff[row] : 0;
+        const int ng = valid ? o.goff[row + 1] - g0 : 0;
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int g = sub; g < ng; g += 8) {
+            const int4 cc = __ldg(reinterpret_cast<const int4*>(o.cols) + g0 + g);
+            const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
+            double xv[4][3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) xv[q][k] = __ldg(v + 3 * (int64_t)cj[q] + k);
+            const VT* vb = o.vals + ((int64_t)g0 * 9 + g) * 4;
+            const int64_t pl = (int64_t)ng * 4;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                VT m0[4], m1[4], m2[4];
+                ld4v(vb + (3 * r) * pl, m0);
+                ld4v(vb + (3 * r + 1) * pl, m1);
+                ld4v(vb + (3 * r + 2) * pl, m2);
+                double t = 0.0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    t += (double)m0[q] * xv[q][0] + (double)m1[q] * xv[q][1] + (double)m2[q] * xv[q][2];
+                acc[r] += t;
+            }
+        }
+#pragma unroll
+        for (int s = 4; s > 0; s >>= 1)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], s);
+        // epilogue: lane c of the row's 8 handles component c
+        const int64_t o3 = 3 * (int64_t)row;
+        const int c = sub < 3 ? sub : 0;
+        const double axc = c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]);
+        double rr[3] = {0.0, 0.0, 0.0};
+        if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
+            if (valid && sub < 3) {
+                const double* src = MODE == kL0Cheb0 ? o.b : o.r;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) rr[k] = src[o3 + k] - acc[k];
+            }
+            __syncwarp();  // every lane has read r before lane c overwrites r[c]
+        }
+        if (!valid || sub >= 3) continue;
+        if (MODE == kL0Resid) {
+            o.y[o3 + c] = o.b ? o.b[o3 + c] - axc : axc;
+        } else if (MODE == kL0RUpd) {
+            o.r[o3 + c] -= axc;
+        } else if (MODE == kL0Apply) {
+            o.y[o3 + c] = axc;
+            dsum += v[o3 + c] * axc;
+        } else {  // Chebyshev steps
+            const double* D = o.dinv + 9 * (int64_t)row + 3 * c;
+            const double z = D[0] * rr[0] + D[1] * rr[1] + D[2] * rr[2];
+            const double rc = c == 0 ? rr[0] : (c == 1 ? rr[1] : rr[2]);
+            o.r[o3 + c] = rc;
+            const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * v[o3 + c]) + o.c2 * z;
+            o.d_out[o3 + c] = dn;
+            const double xn = (MODE == kL0Cheb0 ? v[o3 + c] : o.xo[o3 + c]) + dn;
+            o.xo[o3 + c] = xn;
+            if (o.dot) dsum += o.b[o3 + c] * xn;
+        }
+    }
+    if (o.dot) cta_dot_finalize(dsum, o.dot, o.part, o.counter, o.S);
+}
+
+// first pre-smoothing step from x = 0: d = c2 D^-1 b; x = d; r = b
+__global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const double* __restrict__ b,
+                                double* __restrict__ r, double* __restrict__ d, double* __restrict__ x, double c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t o3 = 3 * (int64_t)i;
+    const double bb[3] = {b[o3], b[o3 + 1], b[o3 + 2]};
+    const double* D = dinv + 9 * (int64_t)i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const double t = c2 * (D[3 * c] * bb[0] + D[3 * c + 1] * bb[1] + D[3 * c + 2] * bb[2]);
+        r[o3 + c] = bb[c];
+        d[o3 + c] = t;
+        x[o3 + c] = t;
+    }
+}
+
+// x += alpha p, r -= alpha q; r.D^-1 r reduced by the last CTA into S[2]
+__global__ void __launch_bounds__(256) k_amg_update2(int n, double* __restrict__ S, const double* __restrict__ p,
+                                                     const double* __restrict__ q, double* __restrict__ x,
+                                                     double* __restrict__ r, const double* __restrict__ dinv,
+                                                     double* __restrict__ part, int* __restrict__ counter) {
+    __shared__ double sh[32];
+    __shared__ int s_last;
+    const double alpha = S[5];
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double rv[3];
+        for (int c = 0; c < 3; ++c) {
+            x[3 * i + c] += alpha * p[3 * i + c];
+            rv[c] = r[3 * i + c] - alpha * q[3 * i + c];
+            r[3 * i + c] = rv[c];
+        }
+        const double* D = dinv + 9 * (int64_t)i;
+        for (int c = 0; c < 3; ++c) acc += rv[c] * (D[3 * c] * rv[0] + D[3 * c + 1] * rv[1] + D[3 * c + 2] * rv[2]);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    acc = warp_sum(acc);
+    if (lane == 0) sh[w] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < nw; ++k) t += sh[k];
+        part[blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last || w != 0) return;
+    __threadfence();
+    double t = 0.0;
+    for (int k = lane; k < (int)gridDim.x; k += 32) t += __ldcg(part + k);
+    t = warp_sum(t);
+    if (lane == 0) {
+        S[2] = t;
+        *counter = 0;
+    }
+}
+
+__global__ void k_f64_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host side
 
+// Grid of the level-0 operators: at most one wave of resident CTAs (grid-stride rows).
+static unsigned l0_grid(int n) {
+    static int cached_dev = -1, cached_cap = 0;
+    int dev = 0;
+    FX_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev != cached_dev) {
+        int sms = 0, per_sm = 0;
+        FX_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_l0_op<double, kL0ChebK>, 256, 0));
+        cached_cap = std::max(1, sms * std::max(1, per_sm));
+        cached_dev = dev;
+    }
+    return (unsigned)std::min<int64_t>(grid_for((int64_t)n * 8), cached_cap);
+}
+
+template <typename VT>
+static L0Op<VT> l0_op(const AmgLevel& l, const VT* vals) {
+    L0Op<VT> o{};
+    o.n = l.n;
+    o.goff = l.S0->goff.ptr;
+    o.cols = l.S0->cols.ptr;
+    o.vals = vals;
+    o.dinv = l.dinv0;
+    return o;
+}
+
 static void level_spmv(const AmgLevel& l, const double* x, const double* b, double* y, cudaStream_t s) {
     if (l.S0) {
-        int blocks = std::min<int64_t>(grid_for((int64_t)l.n * 8), 148 * 16);
-        FX_LAUNCH(k_l0_spmv, blocks, 256, 0, s, l.n, l.S0->goff.ptr, l.S0->cols.ptr, l.vals0, x, b, y);
+        L0Op<double> o = l0_op<double>(l, l.vals0);
+        o.v = x;
+        o.b = b;
+        o.y = y;
+        FX_LAUNCH((k_l0_op<double, kL0Resid>), l0_grid(l.n), 256, 0, s, o);
     } else {
         FX_LAUNCH(k_ln_spmv, grid_for((int64_t)l.n * 32), 256, 0, s, l.n, l.row_ptr.ptr, l.cols.ptr, l.vals.ptr, x, b,
                   y);
     }
 }
 
-static double dot(const double* a, const double* b, int64_t n, DBuf<double>& red, cudaStream_t s) {
+// red[nb] = a . b (deterministic, stays on the device)
+static void dot_dev(const double* a, const double* b, int64_t n, DBuf<double>& red, cudaStream_t s) {
     const int nb = 296;
-    red.alloc(nb + 1, s);
+    if (red.n < (size_t)nb + 1) red.alloc(nb + 1, s);
     FX_LAUNCH(k_dot_part, nb, 256, 0, s, n, a, b, red.ptr);
     FX_LAUNCH(k_sum_part, 1, 32, 0, s, nb, red.ptr, red.ptr + nb);
-    double v = 0.0;
-    FX_CUDA_CHECK(cudaMemcpyAsync(&v, red.ptr + nb, sizeof(double), cudaMemcpyDeviceToHost, s));
-    stream_wait(s, "amg dot");
-    return v;
 }
 
+// Largest eigenvalue of D^-1 A by 12 power iterations from a fixed hashed start
+// vector, normalised on the device; one host read at the end.
 static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s) {
     const int64_t nd = (int64_t)l.n * l.bs;
+    const int nb = 296;
     FX_LAUNCH(k_fill_hash, grid_for(nd), 256, 0, s, nd, l.x.ptr);
-    double lam = 1.0;
+    dot_dev(l.x.ptr, l.x.ptr, nd, red, s);
+    FX_LAUNCH(k_normalize, grid_for(nd), 256, 0, s, nd, red.ptr + nb, l.x.ptr, l.x.ptr);
     for (int it = 0; it < 12; ++it) {
-        level_spmv(l, l.x.ptr, nullptr, l.t.ptr, s);                 // t = A x
+        level_spmv(l, l.x.ptr, nullptr, l.t.ptr, s);  // t = A x, |x| = 1
         FX_LAUNCH(k_cheb_init, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.t.ptr, l.d.ptr, l.r.ptr, 1.0,
-                  1);                                                 // d = D^-1 A x
-        double nd2 = dot(l.d.ptr, l.d.ptr, nd, red, s);
-        double nx2 = dot(l.x.ptr, l.x.ptr, nd, red, s);
-        lam = nx2 > 0 ? std::sqrt(nd2 / nx2) : 1.0;
-        double inv = nd2 > 0 ? 1.0 / std::sqrt(nd2) : 1.0;
-        FX_LAUNCH(k_scale, grid_for(nd), 256, 0, s, nd, inv, l.d.ptr, l.x.ptr);
+                  1);  // d = D^-1 A x
+        dot_dev(l.d.ptr, l.d.ptr, nd, red, s);
+        FX_LAUNCH(k_normalize, grid_for(nd), 256, 0, s, nd, red.ptr + nb, l.d.ptr, l.x.ptr);
     }
-    l.lmax = 1.1 * lam;
+    double nd2 = 0.0;
+    FX_CUDA_CHECK(cudaMemcpyAsync(&nd2, red.ptr + nb, sizeof(double), cudaMemcpyDeviceToHost, s));
+    stream_wait(s, "amg eigenvalue estimate");
+    l.lmax = 1.1 * (nd2 > 0.0 ? std::sqrt(nd2) : 1.0);
 }
 
 void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0, const double* xyz, int n_nodes,
@@ -691,7 +1003,14 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
                       l.dense_inv.ptr);
             DBuf<uint8_t> dead;
             dead.alloc(nd, s);
-            FX_LAUNCH(k_dense_inverse, 1, 1024, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
+            FX_LAUNCH(k_dense_decouple, 1, 1024, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
+            for (int k0 = 0; k0 < (int)nd; k0 += kPanel) {
+                const int b = std::min<int>(kPanel, (int)nd - k0);
+                FX_LAUNCH(k_panel_inverse, 1, 1024, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+                FX_LAUNCH(k_panel_rows, grid_for(nd, 128), 128, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+                FX_LAUNCH(k_panel_trailing, grid_for(nd * 32), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+            }
+            FX_LAUNCH(k_dense_zero_dead, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
             stream_wait(s, "amg coarse inverse");
             break;
         }
@@ -800,8 +1119,12 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
             return cub::DeviceScan::InclusiveSum(t, b, cnt.ptr, c.row_ptr.ptr + 1, na, s);
         }, tmp_, s);
         c.vals.alloc((size_t)ncb * 36, s);
-        FX_LAUNCH(k_galerkin, grid_for(ncb, 128), 128, 0, s, (int64_t)ncb, seg.ptr, cb_s.ptr, F, lf.Q.ptr,
-                  c.vals.ptr);
+        if (F.bs == 3)
+            FX_LAUNCH(k_galerkin<3>, grid_for((int64_t)ncb * 32, 128), 128, 0, s, (int64_t)ncb, seg.ptr, cb_s.ptr, F,
+                      lf.Q.ptr, c.vals.ptr);
+        else
+            FX_LAUNCH(k_galerkin<6>, grid_for((int64_t)ncb * 32, 128), 128, 0, s, (int64_t)ncb, seg.ptr, cb_s.ptr, F,
+                      lf.Q.ptr, c.vals.ptr);
         stream_wait(s, "amg galerkin");
         // next level points and near-null-space
         coords = std::move(cent);
@@ -816,21 +1139,43 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
     }
 }
 
-// Chebyshev polynomial smoother of degree 2 on D^-1 A over [lmax/30, lmax].
-static void smooth(AmgLevel& l, bool zero_x, cudaStream_t s) {
-    const double lmax = l.lmax, lmin = lmax / 30.0;
+// Chebyshev polynomial smoother on D^-1 A over [lmax/30, lmax] (degree = steps):
+// d_1 = D^-1 r_0 / theta, then r_k = r_{k-1} - A d_k,
+// d_{k+1} = rho_k rho_{k-1} d_k + (2 rho_k / delta) D^-1 r_k with
+// rho_0 = delta / theta, rho_k = 1 / (2 theta / delta - rho_{k-1}); x += every d.
+struct ChebCoef {
+    double c2_start;
+    double c1[8], c2[8];
+};
+static ChebCoef cheb_coef(double lmax, int degree) {
+    const double lmin = lmax / 30.0;
     const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
     const double sigma = theta / delta;
-    const double rho = 1.0 / sigma;
-    const double rho1 = 1.0 / (2.0 * sigma - rho);
+    ChebCoef k{};
+    k.c2_start = 1.0 / theta;
+    double rho = 1.0 / sigma;
+    for (int s = 1; s < degree; ++s) {
+        const double rho1 = 1.0 / (2.0 * sigma - rho);
+        k.c1[s] = rho1 * rho;
+        k.c2[s] = 2.0 * rho1 / delta;
+        rho = rho1;
+    }
+    return k;
+}
+
+// coarse levels (6x6 blocks): separate SpMV and update kernels
+static void smooth(AmgLevel& l, bool zero_x, int degree, cudaStream_t s) {
+    const ChebCoef k = cheb_coef(l.lmax, degree);
     const int64_t nd = (int64_t)l.n * l.bs;
     if (zero_x) FX_CUDA_CHECK(cudaMemcpyAsync(l.r.ptr, l.b.ptr, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
     else level_spmv(l, l.x.ptr, l.b.ptr, l.r.ptr, s);  // r = b - A x
-    FX_LAUNCH(k_cheb_init, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.r.ptr, l.d.ptr, l.x.ptr, 1.0 / theta,
+    FX_LAUNCH(k_cheb_init, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.r.ptr, l.d.ptr, l.x.ptr, k.c2_start,
               zero_x ? 1 : 0);
-    level_spmv(l, l.d.ptr, nullptr, l.t.ptr, s);  // t = A d
-    FX_LAUNCH(k_cheb_step, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.r.ptr, l.t.ptr, l.d.ptr, l.x.ptr,
-              rho1 * rho, 2.0 * rho1 / delta);
+    for (int st = 1; st < degree; ++st) {
+        level_spmv(l, l.d.ptr, nullptr, l.t.ptr, s);  // t = A d
+        FX_LAUNCH(k_cheb_step, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.r.ptr, l.t.ptr, l.d.ptr, l.x.ptr,
+                  k.c1[st], k.c2[st]);
+    }
 }
 
 void Amg::vcycle(int lev, cudaStream_t s) {
@@ -841,21 +1186,86 @@ void Amg::vcycle(int lev, cudaStream_t s) {
         return;
     }
     AmgLevel& c = L[lev + 1];
-    smooth(l, true, s);
+    smooth(l, true, degree_, s);
     level_spmv(l, l.x.ptr, l.b.ptr, l.r.ptr, s);  // r = b - A x
-    FX_LAUNCH(k_restrict, grid_for(l.n_agg), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs, l.Q.ptr,
-              l.r.ptr, c.b.ptr);
+    FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs,
+              l.Q.ptr, l.r.ptr, c.b.ptr);
     vcycle(lev + 1, s);
     FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, l.bs, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr);
-    smooth(l, false, s);
+    smooth(l, false, degree_, s);
 }
 
-void Amg::apply(const double* r, double* z, cudaStream_t s) {
+// Level 0 with the fused operators: pre-smoothing from x = 0 (one elementwise
+// start, degree-1 fused steps, one fused residual update), coarse correction,
+// post-smoothing written straight into z. With S != null the last step also
+// reduces r.z and beta for the outer CG.
+template <typename VT>
+void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
+                  cudaStream_t s) {
     AmgLevel& l = L[0];
-    const int64_t nd = (int64_t)l.n * l.bs;
-    FX_CUDA_CHECK(cudaMemcpyAsync(l.b.ptr, r, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    vcycle(0, s);
-    FX_CUDA_CHECK(cudaMemcpyAsync(z, l.x.ptr, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    AmgLevel& c = L[1];
+    const int64_t nd = (int64_t)l.n * 3;
+    const ChebCoef k = cheb_coef(l.lmax, degree_);
+    const unsigned grid = l0_grid(l.n);
+    double* dA = l.d.ptr;
+    double* dB = l.t.ptr;
+    FX_LAUNCH(k_l0_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.dinv0, b, l.r.ptr, dA, l.x.ptr, k.c2_start);
+    L0Op<VT> o = l0_op<VT>(l, vals);
+    for (int st = 1; st < degree_; ++st) {
+        o.v = dA;
+        o.r = l.r.ptr;
+        o.d_out = dB;
+        o.xo = l.x.ptr;
+        o.c1 = k.c1[st];
+        o.c2 = k.c2[st];
+        FX_LAUNCH((k_l0_op<VT, kL0ChebK>), grid, 256, 0, s, o);
+        std::swap(dA, dB);
+    }
+    o = l0_op<VT>(l, vals);
+    o.v = dA;
+    o.r = l.r.ptr;
+    FX_LAUNCH((k_l0_op<VT, kL0RUpd>), grid, 256, 0, s, o);  // r = b - A x
+    FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
+              l.Q.ptr, l.r.ptr, c.b.ptr);
+    vcycle(1, s);
+    FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr);
+    o = l0_op<VT>(l, vals);
+    o.v = l.x.ptr;
+    o.b = b;
+    o.r = l.r.ptr;
+    o.d_out = dA;
+    o.xo = z;
+    o.c2 = k.c2_start;
+    if (degree_ == 1 && S) {
+        o.dot = 2;
+        o.part = part;
+        o.counter = counter;
+        o.S = S;
+    }
+    FX_LAUNCH((k_l0_op<VT, kL0Cheb0>), grid, 256, 0, s, o);
+    for (int st = 1; st < degree_; ++st) {
+        o = l0_op<VT>(l, vals);
+        o.v = dA;
+        o.b = b;
+        o.r = l.r.ptr;
+        o.d_out = dB;
+        o.xo = z;
+        o.c1 = k.c1[st];
+        o.c2 = k.c2[st];
+        if (st == degree_ - 1 && S) {
+            o.dot = 2;
+            o.part = part;
+            o.counter = counter;
+            o.S = S;
+        }
+        FX_LAUNCH((k_l0_op<VT, kL0ChebK>), grid, 256, 0, s, o);
+        std::swap(dA, dB);
+    }
+}
+
+void Amg::apply(const double* r, double* z, double* S, double* part, int* counter, cudaStream_t s) {
+    if (vals0_f32_) vcycle0<float>(vals0_f32_, r, z, S, part, counter, s);
+    else vcycle0<double>(L[0].vals0, r, z, S, part, counter, s);
 }
 
 // ------------------------------------------------------------------ AMG-preconditioned CG (FP64)
@@ -865,36 +1275,50 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
                   int64_t* launches, long long* iters, double* relres, AmgStats* st) {
     const int n = S.n_rows;
     const int64_t nd = 3 * (int64_t)n;
+    if (opt.amg_degree < 1 || opt.amg_degree > 8) fail(FX_INVALID_ARGUMENT, "multigrid smoother degree must be 1..8");
     amg.setup(S, vals64, dinv64, xyz, n, cell0, s, st);
-    AmgLevel& l0 = amg.L[0];
+    const float* v32 = nullptr;
+    if (opt.amg_fp32) {
+        const int64_t nv = (int64_t)S.n_groups * 36;
+        vals32_.alloc(nv, s);
+        FX_LAUNCH(k_f64_to_f32, 148 * 8, 256, 0, s, nv, vals64, vals32_.ptr);
+        v32 = vals32_.ptr;
+    }
+    amg.set_smoother(opt.amg_degree, v32);
     r_.alloc(nd, s);
     z_.alloc(nd, s);
     p_.alloc(nd, s);
     q_.alloc(nd, s);
     const int nb = 296;
-    part_.alloc(nb, s);
+    const unsigned g0 = l0_grid(n);
+    part_.alloc(std::max<int64_t>(nb, g0), s);
     sc_.alloc(8, s);
     sc_.zero(s);
+    counter_.alloc(1, s);
+    counter_.zero(s);
     FX_CUDA_CHECK(cudaMemsetAsync(x, 0, nd * sizeof(double), s));
     FX_CUDA_CHECK(cudaMemcpyAsync(r_.ptr, b, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    // ||b||_D, z = V(b), rz, p = z
+    // ||b||_D, z = V(b) with r.z, p = z
     FX_LAUNCH(k_rdr_part, nb, 256, 0, s, n, r_.ptr, dinv64, part_.ptr);
     FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 1);
     FX_CUDA_CHECK(cudaMemcpyAsync(sc_.ptr + 3, sc_.ptr + 2, sizeof(double), cudaMemcpyDeviceToDevice, s));
-    amg.apply(r_.ptr, z_.ptr, s);
+    amg.apply(r_.ptr, z_.ptr, nullptr, nullptr, nullptr, s);
     FX_LAUNCH(k_dot_part, nb, 256, 0, s, nd, r_.ptr, z_.ptr, part_.ptr);
     FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 3);
     FX_CUDA_CHECK(cudaMemcpyAsync(p_.ptr, z_.ptr, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    const AmgLevel& l0 = amg.L[0];
     auto iteration = [&]() {
-        const int spmv_grid = (int)std::min<int64_t>(grid_for((int64_t)n * 8), 148 * 16);
-        FX_LAUNCH(k_l0_spmv, spmv_grid, 256, 0, s, n, S.goff.ptr, S.cols.ptr, vals64, p_.ptr, nullptr, q_.ptr);
-        FX_LAUNCH(k_dot_part, nb, 256, 0, s, nd, p_.ptr, q_.ptr, part_.ptr);
-        FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 0);
-        FX_LAUNCH(k_amg_update, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr);
-        FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 1);
-        amg.apply(r_.ptr, z_.ptr, s);
-        FX_LAUNCH(k_dot_part, nb, 256, 0, s, nd, r_.ptr, z_.ptr, part_.ptr);
-        FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 2);
+        L0Op<double> o = l0_op<double>(l0, vals64);
+        o.v = p_.ptr;
+        o.y = q_.ptr;
+        o.dot = 1;
+        o.part = part_.ptr;
+        o.counter = counter_.ptr;
+        o.S = sc_.ptr;
+        FX_LAUNCH((k_l0_op<double, kL0Apply>), g0, 256, 0, s, o);  // q = A p, alpha
+        FX_LAUNCH(k_amg_update2, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
+                  counter_.ptr);                                    // x, r, r.D^-1 r
+        amg.apply(r_.ptr, z_.ptr, sc_.ptr, part_.ptr, counter_.ptr, s);  // z = V(r), r.z, beta
         FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, z_.ptr, sc_.ptr, p_.ptr);
     };
     const int per_poll = 4;
@@ -907,8 +1331,9 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         g_launch_counter = &count;
         FX_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         for (int k = 0; k < per_poll; ++k) iteration();
-        FX_CUDA_CHECK(cudaStreamEndCapture(s, &g));
+        const cudaError_t ce = cudaStreamEndCapture(s, &g);
         g_launch_counter = saved;
+        FX_CUDA_CHECK(ce);
         per_iter_launches = count;
         FX_CUDA_CHECK(cudaGraphInstantiate(&gexec, g, 0));
         cudaGraphDestroy(g);
@@ -939,15 +1364,13 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     }
     if (gexec) cudaGraphExecDestroy(gexec);
     // true residual of the assembled FP64 system in the block-Jacobi norm
-    const int spmv_grid = (int)std::min<int64_t>(grid_for((int64_t)n * 8), 148 * 16);
-    FX_LAUNCH(k_l0_spmv, spmv_grid, 256, 0, s, n, S.goff.ptr, S.cols.ptr, vals64, x, b, q_.ptr);
+    level_spmv(l0, x, b, q_.ptr, s);
     FX_LAUNCH(k_rdr_part, nb, 256, 0, s, n, q_.ptr, dinv64, part_.ptr);
     FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 1);
     FX_CUDA_CHECK(cudaMemcpyAsync(h, sc_.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
     stream_wait(s, "amg pcg final");
     if (iters) *iters = it;
     if (relres) *relres = h[3] > 0.0 ? std::sqrt(std::max(0.0, h[2]) / h[3]) : 0.0;
-    (void)l0;
     return rc;
 }
 

@@ -62,12 +62,23 @@ class Amg {
     // xyz: FP64 node coordinates (device, 3 per node); dinv0: fine 3x3 block inverses.
     void setup(const BsrStructure& S0, const double* vals0, const double* dinv0, const double* xyz, int n_nodes,
                double cell0, cudaStream_t s, AmgStats* st);
-    // z = V-cycle(r), FP64 vectors of 3 * n_nodes.
-    void apply(const double* r, double* z, cudaStream_t s);
+    // Smoother settings: Chebyshev degree (1..8) and, when vals_f32 is not null,
+    // FP32 values of the fine matrix for the level-0 smoothing (FP64 vectors).
+    void set_smoother(int degree, const float* vals_f32) {
+        degree_ = degree;
+        vals0_f32_ = vals_f32;
+    }
+    // z = V-cycle(r), FP64 vectors of 3 * n_nodes. With S != null the last
+    // smoothing step also reduces r.z into the outer CG scalars (S[0], S[4]).
+    void apply(const double* r, double* z, double* S, double* part, int* counter, cudaStream_t s);
     std::vector<AmgLevel> L;
 
    private:
     void vcycle(int l, cudaStream_t s);
+    template <typename VT>
+    void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter, cudaStream_t s);
+    int degree_ = 2;
+    const float* vals0_f32_ = nullptr;
     DBuf<uint8_t> tmp_;
     DBuf<double> red_;  // reduction scratch
 };
@@ -82,6 +93,8 @@ class AmgPcg {
 
    private:
     DBuf<double> r_, z_, p_, q_, part_, sc_;
+    DBuf<float> vals32_;
+    DBuf<int> counter_;
 };
 
 }  // namespace fx

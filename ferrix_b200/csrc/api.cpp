@@ -66,6 +66,8 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->verbose = 0;
     o->reference_iterative = 0;
     o->preconditioner = FX_PRECOND_BLOCK_JACOBI;
+    o->amg_aggregate_nodes = 40;
+    o->amg_smoother_degree = 2;
 }
 
 int fx_ctx_create(int device, fx_ctx** out) {

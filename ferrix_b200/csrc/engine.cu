@@ -256,9 +256,10 @@ struct StepRunner {
         csr = o.precision == FX_PREC_FP64_CSR || csr_reference;
         amg = !csr && o.preconditioner == FX_PRECOND_AMG;
         fp64 = o.precision == FX_PREC_FP64 || csr || amg;
-        if (amg) {  // aggregate cells holding ~40 nodes on average
+        if (amg) {  // aggregate cells holding amg_aggregate_nodes nodes on average
             const double vol = m->dense.volume > 0.0 ? m->dense.volume : 1.0;
-            amg_cell = std::cbrt(40.0 * vol / (double)std::max<int64_t>(1, m->dense.n_nodes));
+            const double per = o.amg_aggregate_nodes > 0 ? (double)o.amg_aggregate_nodes : 40.0;
+            amg_cell = std::cbrt(per * vol / (double)std::max<int64_t>(1, m->dense.n_nodes));
         }
         cudaStream_t s = m->ctx->stream;
         ModelDev& d = m->dev;
@@ -539,6 +540,8 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         po.poll = rs[0]->o.poll_interval;
         po.reliable_delta = rs[0]->o.reliable_delta;
         po.graphs = rs[0]->o.use_graphs != 0;
+        po.amg_degree = rs[0]->o.amg_smoother_degree > 0 ? rs[0]->o.amg_smoother_degree : 2;
+        po.amg_fp32 = rs[0]->o.precision == FX_PREC_MIXED;
     }
     while (true) {
         bool any = false;

@@ -87,6 +87,9 @@ struct PcgOptions {
     int stall_limit = 4;  // replacements without halving the best FP64 residual before giving up (mixed)
     int replace_every = 512;  // mixed: FP64 residual replacement at least this often (iterations)
     int stall_iters = 2048;   // mixed: give up on FP32 when the FP64 residual has not halved for this long
+    // multigrid preconditioner
+    int amg_degree = 2;       // Chebyshev smoothing steps per pre/post smoothing
+    bool amg_fp32 = false;    // FP32 fine-matrix values in the level-0 smoother
 };
 
 template <typename T>

@@ -81,12 +81,15 @@ typedef struct {
     int reference_iterative; /* SOLVER=ITERATIVE steps: reference semantics (Jacobi PCG, absolute
                                 sqrt(r.z) < 1e-8, at most 1000 iterations; iterative.rs:82-177) */
     int preconditioner;     /* fx_preconditioner */
+    int amg_aggregate_nodes; /* FX_PRECOND_AMG: mean nodes per fine aggregate (cell size); 0 = 40 */
+    int amg_smoother_degree; /* FX_PRECOND_AMG: Chebyshev steps per pre/post smoothing, 1..8; 0 = 2 */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */
 typedef enum {
     FX_PRECOND_BLOCK_JACOBI = 0, /* 3x3 block-Jacobi */
-    FX_PRECOND_AMG = 1           /* aggregation multigrid V-cycle (rigid-body near-null-space), FP64 CG */
+    FX_PRECOND_AMG = 1           /* aggregation multigrid V-cycle (rigid-body near-null-space), FP64 CG;
+                                    with FX_PREC_MIXED the fine-level smoother reads FP32 matrix values */
 } fx_preconditioner;
 
 typedef struct {

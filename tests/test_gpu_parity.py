@@ -230,12 +230,25 @@ AMG_CASES = {
 
 
 @pytest.mark.parametrize("case", list(AMG_CASES))
-def test_amg_preconditioned_solve(ctx, case):
+@pytest.mark.parametrize("prec", [fx.PREC_FP64, fx.PREC_MIXED])
+def test_amg_preconditioned_solve(ctx, case, prec):
+    """Multigrid-preconditioned CG (FP64 outer iteration; with PREC_MIXED the
+    fine-level smoother reads FP32 values) against the oracle's direct solve."""
     text = AMG_CASES[case]()
     ref, _ = _oracle_run(text)
     p, st = _project(ctx, text)
-    stats = p.steps[0].solve(1, p, st, opts=fx.solve_opts(preconditioner=fx.PRECOND_AMG))
+    stats = p.steps[0].solve(1, p, st, opts=fx.solve_opts(preconditioner=fx.PRECOND_AMG, precision=prec))
     assert stats["amg_levels"] >= (3 if case.endswith("3_levels") else 2)
+    assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref), stats
+
+
+@pytest.mark.parametrize("degree", [1, 3])
+def test_amg_smoother_degree(ctx, degree):
+    text = AMG_CASES["c3d20_box_3_levels"]()
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    opts = fx.solve_opts(preconditioner=fx.PRECOND_AMG, amg_smoother_degree=degree, amg_aggregate_nodes=60)
+    stats = p.steps[0].solve(1, p, st, opts=opts)
     assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref), stats
 
 
