@@ -277,6 +277,13 @@ class Project:
         _check(self.lib.fx_profile_spmv(self.handle, precision, reps, C.byref(ms), C.byref(by)), self.ctx)
         return ms.value, by.value
 
+    def profile_smoother(self, precision: int = PREC_MIXED, reps: int = 20):
+        """(mean ms, compulsory bytes) of one fused fine-level multigrid smoothing step."""
+        ms = C.c_double()
+        by = C.c_double()
+        _check(self.lib.fx_profile_smoother(self.handle, precision, reps, C.byref(ms), C.byref(by)), self.ctx)
+        return ms.value, by.value
+
     def thermal_force(self) -> np.ndarray:
         f = np.empty(self.num_dofs)
         _check(self.lib.fx_thermal_force(self.handle, _p(f)), self.ctx)

@@ -75,6 +75,7 @@ SIGNATURES = {
     "fx_solve_csr": (C.c_int, [P, C.c_int64, P, P, P, P, P, C.POINTER(SolveOpts), C.POINTER(StepStats)]),
     "fx_model_drop_cache": (C.c_int, [P]),
     "fx_profile_spmv": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fx_profile_smoother": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_batch_solve": (C.c_int, [P, P, C.c_int, C.POINTER(SolveOpts), P, P]),
     "fx_spmv_dot_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, P, P, P, P]),
 }

@@ -1270,6 +1270,60 @@ void Amg::apply(const double* r, double* z, double* S, double* part, int* counte
 
 // ------------------------------------------------------------------ AMG-preconditioned CG (FP64)
 
+double profile_smoother_op(const BsrStructure& S, const double* vals64, const double* dinv64, bool fp32, int reps,
+                           cudaStream_t s, double* bytes) {
+    const int n = S.n_rows;
+    const int64_t nd = 3 * (int64_t)n;
+    DBuf<float> v32;
+    if (fp32) {
+        const int64_t nv = (int64_t)S.n_groups * 36;
+        v32.alloc(nv, s);
+        FX_LAUNCH(k_f64_to_f32, 148 * 8, 256, 0, s, nv, vals64, v32.ptr);
+    }
+    DBuf<double> v, r, d, xo;
+    for (DBuf<double>* b : {&v, &r, &d, &xo}) {
+        b->alloc(nd, s);
+        FX_LAUNCH(k_fill_hash, grid_for(nd), 256, 0, s, nd, b->ptr);
+    }
+    AmgLevel l;
+    l.n = n;
+    l.S0 = &S;
+    l.vals0 = vals64;
+    l.dinv0 = dinv64;
+    const unsigned grid = l0_grid(n);
+    auto launch = [&]() {
+        if (fp32) {
+            L0Op<float> o = l0_op<float>(l, v32.ptr);
+            o.v = v.ptr;
+            o.r = r.ptr;
+            o.d_out = d.ptr;
+            o.xo = xo.ptr;
+            o.c1 = 0.5;
+            o.c2 = 1e-9;
+            FX_LAUNCH((k_l0_op<float, kL0ChebK>), grid, 256, 0, s, o);
+        } else {
+            L0Op<double> o = l0_op<double>(l, vals64);
+            o.v = v.ptr;
+            o.r = r.ptr;
+            o.d_out = d.ptr;
+            o.xo = xo.ptr;
+            o.c1 = 0.5;
+            o.c2 = 1e-9;
+            FX_LAUNCH((k_l0_op<double, kL0ChebK>), grid, 256, 0, s, o);
+        }
+    };
+    for (int k = 0; k < 3; ++k) launch();
+    EventTimer t;
+    t.start(s);
+    for (int k = 0; k < reps; ++k) launch();
+    const double ms = t.stop_ms(s) / reps;
+    // compulsory bytes: matrix values + column indices once, row offsets, and per
+    // node the gathered direction (24 B), r read+write (48), new direction (24),
+    // iterate read+write (48) and the 3x3 block inverse (72)
+    *bytes = (double)S.n_blocks * (9.0 * (fp32 ? 4.0 : 8.0) + 4.0) + 4.0 * (n + 1) + 216.0 * n;
+    return ms;
+}
+
 int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
                   double cell0, const double* b, double* x, const PcgOptions& opt, cudaStream_t s,
                   int64_t* launches, long long* iters, double* relres, AmgStats* st) {

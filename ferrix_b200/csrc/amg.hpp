@@ -84,6 +84,12 @@ class Amg {
 };
 
 // CG on the FP64 BSR3 system preconditioned by one V-cycle per iteration.
+// CUDA-event time (ms per launch) of the fused fine-level Chebyshev step (SpMV +
+// smoother update) on the given FP64 system, with FP32 values when fp32; bytes =
+// compulsory traffic of one launch.
+double profile_smoother_op(const BsrStructure& S, const double* vals64, const double* dinv64, bool fp32, int reps,
+                           cudaStream_t s, double* bytes);
+
 class AmgPcg {
    public:
     int solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz, double cell0,

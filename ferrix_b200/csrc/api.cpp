@@ -396,6 +396,30 @@ int fx_profile_spmv(fx_model* m, int precision, int reps, double* ms, double* by
     });
 }
 
+int fx_profile_smoother(fx_model* m, int precision, int reps, double* ms, double* bytes) {
+    if (!m || !m->ctx || !ms || !bytes || reps <= 0 || !m->state_ready) return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        int64_t* saved = g_launch_counter;
+        g_launch_counter = &m->ctx->launches;
+        struct R {
+            int64_t* v;
+            ~R() { g_launch_counter = v; }
+        } r{saved};
+        ensure_dense(m);
+        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        ensure_structure(m);
+        ModelDev& d = m->dev;
+        cudaStream_t s = m->ctx->stream;
+        assemble(m, nullptr, true);
+        DBuf<double> minv;
+        minv.alloc((size_t)m->dense.n_nodes * 9, s);
+        launch_block_jacobi<double>(d.S, d.vals64.ptr, minv.ptr, s);
+        *ms = profile_smoother_op(d.S, d.vals64.ptr, minv.ptr, precision == FX_PREC_MIXED, reps, s, bytes);
+        return FX_OK;
+    });
+}
+
 int fx_batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts* opts, int* status,
                    fx_step_stats* stats) {
     if (!ctx || (!models && n)) return FX_INVALID_ARGUMENT;

@@ -185,6 +185,15 @@ int fx_model_drop_cache(fx_model* model);
  * two gathered vectors + the two written vectors, padding excluded). */
 int fx_profile_spmv(fx_model* model, int precision, int reps, double* ms, double* bytes);
 
+/* Same measurement for the multigrid preconditioner's fine-level operator: one
+ * fused Chebyshev smoothing step (BSR3 SpMV with FP64 vectors, then the
+ * row-local residual / 3x3 block-Jacobi / direction / iterate update), FP32
+ * matrix values when precision is FX_PREC_MIXED, FP64 otherwise; *bytes =
+ * compulsory traffic (values + column indices once, row offsets, 216 B per node
+ * of vector and block-inverse traffic). No reference counterpart: measurement
+ * support for the FX_PRECOND_AMG path. */
+int fx_profile_smoother(fx_model* model, int precision, int reps, double* ms, double* bytes);
+
 /* ---- batched decks ---------------------------------------------------- */
 /* Runs the first step of every model (each fx_state_initialize'd) with all
  * linear solves of the batch advanced together; per-model status in status[]. */
