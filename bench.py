@@ -137,6 +137,30 @@ def run_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _serve_summary(res):
+    return {k: res[k] for k in ("rate_per_s", "requests", "completed", "slots", "p50_ms", "p99_ms", "mean_ms",
+                                "solves_per_s", "mean_dofs")}
+
+
+def run_serve(args, rank: int, local: int) -> None:
+    """--mode serve: Poisson request streams through the request loop, mixed multigrid vs plain FP64 PCG."""
+    if rank != 0:
+        return
+    import ferrix_b200 as fx
+    from ferrix_b200 import serving
+    pool = serving.make_pool()
+    rates = [float(r) for r in args.rates.split(",")]
+    out = {"mode": "serve", "metric": "serving p50/p99 latency (ms) and solves/s at 1e-8",
+           "pool": "16 seeded boxes, 60% C3D4 / 40% C3D20, DOF log-uniform [5k, 500k]", "arms": {}}
+    arms = (("mixed_amg", fx.solve_opts(precision=fx.PREC_MIXED, preconditioner=fx.PRECOND_AMG), rates),
+            ("plain_fp64_csr_jacobi", fx.solve_opts(precision=fx.PREC_FP64_CSR), rates[:2]))
+    for name, o, rs in arms:
+        out["arms"][name] = [_serve_summary(serving.run_stream(pool, r, args.requests, o, device=local,
+                                                               slots=args.slots, seed=int(r)))
+                             for r in rs]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -147,7 +171,10 @@ def main():
     ap.add_argument("--preconditioner", default="amg", choices=["amg", "bj"])
     ap.add_argument("--no-oracle", action="store_true", help="skip the CPU oracle (accuracy / cpu_baseline)")
     ap.add_argument("--no-arms", action="store_true", help="skip the comparison arms")
-    ap.add_argument("--mode", default="solve", choices=["solve", "spmv"],
+    ap.add_argument("--rates", default="10,25,50,100,500", help="serve mode: arrival rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=48, help="serve mode: requests per rate")
+    ap.add_argument("--slots", type=int, default=4, help="serve mode: concurrent requests on the GPU")
+    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "serve"],
                     help="spmv: only assemble and time REPS standalone SpMV launches (profiling case)")
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
@@ -156,6 +183,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.mode == "serve":
+        return run_serve(args, rank, local)
     if args.mode == "spmv":
         import ferrix_b200 as fx
         ctx = fx.Context(local)
@@ -300,6 +329,16 @@ def main():
             except fx.FerrixError as e:
                 arms[name] = {"error": str(e)}
 
+    serving_line = None
+    if rank == 0 and not args.no_arms:
+        from ferrix_b200 import serving
+        pool = serving.make_pool()
+        res = serving.run_stream(pool, 25.0, 32, fx.solve_opts(precision=fx.PREC_MIXED, preconditioner=fx.PRECOND_AMG),
+                                 device=local, slots=4, seed=25)
+        serving_line = _serve_summary(res)
+        serving_line["solver"] = "mixed multigrid CG"
+        serving_line["pool"] = "16 seeded boxes, 60% C3D4 / 40% C3D20, DOF log-uniform [5k, 500k]"
+
     cpu = None
     rel_err = None
     if oracle_p is not None:
@@ -378,6 +417,7 @@ def main():
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "ms_per_step": e2e_elapsed * 1e3 if e2e_elapsed else None},
             "cpu_baseline": cpu,
+            "serving": serving_line,
         }
         print(json.dumps(line), flush=True)
     project.close()

@@ -31,7 +31,7 @@ from . import _lib
 from ._lib import PRECOND_AMG, PRECOND_BLOCK_JACOBI, PREC_FP64, PREC_FP64_CSR, PREC_MIXED, SolveOpts, StepStats
 
 __all__ = ["Context", "Project", "SolutionState", "SolverTime", "FerrixError", "SolveOptions", "solve_opts",
-           "batch_solve", "StepStats", "PREC_MIXED", "PREC_FP64", "PREC_FP64_CSR", "PRECOND_AMG",
+           "batch_solve", "Server", "StepStats", "PREC_MIXED", "PREC_FP64", "PREC_FP64_CSR", "PRECOND_AMG",
            "PRECOND_BLOCK_JACOBI"]
 
 
@@ -353,3 +353,63 @@ def batch_solve(ctx: Context, projects: Sequence[Project], opts: Optional[SolveO
     if rc != 0 and not np.any(st != 0):
         _check(rc, ctx)
     return st, [s.as_dict() for s in stats]
+
+
+class Server:
+    """Request loop with continuous batching on one GPU (fx_server_*).
+
+    Projects are parsed on the host (`Project.from_inp_text(text)` without a
+    context) and submitted; `slots` worker threads admit them by HBM footprint
+    and solve their first step concurrently, each on its own stream. `wait`
+    returns the displacements and the request's timing."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: float = 0.0,
+                 opts: Optional[SolveOpts] = None):
+        self.lib = _lib.load()
+        so = _lib.ServerOpts()
+        self.lib.fx_default_server_opts(C.byref(so))
+        so.device = device
+        so.slots = slots
+        so.hbm_budget_bytes = float(hbm_budget_bytes)
+        if opts is not None:
+            so.opts = opts
+        h = C.c_void_p()
+        _check(self.lib.fx_server_create(C.byref(so), C.byref(h)), None, "fx_server_create")
+        self.handle = h
+        self._pending = {}  # ticket -> project (kept alive while the server uses it)
+
+    def submit(self, project: "Project") -> int:
+        if project.ctx is not None:
+            raise ValueError("submit a host-only project (Project.from_inp_text(text) without a context)")
+        t = C.c_int64()
+        _check(self.lib.fx_server_submit(self.handle, project.handle, C.byref(t)), None, "fx_server_submit")
+        self._pending[t.value] = project
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = -1.0):
+        """(displacements or None, result dict); raises FerrixError(FX_TIMEOUT) when not done in time."""
+        p = self._pending[ticket]
+        u = np.empty(p.num_dofs)
+        res = _lib.RequestResult()
+        res.status = -1  # filled only once the request is done
+        rc = self.lib.fx_server_wait(self.handle, ticket, float(timeout), _p(u), C.byref(res))
+        if res.status == -1:
+            raise FerrixError(rc, "request not finished" if rc == 16 else "fx_server_wait failed")
+        self._pending.pop(ticket, None)
+        out = {"status": res.status, "slot": res.slot, "queue_ms": res.queue_ms, "service_ms": res.service_ms,
+               "latency_ms": res.latency_ms, "footprint_bytes": res.footprint_bytes,
+               "admit_at_ms": res.admit_at_ms, "done_at_ms": res.done_at_ms,
+               "stats": res.stats.as_dict(), "error": res.error.decode(errors="replace")}
+        return (u if res.status == 0 else None), out
+
+    def close(self):
+        if self.handle:
+            self.lib.fx_server_destroy(self.handle)
+            self.handle = None
+            self._pending.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -44,6 +44,17 @@ class StepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("slots", C.c_int), ("hbm_budget_bytes", C.c_double), ("opts", SolveOpts)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("slot", C.c_int), ("queue_ms", C.c_double), ("service_ms", C.c_double),
+                ("latency_ms", C.c_double), ("footprint_bytes", C.c_double), ("admit_at_ms", C.c_double),
+                ("done_at_ms", C.c_double), ("stats", StepStats),
+                ("error", C.c_char * 256)]
+
+
 # name -> (restype, argtypes); every symbol of include/ferrix_b200.h
 P = C.c_void_p
 I64P = C.POINTER(C.c_int64)
@@ -77,6 +88,11 @@ SIGNATURES = {
     "fx_profile_spmv": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_profile_smoother": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_batch_solve": (C.c_int, [P, P, C.c_int, C.POINTER(SolveOpts), P, P]),
+    "fx_default_server_opts": (None, [C.POINTER(ServerOpts)]),
+    "fx_server_create": (C.c_int, [C.POINTER(ServerOpts), P]),
+    "fx_server_submit": (C.c_int, [P, P, C.POINTER(C.c_int64)]),
+    "fx_server_wait": (C.c_int, [P, C.c_int64, C.c_double, P, C.POINTER(RequestResult)]),
+    "fx_server_destroy": (None, [P]),
     "fx_spmv_dot_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, P, P, P, P]),
 }
 

@@ -894,7 +894,7 @@ __global__ void k_f64_to_f32(int64_t n, const double* __restrict__ a, float* __r
 
 // Grid of the level-0 operators: at most one wave of resident CTAs (grid-stride rows).
 static unsigned l0_grid(int n) {
-    static int cached_dev = -1, cached_cap = 0;
+    thread_local int cached_dev = -1, cached_cap = 0;  // per host thread: contexts live on one thread each
     int dev = 0;
     FX_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev != cached_dev) {

@@ -200,6 +200,50 @@ int fx_profile_smoother(fx_model* model, int precision, int reps, double* ms, do
 int fx_batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts* opts, int* status,
                    fx_step_stats* stats);
 
+/* ---- request loop (continuous batching) ---------------------------------
+ * No reference counterpart (FerriX solves one deck per process, src/main.rs:49-64).
+ * The server runs `slots` worker threads on one GPU, each with its own context
+ * and stream. Submitted models wait in a FIFO queue; a free slot admits the head
+ * request when the summed device-footprint estimate of the running requests
+ * plus its own fits the HBM budget (a request larger than the budget runs
+ * alone). An admitted model is bound to the slot's context, its first *STATIC
+ * step is solved (fx_step_solve semantics, the server's solve options), the
+ * displacements are copied to host memory and all of its device memory is
+ * released again. Requests on different slots overlap on the device; each
+ * result is the same as when the model is solved alone. */
+typedef struct {
+    int device;
+    int slots;               /* concurrent requests (worker threads, one stream each), 1..64 */
+    double hbm_budget_bytes; /* admission budget for the summed footprint estimates; 0 = 70% of free memory */
+    fx_solve_opts opts;      /* solve options of every request */
+} fx_server_opts;
+
+typedef struct {
+    int status;             /* fx_status of the request */
+    int slot;               /* worker that ran it */
+    double queue_ms;        /* submit -> admission */
+    double service_ms;      /* admission -> displacements on the host */
+    double latency_ms;      /* submit -> displacements on the host */
+    double footprint_bytes; /* admission estimate */
+    double admit_at_ms;     /* admission time, ms since fx_server_create */
+    double done_at_ms;      /* completion time, ms since fx_server_create */
+    fx_step_stats stats;    /* of the solved step */
+    char error[256];        /* message when status != FX_OK */
+} fx_request_result;
+
+void fx_default_server_opts(fx_server_opts* opts);
+int fx_server_create(const fx_server_opts* opts, fx_server** out);
+/* `model` must come from fx_model_from_inp with ctx NULL and must stay alive,
+ * unused by the caller, until fx_server_wait has returned its result. */
+int fx_server_submit(fx_server* server, fx_model* model, int64_t* ticket);
+/* Waits up to timeout_s (< 0: no limit) for the request; FX_TIMEOUT if it is
+ * not done yet (the ticket stays valid). Otherwise copies the displacements
+ * (3 * nodes doubles, node-id order; u may be NULL), fills *result, releases
+ * the ticket and returns the request's status. */
+int fx_server_wait(fx_server* server, int64_t ticket, double timeout_s, double* u, fx_request_result* result);
+/* Finishes the running requests, cancels the queued ones, joins the workers. */
+void fx_server_destroy(fx_server* server);
+
 /* ---- allocation-free SpMV with fused dot -------------------------------
  * No counterpart in the reference. y = A x and *dot = x . y for an FP64 CSR
  * matrix of n rows, all pointers on `device`, work queued on `stream`

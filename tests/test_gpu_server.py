@@ -1,0 +1,87 @@
+"""Request loop (fx_server_*): results alone vs in the mix, admission by HBM
+footprint, and agreement with the oracle's direct solve.
+
+Tolerance: displacement 1e-8 relative (2-norm) against the oracle; results of
+the same deck alone and in the mix are compared bit for bit (each request runs
+the same launch sequence on its own stream)."""
+import numpy as np
+import pytest
+
+import ferrix_b200 as fx
+from ferrix_b200 import decks
+from oracle import inp, static_step
+
+pytestmark = pytest.mark.gpu
+
+
+def _pool():
+    # mixed C3D4 / C3D20 boxes of uneven size (1.5k - 40k DOF)
+    return [text for text, _ in decks.batch_population(8, seed=5, dof_lo=1500, dof_hi=40000, c3d20_fraction=0.4)]
+
+
+def _host_project(text):
+    p = fx.Project.from_inp_text(text)
+    p.default_initial_temperature = 20.0
+    return p
+
+
+def _serve(texts, slots, budget=0.0, opts=None):
+    srv = fx.Server(0, slots=slots, hbm_budget_bytes=budget, opts=opts)
+    try:
+        projs = [_host_project(t) for t in texts]
+        tickets = [srv.submit(p) for p in projs]
+        out = [srv.wait(t, timeout=600.0) for t in tickets]
+    finally:
+        srv.close()
+    for p in projs:
+        p.close()
+    return out
+
+
+@pytest.mark.parametrize("preconditioner", [fx.PRECOND_BLOCK_JACOBI, fx.PRECOND_AMG])
+def test_results_same_alone_and_in_the_mix(preconditioner):
+    texts = _pool()
+    # residual tolerance 1e-10 so that the displacement error stays below 1e-8 also on the
+    # thin, badly conditioned boxes of the pool
+    opts = fx.solve_opts(precision=fx.PREC_MIXED, preconditioner=preconditioner, rtol=1e-10)
+    alone = [_serve([t], 1, opts=opts)[0] for t in texts]
+    mixed = _serve(texts, 4, opts=opts)
+    for (ua, ra), (um, rm) in zip(alone, mixed):
+        assert ra["status"] == 0 and rm["status"] == 0, (ra["error"], rm["error"])
+        assert np.array_equal(ua, um)
+    # the mix overlapped on the device: some admission happened before an earlier request finished
+    spans = sorted((r["admit_at_ms"], r["done_at_ms"]) for _, r in mixed)
+    assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+    for text, (u, _) in list(zip(texts, mixed))[:3]:
+        o = inp.parse_inp_text(text)
+        o.default_initial_temperature = 20.0
+        ref = static_step.Runner(o).run().displacements
+        assert np.linalg.norm(u - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
+def test_admission_by_footprint_serialises_when_budget_is_small():
+    texts = _pool()[:4]
+    out = _serve(texts, 4, budget=1.0)  # every request exceeds the budget: each runs alone
+    spans = sorted((r["admit_at_ms"], r["done_at_ms"]) for _, r in out)
+    for i in range(len(spans) - 1):
+        assert spans[i + 1][0] >= spans[i][1]
+    assert all(r["status"] == 0 for _, r in out)
+    assert all(r["footprint_bytes"] > 1.0 for _, r in out)
+
+
+def test_failed_request_reports_its_error_and_the_loop_continues():
+    # parses, but its elements have no section (no material): fails at solve time
+    bad = decks.c3d4_cantilever(2, 2, 2).replace("*Solid section, Elset=Vol, Material=Mat", "**", 1)
+    good = decks.c3d4_cantilever(2, 2, 4)
+    srv = fx.Server(0, slots=2)
+    try:
+        pb = _host_project(bad)
+        pg = _host_project(good)
+        tb = srv.submit(pb)
+        tg = srv.submit(pg)
+        u, r = srv.wait(tb, timeout=120.0)
+        assert u is None and r["status"] == 13 and "material" in r["error"].lower()
+        u, r = srv.wait(tg, timeout=120.0)
+        assert r["status"] == 0 and np.all(np.isfinite(u))
+    finally:
+        srv.close()
