@@ -161,6 +161,95 @@ def run_serve(args, rank: int, local: int) -> None:
     print(json.dumps(out), flush=True)
 
 
+def run_batch(args, rank: int, local: int) -> None:
+    """--mode batch: many independent C3D4 decks (DOF log-uniform [2k, 60k]) solved to 1e-8, solves/s.
+
+    Arms: one fx_batch_solve over all decks (mixed block-Jacobi PCG, all systems in
+    one launch sequence per iteration block), the same decks one after another, and
+    the request loop (4 slots, multigrid) fed with all decks at once."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+    import ferrix_b200 as fx
+    from ferrix_b200 import decks
+    from oracle import inp, static_step
+    t0 = time.perf_counter()
+    pop = decks.batch_population(args.decks, seed=7, dof_lo=2e3, dof_hi=6e4, c3d20_fraction=0.0)
+    gen_s = time.perf_counter() - t0
+    texts = [t for t, _ in pop]
+    dofs = np.array([d for _, d in pop])
+    ctx = fx.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {"mode": "batch", "metric": "batched linear static solves/s (C3D4 decks, mixed precision, 1e-8)",
+           "decks": len(texts), "total_dofs": int(dofs.sum()), "mean_dofs": float(dofs.mean()),
+           "deck_generation_s": gen_s, "arms": {}}
+
+    def projects():
+        ps = [fx.Project.from_inp_text(t, ctx) for t in texts]
+        for p in ps:
+            p.default_initial_temperature = 20.0
+            fx.SolutionState(p.num_dofs, p.num_nodes).initialize(p)
+        return ps
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        w0 = time.perf_counter()
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3, time.perf_counter() - w0
+
+    o_bj = fx.solve_opts(precision=fx.PREC_MIXED, rtol=1e-8)
+    for rep in range(2):  # the first pass also loads kernels and builds graphs
+        ps = projects()
+        (st, stats), dev_s, wall_s = timed(lambda: fx.batch_solve(ctx, ps, o_bj))
+        us = [fx.SolutionState(p.num_dofs, p.num_nodes) for p in ps]
+        u_batch = []
+        for p, s in zip(ps, us):
+            s.project = p
+            u_batch.append(s.displacements)
+        for p in ps:
+            p.close()
+    out["arms"]["fx_batch_solve_mixed_bj"] = {"solves_per_s": len(texts) / dev_s, "device_s": dev_s,
+                                              "wall_s": wall_s, "failed": int(np.sum(st != 0)),
+                                              "pcg_iterations_max": int(max(s["pcg_iterations"] for s in stats))}
+    ps = projects()
+
+    def seq():
+        bad = 0
+        for p in ps:
+            try:
+                p.steps[0].solve(1, p, fx.SolutionState(p.num_dofs, p.num_nodes), opts=o_bj)
+            except fx.FerrixError:
+                bad += 1
+        return bad
+    bad, dev_s, wall_s = timed(seq)
+    for p in ps:
+        p.close()
+    out["arms"]["sequential_mixed_bj"] = {"solves_per_s": len(texts) / dev_s, "device_s": dev_s, "wall_s": wall_s,
+                                          "failed": bad}
+    ctx.close()
+    from ferrix_b200 import serving
+    res = serving.run_stream(texts, 1e6, len(texts), fx.solve_opts(precision=fx.PREC_MIXED,
+                                                                  preconditioner=fx.PRECOND_AMG, rtol=1e-8),
+                             device=local, slots=4, seed=1)
+    out["arms"]["request_loop_mixed_amg_4_slots"] = {"solves_per_s": res["solves_per_s"], "wall_s": res["span_s"],
+                                                     "failed": len(texts) - res["completed"]}
+    # accuracy of the batched result on the first decks against the oracle's direct solve
+    errs = []
+    for k in range(min(4, len(texts))):
+        o = inp.parse_inp_text(texts[k])
+        o.default_initial_temperature = 20.0
+        ref = static_step.Runner(o).run().displacements
+        errs.append(float(np.linalg.norm(u_batch[k] - ref) / np.linalg.norm(ref)))
+    out["rel_err_vs_oracle_first4"] = errs
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -174,7 +263,8 @@ def main():
     ap.add_argument("--rates", default="10,25,50,100,500", help="serve mode: arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=48, help="serve mode: requests per rate")
     ap.add_argument("--slots", type=int, default=4, help="serve mode: concurrent requests on the GPU")
-    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "serve"],
+    ap.add_argument("--decks", type=int, default=256, help="batch mode: number of decks")
+    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "serve", "batch"],
                     help="spmv: only assemble and time REPS standalone SpMV launches (profiling case)")
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
@@ -185,6 +275,8 @@ def main():
         return run_reference(args, rank, world)
     if args.mode == "serve":
         return run_serve(args, rank, local)
+    if args.mode == "batch":
+        return run_batch(args, rank, local)
     if args.mode == "spmv":
         import ferrix_b200 as fx
         ctx = fx.Context(local)

@@ -92,9 +92,9 @@ class Context:
             pass
 
 
-def solve_opts(precision: int = PREC_FP64, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
+def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
                reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
-               reference_iterative: bool = False, preconditioner: int = PRECOND_BLOCK_JACOBI,
+               reference_iterative: bool = False, preconditioner: int = PRECOND_AMG,
                amg_aggregate_nodes: int = 40, amg_smoother_degree: int = 2) -> SolveOpts:
     o = SolveOpts()
     _lib.load().fx_default_solve_opts(C.byref(o))

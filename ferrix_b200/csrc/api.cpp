@@ -57,7 +57,7 @@ extern "C" {
 
 void fx_default_solve_opts(fx_solve_opts* o) {
     if (!o) return;
-    o->precision = FX_PREC_FP64;
+    o->precision = FX_PREC_MIXED;
     o->rtol = 1e-8;
     o->max_iter = 50000;
     o->poll_interval = 32;
@@ -65,7 +65,7 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->use_graphs = 1;
     o->verbose = 0;
     o->reference_iterative = 0;
-    o->preconditioner = FX_PRECOND_BLOCK_JACOBI;
+    o->preconditioner = FX_PRECOND_AMG;
     o->amg_aggregate_nodes = 40;
     o->amg_smoother_degree = 2;
 }

@@ -65,8 +65,9 @@ typedef struct fx_server fx_server;
 
 /* Arithmetic of the PCG that stands in for the reference's FP64 Cholesky. */
 typedef enum {
-    FX_PREC_MIXED = 0, /* FP32 BSR3 SpMV + 3x3 block-Jacobi, FP64 residual replacement and accumulation */
-    FX_PREC_FP64 = 1,  /* FP64 BSR3 SpMV + 3x3 block-Jacobi throughout */
+    FX_PREC_MIXED = 0, /* block-Jacobi: FP32 BSR3 SpMV and preconditioner, FP64 residual replacement and
+                          accumulation; multigrid: FP64 CG, FP32 matrix values in the fine-level smoother */
+    FX_PREC_FP64 = 1,  /* FP64 throughout */
     FX_PREC_FP64_CSR = 2 /* plain FP64 PCG: scalar CSR SpMV + Jacobi (the reference IterativeSolver's algorithm) */
 } fx_precision;
 
@@ -107,6 +108,9 @@ typedef struct {
     double amg_setup_ms;       /* multigrid setup time, summed over the step */
 } fx_step_stats;
 
+/* Defaults: FX_PREC_MIXED, FX_PRECOND_AMG, rtol 1e-8, max_iter 50000, poll 32,
+ * reliable_delta 1e-2, graphs on, 40 nodes per aggregate, Chebyshev degree 2.
+ * fx_solve_csr has no node coordinates and always uses block-Jacobi. */
 void fx_default_solve_opts(fx_solve_opts* opts);
 
 /* ---- context ---------------------------------------------------------- */
