@@ -360,35 +360,6 @@ def main():
         spmv_ms, spmv_bytes = project.profile_spmv(prec if prec != fx.PREC_FP64_CSR else fx.PREC_FP64, 30)
     bj_ms, bj_bytes = project.profile_spmv(fx.PREC_MIXED, 30)
 
-    # e2e through the public API from host text and host buffers
-    h2d = d2h = 0
-    e2e_elapsed = None
-    if rank == 0 or True:
-        def e2e_step():
-            p = fx.Project.from_inp_text(text, ctx)
-            s = fx.SolutionState(p.num_dofs, p.num_nodes)
-            s.initialize(p)
-            p.steps[0].solve(1, p, s, opts=opts)
-            u = s.displacements
-            p.close()
-            return u
-        e2e_step()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        ke = max(1, min(args.steps, 3))
-        for _ in range(ke):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_elapsed = e0.elapsed_time(e1) / 1e3 / ke
-        xyz, groups = project.export()
-        n_el = sum(len(g[1]) for g in groups.values())
-        h2d = (xyz.size * 8 + sum(g[0].size * 4 + g[1].size * 4 for g in groups.values())
-               + 2 * project.num_nodes * 8)
-        d2h = project.num_dofs * 8
-
     arms = {}
     if rank == 0 and not args.no_arms:
         arm_list = (("plain_fp64_csr_jacobi", fx.PREC_FP64_CSR, fx.PRECOND_BLOCK_JACOBI),
@@ -421,16 +392,6 @@ def main():
             except fx.FerrixError as e:
                 arms[name] = {"error": str(e)}
 
-    serving_line = None
-    if rank == 0 and not args.no_arms:
-        from ferrix_b200 import serving
-        pool = serving.make_pool()
-        res = serving.run_stream(pool, 25.0, 32, fx.solve_opts(precision=fx.PREC_MIXED, preconditioner=fx.PRECOND_AMG),
-                                 device=local, slots=4, seed=25)
-        serving_line = _serve_summary(res)
-        serving_line["solver"] = "mixed multigrid CG"
-        serving_line["pool"] = "16 seeded boxes, 60% C3D4 / 40% C3D20, DOF log-uniform [5k, 500k]"
-
     cpu = None
     rel_err = None
     if oracle_p is not None:
@@ -451,6 +412,47 @@ def main():
             pass
     for a in arms.values():
         a.pop("u", None)
+
+    # host-side measurements after the oracle process has finished with the host cores
+    # e2e through the public API from host text and host buffers
+    h2d = d2h = 0
+    e2e_elapsed = None
+    if rank == 0 or True:
+        def e2e_step():
+            p = fx.Project.from_inp_text(text, ctx)
+            s = fx.SolutionState(p.num_dofs, p.num_nodes)
+            s.initialize(p)
+            p.steps[0].solve(1, p, s, opts=opts)
+            u = s.displacements
+            p.close()
+            return u
+        e2e_step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ke = max(1, min(args.steps, 3))
+        for _ in range(ke):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_elapsed = e0.elapsed_time(e1) / 1e3 / ke
+        xyz, groups = project.export()
+        n_el = sum(len(g[1]) for g in groups.values())
+        h2d = (xyz.size * 8 + sum(g[0].size * 4 + g[1].size * 4 for g in groups.values())
+               + 2 * project.num_nodes * 8)
+        d2h = project.num_dofs * 8
+
+    serving_line = None
+    if rank == 0 and not args.no_arms:
+        from ferrix_b200 import serving
+        pool = serving.make_pool()
+        res = serving.run_stream(pool, 25.0, 32, fx.solve_opts(precision=fx.PREC_MIXED, preconditioner=fx.PRECOND_AMG),
+                                 device=local, slots=4, seed=25)
+        serving_line = _serve_summary(res)
+        serving_line["solver"] = "mixed multigrid CG"
+        serving_line["pool"] = "16 seeded boxes, 60% C3D4 / 40% C3D20, DOF log-uniform [5k, 500k]"
+
 
     if rank == 0:
         import json as _j
