@@ -156,13 +156,6 @@ struct FineView {
         int k = (int)(b - row_ptr[i]);
         return cols4[4 * (int64_t)goff[i] + k];
     }
-    __device__ __forceinline__ double val(int64_t b, int i, int r, int c) const {
-        if (bs == 6) return vals[b * 36 + r * 6 + c];
-        int k = (int)(b - row_ptr[i]);
-        int64_t g0 = goff[i];
-        int ng = goff[i + 1] - (int)g0;
-        return vals[(g0 * 9 + (int64_t)(3 * r + c) * ng + k / 4) * 4 + (k & 3)];
-    }
     template <int BS>
     __device__ __forceinline__ void load(int64_t b, int i, double* v) const {
         if (BS == 6) {
@@ -375,28 +368,6 @@ __global__ void k_cheb_init(int n, int bs, const double* __restrict__ dinv, cons
     }
 }
 
-// Chebyshev step: r -= t; d = c1 d + c2 D^-1 r; x += d
-__global__ void k_cheb_step(int n, int bs, const double* __restrict__ dinv, double* __restrict__ r,
-                            const double* __restrict__ t, double* __restrict__ d, double* __restrict__ x, double c1,
-                            double c2) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t o = (int64_t)i * bs;
-    double rr[6];
-    for (int k = 0; k < bs; ++k) {
-        rr[k] = r[o + k] - t[o + k];
-        r[o + k] = rr[k];
-    }
-    const double* Di = dinv + (int64_t)i * bs * bs;
-    for (int k = 0; k < bs; ++k) {
-        double z = 0.0;
-        for (int c = 0; c < bs; ++c) z += Di[k * bs + c] * rr[c];
-        double dn = c1 * d[o + k] + c2 * z;
-        d[o + k] = dn;
-        x[o + k] += dn;
-    }
-}
-
 // bc = Q^T rf per aggregate: one warp per aggregate, lanes over member rows
 __global__ void k_restrict(int na, const int32_t* __restrict__ ptr, const int32_t* __restrict__ nodes, int bs,
                            const double* __restrict__ Q, const double* __restrict__ rf, double* __restrict__ bc) {
@@ -599,10 +570,6 @@ __global__ void k_fill_hash(int64_t n, double* __restrict__ v) {
     v[i] = (double)(h & 0xFFFFF) / 1048576.0 + 0.5;
 }
 
-__global__ void k_scale(int64_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) y[i] = a * x[i];
-}
 
 unsigned grid_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
@@ -686,6 +653,7 @@ struct L0Op {
     const double* dinv;
     double c1, c2;
     int dot;
+    const double* zold;  // dot = 2 with a flexible outer CG: the previous preconditioned residual
     double* part;
     int* counter;
     double* S;
@@ -707,28 +675,43 @@ __device__ __forceinline__ void ld4v(const double* p, double o[4]) {
     o[3] = b.y;
 }
 
-// Fixed-order CTA sum, then the last CTA to arrive reduces all CTA partials and
-// finalises the outer CG scalars.
-__device__ __forceinline__ void cta_dot_finalize(double v, int mode, double* part, int* counter, double* S) {
-    __shared__ double sh[32];
+// Fixed-order CTA sums of (v, v2), then the last CTA to arrive reduces all CTA
+// partials and finalises the outer CG scalars: mode 1 alpha = r.z / p.q; mode 2
+// beta = (r.z_new - r.z_old) / r.z_prev (Polak-Ribiere, flexible CG; v2 = 0 for
+// the plain form) and r.z.
+__device__ __forceinline__ void cta_dot_finalize(double v, double v2, int mode, double* part, int* counter,
+                                                 double* S) {
+    __shared__ double sh[2][32];
     __shared__ int s_last;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     v = warp_sum(v);
-    if (lane == 0) sh[w] = v;
+    v2 = warp_sum(v2);
+    if (lane == 0) {
+        sh[0][w] = v;
+        sh[1][w] = v2;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int k = 0; k < nw; ++k) t += sh[k];
-        part[blockIdx.x] = t;
+        double t = 0.0, t2 = 0.0;
+        for (int k = 0; k < nw; ++k) {
+            t += sh[0][k];
+            t2 += sh[1][k];
+        }
+        part[2 * blockIdx.x] = t;
+        part[2 * blockIdx.x + 1] = t2;
         __threadfence();
         s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
     }
     __syncthreads();
     if (!s_last || w != 0) return;
     __threadfence();
-    double t = 0.0;
-    for (int k = lane; k < (int)gridDim.x; k += 32) t += __ldcg(part + k);
+    double t = 0.0, t2 = 0.0;
+    for (int k = lane; k < (int)gridDim.x; k += 32) {
+        t += __ldcg(part + 2 * k);
+        t2 += __ldcg(part + 2 * k + 1);
+    }
     t = warp_sum(t);
+    t2 = warp_sum(t2);
     if (lane != 0) return;
     *counter = 0;
     if (mode == 1) {  // p.q -> alpha
@@ -740,12 +723,15 @@ __device__ __forceinline__ void cta_dot_finalize(double v, int mode, double* par
             S[5] = S[0] / t;
         }
     } else {  // new r.z -> beta
-        S[4] = S[0] > 0.0 ? t / S[0] : 0.0;
+        S[4] = S[0] > 0.0 ? (t - t2) / S[0] : 0.0;
         S[0] = t;
     }
 }
 
-constexpr int kL0MinBlocks = 4;  // 256-thread CTAs resident per SM (caps registers at 64)
+#ifndef FX_L0_MIN_BLOCKS
+#define FX_L0_MIN_BLOCKS 3
+#endif
+constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per SM (3: at most 85 registers)
 
 template <typename VT, int MODE>
 __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
@@ -754,12 +740,37 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
     const int rows_per_grid = (gridDim.x * blockDim.x) >> 3;
     const int nb = ((o.n + 3) / 4) * 4;  // uniform trip count per warp (4 rows per warp)
     const double* __restrict__ v = o.v;
-    double dsum = 0.0;
+    double dsum = 0.0, dsum2 = 0.0;
     for (int base = row0 - (row0 & 3); base < nb; base += rows_per_grid) {
         const int row = base + (row0 & 3);
         const bool valid = row < o.n;
         const int g0 = valid ? o.goff[row] : 0;
         const int ng = valid ? o.goff[row + 1] - g0 : 0;
+        // row-local operands of the epilogue, loaded before the gathers so that their latency overlaps
+        const int64_t o3 = 3 * (int64_t)row;
+        const int c = sub < 3 ? sub : 0;
+        const bool epi = valid && sub < 3;
+        double src3[3] = {0.0, 0.0, 0.0}, Dr[3] = {0.0, 0.0, 0.0}, vc = 0.0, xoc = 0.0, bc = 0.0, zoc = 0.0;
+        if (epi) {
+            if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
+                const double* src = MODE == kL0Cheb0 ? o.b : o.r;
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk) {
+                    src3[kk] = src[o3 + kk];
+                    Dr[kk] = o.dinv[9 * (int64_t)row + 3 * c + kk];
+                }
+                vc = v[o3 + c];
+                if (MODE == kL0ChebK) xoc = o.xo[o3 + c];
+                if (o.dot) bc = o.b[o3 + c];
+                if (o.dot && o.zold) zoc = o.zold[o3 + c];
+            } else if (MODE == kL0Apply) {
+                vc = v[o3 + c];
+            } else if (MODE == kL0Resid) {
+                bc = o.b ? o.b[o3 + c] : 0.0;
+            } else {
+                src3[0] = o.r[o3 + c];
+            }
+        }
         double acc[3] = {0.0, 0.0, 0.0};
         for (int g = sub; g < ng; g += 8) {
             const int4 cc = __ldg(reinterpret_cast<const int4*>(o.cols) + g0 + g);
@@ -789,39 +800,196 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
 #pragma unroll
             for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], s);
         // epilogue: lane c of the row's 8 handles component c
-        const int64_t o3 = 3 * (int64_t)row;
-        const int c = sub < 3 ? sub : 0;
         const double axc = c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]);
-        double rr[3] = {0.0, 0.0, 0.0};
-        if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
-            if (valid && sub < 3) {
-                const double* src = MODE == kL0Cheb0 ? o.b : o.r;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) rr[k] = src[o3 + k] - acc[k];
-            }
-            __syncwarp();  // every lane has read r before lane c overwrites r[c]
-        }
-        if (!valid || sub >= 3) continue;
+        __syncwarp();  // every lane's reads of r (above) are ordered before any lane writes r[c]
+        if (!epi) continue;
         if (MODE == kL0Resid) {
-            o.y[o3 + c] = o.b ? o.b[o3 + c] - axc : axc;
+            o.y[o3 + c] = o.b ? bc - axc : axc;
         } else if (MODE == kL0RUpd) {
-            o.r[o3 + c] -= axc;
+            o.r[o3 + c] = src3[0] - axc;
         } else if (MODE == kL0Apply) {
             o.y[o3 + c] = axc;
-            dsum += v[o3 + c] * axc;
+            dsum += vc * axc;
         } else {  // Chebyshev steps
-            const double* D = o.dinv + 9 * (int64_t)row + 3 * c;
-            const double z = D[0] * rr[0] + D[1] * rr[1] + D[2] * rr[2];
-            const double rc = c == 0 ? rr[0] : (c == 1 ? rr[1] : rr[2]);
-            o.r[o3 + c] = rc;
-            const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * v[o3 + c]) + o.c2 * z;
+            const double rr[3] = {src3[0] - acc[0], src3[1] - acc[1], src3[2] - acc[2]};
+            const double z = Dr[0] * rr[0] + Dr[1] * rr[1] + Dr[2] * rr[2];
+            o.r[o3 + c] = c == 0 ? rr[0] : (c == 1 ? rr[1] : rr[2]);
+            const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * vc) + o.c2 * z;
             o.d_out[o3 + c] = dn;
-            const double xn = (MODE == kL0Cheb0 ? v[o3 + c] : o.xo[o3 + c]) + dn;
+            const double xn = (MODE == kL0Cheb0 ? vc : xoc) + dn;
             o.xo[o3 + c] = xn;
-            if (o.dot) dsum += o.b[o3 + c] * xn;
+            if (o.dot) {
+                dsum += bc * xn;
+                dsum2 += bc * zoc;
+            }
         }
     }
-    if (o.dot) cta_dot_finalize(dsum, o.dot, o.part, o.counter, o.S);
+    if (o.dot) cta_dot_finalize(dsum, dsum2, o.dot, o.part, o.counter, o.S);
+}
+
+// ---- K-cycle on a coarse level (one CTA; the level has at most a few 10k DOF)
+// Two steps of a flexible CG for A x = b preconditioned by the next cycle:
+//   z1 = B(b), v1 = A z1, alpha1 = z1.b / z1.v1, x = alpha1 z1, r = b - alpha1 v1;
+//   z2 = B(r), v2 = A z2, w = z2 - (z2.v1 / z1.v1) z1, x += (w.r / w.Aw) w.
+template <int NV>
+__device__ __forceinline__ void block_sums(double (&v)[NV], double* sh /* [NV][32] */) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k * 32 + w] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {  // every thread sums in the same fixed order
+        double t = 0.0;
+        for (int j = 0; j < nw; ++j) t += sh[k * 32 + j];
+        v[k] = t;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(1024) k_kcycle1(int64_t n, const double* __restrict__ b,
+                                                  const double* __restrict__ z1, const double* __restrict__ v1,
+                                                  double* __restrict__ x, double* __restrict__ r,
+                                                  double* __restrict__ kc) {
+    __shared__ double sh[2 * 32];
+    double s[2] = {0.0, 0.0};
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        s[0] += z1[i] * b[i];
+        s[1] += z1[i] * v1[i];
+    }
+    block_sums<2>(s, sh);
+    const double sigma = s[1];
+    const double alpha = sigma > 0.0 && isfinite(sigma) ? s[0] / sigma : 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        x[i] = alpha * z1[i];
+        r[i] = b[i] - alpha * v1[i];
+    }
+    if (threadIdx.x == 0) kc[0] = sigma;
+}
+
+__global__ void __launch_bounds__(1024) k_kcycle2(int64_t n, const double* __restrict__ z1,
+                                                  const double* __restrict__ v1, const double* __restrict__ z2,
+                                                  const double* __restrict__ v2, const double* __restrict__ r,
+                                                  double* __restrict__ x, const double* __restrict__ kc) {
+    __shared__ double sh[2 * 32];
+    const double sigma = kc[0];
+    double g[1] = {0.0};
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) g[0] += z2[i] * v1[i];
+    block_sums<1>(g, sh);
+    const double beta = sigma > 0.0 && isfinite(sigma) ? g[0] / sigma : 0.0;
+    double s[2] = {0.0, 0.0};
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double w = z2[i] - beta * z1[i];
+        const double aw = v2[i] - beta * v1[i];
+        s[0] += w * r[i];
+        s[1] += w * aw;
+    }
+    block_sums<2>(s, sh);
+    const double alpha = s[1] > 0.0 && isfinite(s[1]) ? s[0] / s[1] : 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] += alpha * (z2[i] - beta * z1[i]);
+}
+
+// ---- coarse levels (row-major 6x6 block CSR): SpMV fused with the smoother
+// update, one warp per block row, lanes over the row's blocks; the same modes as
+// the fine-level operator (kL0Resid, kL0RUpd, kL0Cheb0, kL0ChebK).
+struct LnOp {
+    int n;
+    const int32_t* row_ptr;
+    const int32_t* cols;
+    const double* vals;
+    const double* v;
+    const double* b;
+    double* y;
+    double* r;
+    double* d_out;
+    double* xo;
+    const double* dinv;  // 6x6 block inverses
+    double c1, c2;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_ln_op(LnOp o) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= o.n) return;  // warp-uniform
+    const int64_t o6 = 6 * (int64_t)row;
+    const int c = lane < 6 ? lane : 0;
+    const bool epi = lane < 6;
+    double src6[6] = {0, 0, 0, 0, 0, 0}, Dr[6] = {0, 0, 0, 0, 0, 0}, vc = 0.0, xoc = 0.0, bc = 0.0;
+    if (epi) {  // row-local operands, loaded before the gathers
+        if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
+            const double* src = MODE == kL0Cheb0 ? o.b : o.r;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                src6[k] = src[o6 + k];
+                Dr[k] = o.dinv[36 * (int64_t)row + 6 * c + k];
+            }
+            vc = o.v[o6 + c];
+            if (MODE == kL0ChebK) xoc = o.xo[o6 + c];
+        } else if (MODE == kL0Resid) {
+            bc = o.b ? o.b[o6 + c] : 0.0;
+        } else {
+            src6[0] = o.r[o6 + c];
+        }
+    }
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int blk = o.row_ptr[row] + lane; blk < o.row_ptr[row + 1]; blk += 32) {
+        const double* vb = o.vals + (int64_t)blk * 36;
+        const double* xx = o.v + 6 * (int64_t)o.cols[blk];
+        double xv[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) xv[k] = xx[k];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+            double t = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) t += vb[r * 6 + k] * xv[k];
+            acc[r] += t;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) acc[r] = warp_sum(acc[r]);
+    double axc = acc[0];
+#pragma unroll
+    for (int r = 1; r < 6; ++r)
+        if (c == r) axc = acc[r];
+    __syncwarp();  // every lane's reads of r are ordered before any lane writes r[c]
+    if (!epi) return;
+    if (MODE == kL0Resid) {
+        o.y[o6 + c] = o.b ? bc - axc : axc;
+    } else if (MODE == kL0RUpd) {
+        o.r[o6 + c] = src6[0] - axc;
+    } else {
+        double z = 0.0, rc = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const double rk = src6[k] - acc[k];
+            z += Dr[k] * rk;
+            if (k == c) rc = rk;
+        }
+        o.r[o6 + c] = rc;
+        const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * vc) + o.c2 * z;
+        o.d_out[o6 + c] = dn;
+        o.xo[o6 + c] = (MODE == kL0Cheb0 ? vc : xoc) + dn;
+    }
+}
+
+// first smoothing step from x = 0 at any level: d = c2 D^-1 b; x = d; r = b
+__global__ void k_cheb_start(int n, int bs, const double* __restrict__ dinv, const double* __restrict__ b,
+                             double* __restrict__ r, double* __restrict__ d, double* __restrict__ x, double c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t o = (int64_t)i * bs;
+    const double* Di = dinv + (int64_t)i * bs * bs;
+    for (int k = 0; k < bs; ++k) {
+        double t = 0.0;
+        for (int j = 0; j < bs; ++j) t += Di[k * bs + j] * b[o + j];
+        t *= c2;
+        d[o + k] = t;
+        x[o + k] = t;
+    }
+    for (int k = 0; k < bs; ++k) r[o + k] = b[o + k];
 }
 
 // first pre-smoothing step from x = 0: d = c2 D^-1 b; x = d; r = b
@@ -990,6 +1158,7 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         AmgLevel& l = L[lev];
         const int64_t nd = (int64_t)l.n * l.bs;
         for (DBuf<double>* v : {&l.x, &l.b, &l.r, &l.d, &l.t}) v->alloc(nd, s);
+        if (lev > 0) l.xs.alloc(nd, s);
         if (lev > 0) {
             l.dinv.alloc((size_t)l.n * 36, s);
             FX_LAUNCH(k_block_inv6, grid_for(l.n, 128), 128, 0, s, l.n, l.row_ptr.ptr, l.cols.ptr, l.vals.ptr,
@@ -1131,6 +1300,13 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         Rprev = std::move(Rnext);
         cell *= 2.0;
     }
+    if (L.size() > 2) {  // K-cycle work vectors on the first coarse level
+        AmgLevel& l1 = L[1];
+        const int64_t nd1 = (int64_t)l1.n * l1.bs;
+        for (auto& v : l1.kc) v.alloc(nd1, s);
+        l1.kcs.alloc(8, s);
+        l1.kcs.zero(s);
+    }
     if (st) {
         st->levels = (int)L.size();
         st->sizes.clear();
@@ -1163,36 +1339,94 @@ static ChebCoef cheb_coef(double lmax, int degree) {
     return k;
 }
 
-// coarse levels (6x6 blocks): separate SpMV and update kernels
-static void smooth(AmgLevel& l, bool zero_x, int degree, cudaStream_t s) {
-    const ChebCoef k = cheb_coef(l.lmax, degree);
-    const int64_t nd = (int64_t)l.n * l.bs;
-    if (zero_x) FX_CUDA_CHECK(cudaMemcpyAsync(l.r.ptr, l.b.ptr, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    else level_spmv(l, l.x.ptr, l.b.ptr, l.r.ptr, s);  // r = b - A x
-    FX_LAUNCH(k_cheb_init, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.r.ptr, l.d.ptr, l.x.ptr, k.c2_start,
-              zero_x ? 1 : 0);
-    for (int st = 1; st < degree; ++st) {
-        level_spmv(l, l.d.ptr, nullptr, l.t.ptr, s);  // t = A d
-        FX_LAUNCH(k_cheb_step, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.r.ptr, l.t.ptr, l.d.ptr, l.x.ptr,
-                  k.c1[st], k.c2[st]);
-    }
+static LnOp ln_op(const AmgLevel& l) {
+    LnOp o{};
+    o.n = l.n;
+    o.row_ptr = l.row_ptr.ptr;
+    o.cols = l.cols.ptr;
+    o.vals = l.vals.ptr;
+    o.dinv = l.dinv.ptr;
+    return o;
 }
 
-void Amg::vcycle(int lev, cudaStream_t s) {
+// Cycle at a coarse level (6x6 blocks) for A x = b (b and x of that level's size):
+// Chebyshev pre-smoothing from x = 0 into the scratch iterate xs (start kernel,
+// then SpMVs fused with the updates), the residual, the coarse correction added
+// to xs, and post-smoothing that reads xs and writes the result into x.
+void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
     AmgLevel& l = L[lev];
     const int64_t nd = (int64_t)l.n * l.bs;
     if (l.coarsest) {
-        FX_LAUNCH(k_dense_matvec, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, l.b.ptr, l.x.ptr);
+        FX_LAUNCH(k_dense_matvec, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, b, x);
         return;
     }
     AmgLevel& c = L[lev + 1];
-    smooth(l, true, degree_, s);
-    level_spmv(l, l.x.ptr, l.b.ptr, l.r.ptr, s);  // r = b - A x
+    const ChebCoef k = cheb_coef(l.lmax, degree_);
+    const unsigned grid = grid_for((int64_t)l.n * 32);
+    double* dA = l.d.ptr;
+    double* dB = l.t.ptr;
+    double* xs = l.xs.ptr;
+    FX_LAUNCH(k_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv.ptr, b, l.r.ptr, dA, xs, k.c2_start);
+    for (int st = 1; st < degree_; ++st) {
+        LnOp o = ln_op(l);
+        o.v = dA;
+        o.r = l.r.ptr;
+        o.d_out = dB;
+        o.xo = xs;
+        o.c1 = k.c1[st];
+        o.c2 = k.c2[st];
+        FX_LAUNCH(k_ln_op<kL0ChebK>, grid, 256, 0, s, o);
+        std::swap(dA, dB);
+    }
+    {
+        LnOp o = ln_op(l);
+        o.v = dA;
+        o.r = l.r.ptr;
+        FX_LAUNCH(k_ln_op<kL0RUpd>, grid, 256, 0, s, o);  // r = b - A xs
+    }
     FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs,
               l.Q.ptr, l.r.ptr, c.b.ptr);
-    vcycle(lev + 1, s);
-    FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, l.bs, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr);
-    smooth(l, false, degree_, s);
+    coarse(lev + 1, s);
+    FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, l.bs, l.agg.ptr, l.Q.ptr, c.x.ptr, xs);
+    {
+        LnOp o = ln_op(l);
+        o.v = xs;
+        o.b = b;
+        o.r = l.r.ptr;
+        o.d_out = dA;
+        o.xo = x;
+        o.c2 = k.c2_start;
+        FX_LAUNCH(k_ln_op<kL0Cheb0>, grid, 256, 0, s, o);
+    }
+    for (int st = 1; st < degree_; ++st) {
+        LnOp o = ln_op(l);
+        o.v = dA;
+        o.r = l.r.ptr;
+        o.d_out = dB;
+        o.xo = x;
+        o.c1 = k.c1[st];
+        o.c2 = k.c2[st];
+        FX_LAUNCH(k_ln_op<kL0ChebK>, grid, 256, 0, s, o);
+        std::swap(dA, dB);
+    }
+}
+
+// Coarse correction at level m: L[m].x ~ A_m^-1 L[m].b, by a K-cycle at the first
+// coarse level (when it is not the coarsest) and V-cycles below.
+void Amg::coarse(int m, cudaStream_t s) {
+    AmgLevel& l = L[m];
+    if (!(kcycle_ && m == 1 && !l.coarsest)) {
+        cycle(m, l.b.ptr, l.x.ptr, s);
+        return;
+    }
+    const int64_t nd = (int64_t)l.n * l.bs;
+    double *z1 = l.kc[0].ptr, *v1 = l.kc[1].ptr, *r = l.kc[2].ptr, *z2 = l.kc[3].ptr, *v2 = l.kc[4].ptr;
+    cycle(m, l.b.ptr, z1, s);
+    level_spmv(l, z1, nullptr, v1, s);
+    FX_LAUNCH(k_kcycle1, 1, 1024, 0, s, nd, l.b.ptr, z1, v1, l.x.ptr, r, l.kcs.ptr);
+    cycle(m, r, z2, s);
+    level_spmv(l, z2, nullptr, v2, s);
+    FX_LAUNCH(k_kcycle2, 1, 1024, 0, s, nd, z1, v1, z2, v2, r, l.x.ptr, l.kcs.ptr);
 }
 
 // Level 0 with the fused operators: pre-smoothing from x = 0 (one elementwise
@@ -1201,7 +1435,7 @@ void Amg::vcycle(int lev, cudaStream_t s) {
 // reduces r.z and beta for the outer CG.
 template <typename VT>
 void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
-                  cudaStream_t s) {
+                  const double* zold, cudaStream_t s) {
     AmgLevel& l = L[0];
     AmgLevel& c = L[1];
     const int64_t nd = (int64_t)l.n * 3;
@@ -1227,7 +1461,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     FX_LAUNCH((k_l0_op<VT, kL0RUpd>), grid, 256, 0, s, o);  // r = b - A x
     FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
               l.Q.ptr, l.r.ptr, c.b.ptr);
-    vcycle(1, s);
+    coarse(1, s);
     FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr);
     o = l0_op<VT>(l, vals);
     o.v = l.x.ptr;
@@ -1238,6 +1472,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     o.c2 = k.c2_start;
     if (degree_ == 1 && S) {
         o.dot = 2;
+        o.zold = zold;
         o.part = part;
         o.counter = counter;
         o.S = S;
@@ -1254,6 +1489,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
         o.c2 = k.c2[st];
         if (st == degree_ - 1 && S) {
             o.dot = 2;
+            o.zold = zold;
             o.part = part;
             o.counter = counter;
             o.S = S;
@@ -1263,9 +1499,10 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     }
 }
 
-void Amg::apply(const double* r, double* z, double* S, double* part, int* counter, cudaStream_t s) {
-    if (vals0_f32_) vcycle0<float>(vals0_f32_, r, z, S, part, counter, s);
-    else vcycle0<double>(L[0].vals0, r, z, S, part, counter, s);
+void Amg::apply(const double* r, double* z, double* S, double* part, int* counter, const double* zold,
+                cudaStream_t s) {
+    if (vals0_f32_) vcycle0<float>(vals0_f32_, r, z, S, part, counter, zold, s);
+    else vcycle0<double>(L[0].vals0, r, z, S, part, counter, zold, s);
 }
 
 // ------------------------------------------------------------------ AMG-preconditioned CG (FP64)
@@ -1339,13 +1576,14 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         v32 = vals32_.ptr;
     }
     amg.set_smoother(opt.amg_degree, v32);
+    amg.set_cycle(opt.amg_kcycle);
     r_.alloc(nd, s);
     z_.alloc(nd, s);
     p_.alloc(nd, s);
     q_.alloc(nd, s);
     const int nb = 296;
     const unsigned g0 = l0_grid(n);
-    part_.alloc(std::max<int64_t>(nb, g0), s);
+    part_.alloc(std::max<int64_t>(nb, 2 * (int64_t)g0), s);
     sc_.alloc(8, s);
     sc_.zero(s);
     counter_.alloc(1, s);
@@ -1356,12 +1594,19 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     FX_LAUNCH(k_rdr_part, nb, 256, 0, s, n, r_.ptr, dinv64, part_.ptr);
     FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 1);
     FX_CUDA_CHECK(cudaMemcpyAsync(sc_.ptr + 3, sc_.ptr + 2, sizeof(double), cudaMemcpyDeviceToDevice, s));
-    amg.apply(r_.ptr, z_.ptr, nullptr, nullptr, nullptr, s);
+    z2_.alloc(nd, s);
+    amg.apply(r_.ptr, z_.ptr, nullptr, nullptr, nullptr, nullptr, s);
     FX_LAUNCH(k_dot_part, nb, 256, 0, s, nd, r_.ptr, z_.ptr, part_.ptr);
     FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 3);
     FX_CUDA_CHECK(cudaMemcpyAsync(p_.ptr, z_.ptr, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
     const AmgLevel& l0 = amg.L[0];
+    // flexible CG (the K-cycle makes the preconditioner vary slightly between
+    // iterations): z alternates between two buffers so that r.z_old is at hand
+    int parity = 0;
     auto iteration = [&]() {
+        double* zn = parity ? z_.ptr : z2_.ptr;
+        const double* zo = parity ? z2_.ptr : z_.ptr;
+        parity ^= 1;
         L0Op<double> o = l0_op<double>(l0, vals64);
         o.v = p_.ptr;
         o.y = q_.ptr;
@@ -1372,8 +1617,8 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         FX_LAUNCH((k_l0_op<double, kL0Apply>), g0, 256, 0, s, o);  // q = A p, alpha
         FX_LAUNCH(k_amg_update2, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
                   counter_.ptr);                                    // x, r, r.D^-1 r
-        amg.apply(r_.ptr, z_.ptr, sc_.ptr, part_.ptr, counter_.ptr, s);  // z = V(r), r.z, beta
-        FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, z_.ptr, sc_.ptr, p_.ptr);
+        amg.apply(r_.ptr, zn, sc_.ptr, part_.ptr, counter_.ptr, amg.kcycle() ? zo : nullptr, s);  // z, r.z, beta
+        FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, zn, sc_.ptr, p_.ptr);
     };
     const int per_poll = 4;
     cudaGraphExec_t gexec = nullptr;

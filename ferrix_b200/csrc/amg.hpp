@@ -43,11 +43,13 @@ struct AmgLevel {
     DBuf<double> Q;                    // n * bs * 6 prolongator rows
     DBuf<int32_t> agg_ptr, agg_nodes;  // members of each aggregate
     int n_agg = 0;
-    // work vectors (n * bs)
-    DBuf<double> x, b, r, d, t;
+    // work vectors (n * bs); xs: pre-smoothed iterate of the coarse-level cycle
+    DBuf<double> x, b, r, d, t, xs;
     // coarsest level: dense inverse (n*bs)^2
     bool coarsest = false;
     DBuf<double> dense_inv;
+    // K-cycle work vectors (first coarse level): z1, v1, r, z2, v2 and scalars
+    DBuf<double> kc[5], kcs;
     const double* dinv_ptr() const { return S0 ? dinv0 : dinv.ptr; }
 };
 
@@ -68,15 +70,23 @@ class Amg {
         degree_ = degree;
         vals0_f32_ = vals_f32;
     }
-    // z = V-cycle(r), FP64 vectors of 3 * n_nodes. With S != null the last
-    // smoothing step also reduces r.z into the outer CG scalars (S[0], S[4]).
-    void apply(const double* r, double* z, double* S, double* part, int* counter, cudaStream_t s);
+    // K-cycle at the first coarse level (true) or V-cycles throughout.
+    void set_cycle(bool kcycle) { kcycle_ = kcycle; }
+    bool kcycle() const { return kcycle_; }
+    // z = cycle(r), FP64 vectors of 3 * n_nodes. With S != null the last
+    // smoothing step also reduces r.z (and r.zold when zold != null, for the
+    // flexible CG) into the outer CG scalars (S[0], S[4]).
+    void apply(const double* r, double* z, double* S, double* part, int* counter, const double* zold,
+               cudaStream_t s);
     std::vector<AmgLevel> L;
 
    private:
-    void vcycle(int l, cudaStream_t s);
+    void cycle(int l, const double* b, double* x, cudaStream_t s);
+    void coarse(int m, cudaStream_t s);
     template <typename VT>
-    void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter, cudaStream_t s);
+    void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
+                 const double* zold, cudaStream_t s);
+    bool kcycle_ = false;
     int degree_ = 2;
     const float* vals0_f32_ = nullptr;
     DBuf<uint8_t> tmp_;
@@ -98,7 +108,7 @@ class AmgPcg {
     Amg amg;
 
    private:
-    DBuf<double> r_, z_, p_, q_, part_, sc_;
+    DBuf<double> r_, z_, z2_, p_, q_, part_, sc_;
     DBuf<float> vals32_;
     DBuf<int> counter_;
 };

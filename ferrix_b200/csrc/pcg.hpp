@@ -90,6 +90,7 @@ struct PcgOptions {
     // multigrid preconditioner
     int amg_degree = 2;       // Chebyshev smoothing steps per pre/post smoothing
     bool amg_fp32 = false;    // FP32 fine-matrix values in the level-0 smoother
+    bool amg_kcycle = false;  // K-cycle at the first coarse level (flexible outer CG)
 };
 
 template <typename T>

@@ -84,6 +84,8 @@ typedef struct {
     int preconditioner;     /* fx_preconditioner */
     int amg_aggregate_nodes; /* FX_PRECOND_AMG: mean nodes per fine aggregate (cell size); 0 = 40 */
     int amg_smoother_degree; /* FX_PRECOND_AMG: Chebyshev steps per pre/post smoothing, 1..8; 0 = 2 */
+    int amg_cycle;           /* FX_PRECOND_AMG: 0 = V-cycle, 1 = K-cycle at the first coarse level (two
+                                flexible-CG steps per coarse correction; the outer CG is then flexible) */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */
