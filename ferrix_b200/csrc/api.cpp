@@ -83,6 +83,12 @@ int fx_ctx_create(int device, fx_ctx** out) {
         c->device = device;
         FX_CUDA_CHECK(cudaSetDevice(device));
         FX_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        // keep freed stream-ordered allocations in this process's pool between solves
+        // instead of returning them to the driver at every synchronisation
+        cudaMemPool_t pool;
+        FX_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = UINT64_MAX;
+        FX_CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         c->tables.init(c->stream);
         return FX_OK;
     });
