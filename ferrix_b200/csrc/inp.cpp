@@ -17,6 +17,9 @@
 #include <cstring>
 #include <unordered_set>
 
+#include <charconv>
+#include <string_view>
+
 #include "common.hpp"
 #include "model.hpp"
 
@@ -48,7 +51,7 @@ static std::vector<std::string> split(const std::string& s, char sep) {
 static bool starts_with(const std::string& s, const char* p) { return s.rfind(p, 0) == 0; }
 
 // f64::from_str: decimal / exponent forms, inf / infinity / nan; nothing else.
-static bool parse_f64(const std::string& s, double* out) {
+static bool parse_f64_slow(const std::string& s, double* out) {
     if (s.empty()) return false;
     std::string low;
     for (char c : s) low.push_back((char)std::tolower((unsigned char)c));
@@ -90,6 +93,67 @@ static bool parse_usize(const std::string& s, int64_t* out) {
     *out = (int64_t)v;
     return true;
 }
+
+// Allocation-free forms for the bulk data lines (*NODE, *ELEMENT): fields as
+// views into the line, trimmed like trim().
+static void split_views(const std::string& s, char sep, std::vector<std::string_view>& out) {
+    out.clear();
+    size_t start = 0;
+    for (size_t i = 0; i <= s.size(); ++i) {
+        if (i == s.size() || s[i] == sep) {
+            size_t a = start, b = i;
+            while (a < b && is_ws(s[a])) ++a;
+            while (b > a && is_ws(s[b - 1])) --b;
+            out.emplace_back(s.data() + a, b - a);
+            start = i + 1;
+        }
+    }
+}
+
+static bool parse_usize_sv(std::string_view s, int64_t* out) {  // usize::from_str
+    size_t i = 0;
+    if (!s.empty() && s[0] == '+') i = 1;
+    if (i >= s.size()) return false;
+    uint64_t v = 0;
+    for (; i < s.size(); ++i) {
+        const unsigned d = (unsigned)(s[i] - '0');
+        if (d > 9) return false;
+        if (v > (UINT64_MAX - d) / 10) return false;
+        v = v * 10 + d;
+    }
+    if (v > (uint64_t)INT64_MAX) return false;
+    *out = (int64_t)v;
+    return true;
+}
+
+// f64::from_str without allocation: same accepted forms as parse_f64 below.
+static bool parse_f64_sv(std::string_view s, double* out) {
+    if (s.empty() || s.size() > 64) {
+        if (s.empty()) return false;
+        return parse_f64_slow(std::string(s), out);
+    }
+    size_t i = (s[0] == '+' || s[0] == '-') ? 1 : 0;
+    bool digit = false, other = false;
+    for (size_t k = i; k < s.size(); ++k) {
+        const char c = s[k];
+        if (c >= '0' && c <= '9') digit = true;
+        else if (!(c == '.' || c == 'e' || c == 'E' || c == '+' || c == '-')) other = true;
+    }
+    if (other || !digit) return parse_f64_slow(std::string(s), out);  // inf / nan spellings, or invalid
+    const char* b = s.data() + (s[0] == '+' ? 1 : 0);
+    const char* e = s.data() + s.size();
+    if (s[0] == '+' && (b == e || *b == '+' || *b == '-')) return false;
+    double v = 0.0;
+    const auto r = std::from_chars(b, e, v);
+    if (r.ec == std::errc() && r.ptr == e) {
+        *out = v;
+        return true;
+    }
+    if (r.ec == std::errc::result_out_of_range) return parse_f64_slow(std::string(s), out);  // inf / 0 like strtod
+    return false;
+}
+
+static bool parse_f64(const std::string& s, double* out) { return parse_f64_sv(std::string_view(s), out); }
 
 // get_keyword_arguments (parser.rs:879-890): later duplicates win.
 using KwArgs = std::unordered_map<std::string, std::pair<bool, std::string>>;  // key -> (has value, value)
@@ -157,7 +221,8 @@ double Record::eval(const SolverTime& t, int64_t current_step) const {  // ampli
 
 std::string preprocess_inp(const std::string& text) {  // parser.rs:903-921
     std::string out;
-    out.reserve(text.size());
+    out.resize(text.size() + 1);
+    size_t w = 0;  // write position (the output is never longer than the input plus one)
     size_t start = 0;
     const size_t n = text.size();
     while (start <= n) {
@@ -170,17 +235,22 @@ std::string preprocess_inp(const std::string& text) {  // parser.rs:903-921
         if (a < b) {
             bool comment = b - a >= 2 && text[a] == '*' && text[a + 1] == '*';
             if (!comment) {
-                for (size_t k = a; k < b; ++k) out.push_back((char)std::toupper((unsigned char)text[k]));
-                out.push_back(text[b - 1] == ',' ? ' ' : '\n');
+                for (size_t k = a; k < b; ++k) {
+                    const char c = text[k];
+                    out[w++] = (c >= 'a' && c <= 'z') ? (char)(c - 'a' + 'A') : c;  // ASCII to_uppercase
+                }
+                out[w++] = text[b - 1] == ',' ? ' ' : '\n';
             }
         }
         if (nl == std::string::npos) break;
         start = nl + 1;
     }
+    out.resize(w);
     // substitute_ccx_solvers (parser.rs:930-942)
     static const char* pats[] = {"ITERATIVE CHOLESKY", "ITERATIVE SCALING", "PASTIX", "PARDISO", "SPOOLES"};
     static const char* reps[] = {"ITERATIVE", "ITERATIVE", "DIRECT", "DIRECT", "DIRECT"};
     for (int k = 0; k < 5; ++k) {
+        if (out.find(pats[k]) == std::string::npos) continue;  // nothing to replace: keep the string
         std::string r;
         r.reserve(out.size());
         size_t pos = 0, plen = std::strlen(pats[k]);
@@ -260,14 +330,19 @@ struct Parser {
     void run() {
         while (pos < lines.size()) {
             line_nr = (int64_t)pos + 1;
-            const std::string line = lines[pos++];
+            const std::string& line = lines[pos++];
             if (!line.empty() && line[0] == '*') {
                 keyword(line);
                 continue;
             }
+            if (line.empty() || kw.empty()) continue;
+            if (!is_ws(line.front()) && !is_ws(line.back())) {  // already trimmed (the usual case)
+                data(line);
+                continue;
+            }
             std::string t = trim(line);
             if (t.empty()) continue;
-            if (!kw.empty()) data(t);
+            data(t);
         }
         if (in_step) finish_step();
         std::vector<int64_t> ids;
@@ -475,23 +550,25 @@ struct Parser {
                 }
     }
 
+    std::vector<std::string_view> fields;  // reused by the bulk data lines
+
     void data(const std::string& line) {
         if (kw == "NODE") {
-            auto f = split(line, ',');
+            split_views(line, ',', fields);
             int64_t id;
             std::array<double, 3> x;
-            if (f.size() != 4 || !parse_usize(trim(f[0]), &id) || !parse_f64(trim(f[1]), &x[0]) ||
-                !parse_f64(trim(f[2]), &x[1]) || !parse_f64(trim(f[3]), &x[2]))
+            if (fields.size() != 4 || !parse_usize_sv(fields[0], &id) || !parse_f64_sv(fields[1], &x[0]) ||
+                !parse_f64_sv(fields[2], &x[1]) || !parse_f64_sv(fields[3], &x[2]))
                 perr("Invalid node definition: " + line);
             p.nodes[id] = x;
         } else if (kw == "ELEMENT") {
             if (!has_elem_type) return;
-            auto f = split(line, ',');
+            split_views(line, ',', fields);
             std::vector<int64_t> nums;
-            nums.reserve(f.size());
-            for (auto& s : f) {
+            nums.reserve(fields.size());
+            for (auto s : fields) {
                 int64_t v;
-                if (!parse_usize(trim(s), &v)) fail(FX_PARSE, "Parsing error at line 0: Integer conversion failed");
+                if (!parse_usize_sv(s, &v)) fail(FX_PARSE, "Parsing error at line 0: Integer conversion failed");
                 nums.push_back(v);
             }
             int npe;
