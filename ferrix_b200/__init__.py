@@ -278,6 +278,18 @@ class Project:
         _check(self.lib.fx_profile_spmv(self.handle, precision, reps, C.byref(ms), C.byref(by)), self.ctx)
         return ms.value, by.value
 
+    def nodal_stress_strain(self):
+        """(S, E): nodal-averaged stress and mechanical strain, (N, 6) each, Voigt xx yy zz xy yz zx
+        (StaticStep::calculate_stress_strain, src/solver/step/static_step.rs:271-379)."""
+        S = np.empty((self.num_nodes, 6))
+        E = np.empty((self.num_nodes, 6))
+        _check(self.lib.fx_nodal_stress_strain(self.handle, _p(S), _p(E)), self.ctx)
+        return S, E
+
+    def write_vtk(self, path: str) -> None:
+        """Legacy ASCII VTK of the current state (VtkWriter::write_increment, src/solver/io/vtk.rs:72-319)."""
+        _check(self.lib.fx_write_vtk(self.handle, os.fsencode(path)), self.ctx)
+
     def profile_smoother(self, precision: int = PREC_MIXED, reps: int = 20):
         """(mean ms, compulsory bytes) of one fused fine-level multigrid smoothing step."""
         ms = C.c_double()

@@ -8,21 +8,6 @@
 
 using namespace fx;
 
-template <typename F>
-static int guarded(fx_ctx* ctx, F&& f) {
-    try {
-        return f();
-    } catch (const fx::Error& e) {
-        if (ctx) ctx->last_error = e.what();
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        if (ctx) ctx->last_error = "host allocation failed";
-        return FX_GENERIC;
-    } catch (const std::exception& e) {
-        if (ctx) ctx->last_error = e.what();
-        return FX_GENERIC;
-    }
-}
 
 namespace {
 template <typename T>

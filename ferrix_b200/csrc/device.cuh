@@ -98,6 +98,7 @@ struct RuleTables {
     const float* dn20_f;
     const double* w20;     // 27
     const uint8_t* pair20; // 210 x 2 (a, b), a <= b
+    const double* dn20_nodes;  // 20 x 3 x 20: shape derivatives at the element's own nodes
 };
 
 __host__ __device__ constexpr int pair_index(int npe, int a, int b) {  // a <= b

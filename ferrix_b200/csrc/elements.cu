@@ -88,6 +88,14 @@ void DeviceTables::init(cudaStream_t s) {
             pairs.push_back((uint8_t)a);
             pairs.push_back((uint8_t)b);
         }
+    // derivatives at the 20 node positions (local coordinates of c3d20.rs:61-84) for stress recovery
+    static const double nodes20[20][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}, {-1, -1, 1},
+                                          {1, -1, 1},   {1, 1, 1},   {-1, 1, 1}, {0, -1, -1}, {1, 0, -1},
+                                          {0, 1, -1},   {-1, 0, -1}, {0, -1, 1}, {1, 0, 1},   {0, 1, 1},
+                                          {-1, 0, 1},   {-1, -1, 0}, {1, -1, 0}, {1, 1, 0},   {-1, 1, 0}};
+    std::vector<double> nn(20), dnn(20 * 60);
+    for (int a = 0; a < 20; ++a) c3d20_shape(nodes20[a][0], nodes20[a][1], nodes20[a][2], nn.data(), &dnn[a * 60]);
+    dn20_nodes.upload(dnn, s);
     n20_d.upload(n, s);
     dn20_d.upload(dn, s);
     n20_f.upload(nf, s);
@@ -98,7 +106,7 @@ void DeviceTables::init(cudaStream_t s) {
 }
 
 RuleTables DeviceTables::view() const {
-    return RuleTables{n20_d.ptr, dn20_d.ptr, n20_f.ptr, dn20_f.ptr, w20.ptr, pair20.ptr};
+    return RuleTables{n20_d.ptr, dn20_d.ptr, n20_f.ptr, dn20_f.ptr, w20.ptr, pair20.ptr, dn20_nodes.ptr};
 }
 
 // ------------------------------------------------------------------ helpers
@@ -508,6 +516,113 @@ __global__ void k_node_gather(int n_nodes, const int32_t* __restrict__ ptr, cons
     out[3 * i] = a0;
     out[3 * i + 1] = a1;
     out[3 * i + 2] = a2;
+}
+
+// ------------------------------------------------------------------ stress recovery
+// StaticStep::calculate_stress_strain (static_step.rs:271-379) with
+// Element::calculate_stress_strain_at_local_coords (element.rs:526-566): at every
+// node of every element, strain = B(xi_node) u_e on the undeformed coordinates,
+// minus the thermal strain change alpha(Tc)(Tc - Tref) - alpha(Ti)(Ti - Tref) on
+// the normal components, stress = D(E(Tc), nu(Tc)) strain (update_state of the
+// elastic material, material.rs:180-195). One thread per (element, node); the
+// 12 values go to the element-node slot and are averaged per node in a fixed
+// order (element count = slots of the node).
+template <int NPE>
+__global__ void __launch_bounds__(128) k_node_stress(int nelem, const int32_t* __restrict__ conn,
+                                                     const int32_t* __restrict__ mat, const double* __restrict__ X,
+                                                     const double* __restrict__ u, const double* __restrict__ tinit,
+                                                     const double* __restrict__ tcur, MatDev md, RuleTables rt,
+                                                     double* __restrict__ out, int* __restrict__ err) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nelem * NPE) return;
+    const int e = (int)(t / NPE), a = (int)(t % NPE);
+    const int32_t* cn = conn + (int64_t)e * NPE;
+    const int k = mat[e];
+    double* o = out + t * 12;
+    // local derivatives at this node: C3D4 constant (c3d4.rs:31-51), C3D20 tabulated
+    auto dnl = [&](int d, int b) -> double {
+        if (NPE == 4) return b == 0 ? -1.0 : (b == d + 1 ? 1.0 : 0.0);
+        return rt.dn20_nodes[a * 60 + d * 20 + b];
+    };
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < NPE; ++b) {
+        const double* xb = X + 3 * (int64_t)cn[b];
+        for (int d = 0; d < 3; ++d) {
+            const double g = dnl(d, b);
+            J[d * 3] += g * xb[0];
+            J[d * 3 + 1] += g * xb[1];
+            J[d * 3 + 2] += g * xb[2];
+        }
+    }
+    double Ji[9];
+    const double det = inv3(J, Ji);
+    Lame L;
+    if (det == 0.0) {
+        atomicOr(err, kErrSingularJ);
+        for (int c = 0; c < 12; ++c) o[c] = 0.0;
+        return;
+    }
+    const int node = cn[a];
+    const double tc = tcur[node], ti = tinit[node];
+    if (k < 0 || !material_d(md, k, tc, &L)) {
+        atomicOr(err, kErrNoMaterial);
+        for (int c = 0; c < 12; ++c) o[c] = 0.0;
+        return;
+    }
+    double eps[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < NPE; ++b) {
+        const double l0 = dnl(0, b), l1 = dnl(1, b), l2 = dnl(2, b);
+        const double gx = Ji[0] * l0 + Ji[1] * l1 + Ji[2] * l2;  // dn_global = inv(J) dn_local
+        const double gy = Ji[3] * l0 + Ji[4] * l1 + Ji[5] * l2;
+        const double gz = Ji[6] * l0 + Ji[7] * l1 + Ji[8] * l2;
+        const double* ub = u + 3 * (int64_t)cn[b];
+        eps[0] += gx * ub[0];
+        eps[1] += gy * ub[1];
+        eps[2] += gz * ub[2];
+        eps[3] += gy * ub[0] + gx * ub[1];  // engineering shear, B rows of element.rs:588-606
+        eps[4] += gz * ub[1] + gy * ub[2];
+        eps[5] += gz * ub[0] + gx * ub[2];
+    }
+    const double dth = thermal_delta(md, k, tc, ti);
+    eps[0] -= dth;
+    eps[1] -= dth;
+    eps[2] -= dth;
+    o[0] = L.d11 * eps[0] + L.d12 * (eps[1] + eps[2]);
+    o[1] = L.d11 * eps[1] + L.d12 * (eps[0] + eps[2]);
+    o[2] = L.d11 * eps[2] + L.d12 * (eps[0] + eps[1]);
+    o[3] = L.d44 * eps[3];
+    o[4] = L.d44 * eps[4];
+    o[5] = L.d44 * eps[5];
+    for (int c = 0; c < 6; ++c) o[6 + c] = eps[c];
+}
+
+__global__ void k_node_average12(int n_nodes, const int32_t* __restrict__ ptr, const int32_t* __restrict__ slots,
+                                 const double* __restrict__ in, double* __restrict__ S, double* __restrict__ E) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes) return;
+    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int cnt = ptr[i + 1] - ptr[i];
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) {
+        const double* f = in + (size_t)slots[k] * 12;
+        for (int c = 0; c < 12; ++c) acc[c] += f[c];
+    }
+    for (int c = 0; c < 6; ++c) {
+        S[6 * (int64_t)i + c] = cnt ? acc[c] / cnt : 0.0;
+        E[6 * (int64_t)i + c] = cnt ? acc[6 + c] / cnt : 0.0;
+    }
+}
+
+void launch_nodal_stress(const ElemView& g4, const ElemView& g20, const double* X, const double* u,
+                         const double* tinit, const double* tcur, const MatDev& md, const RuleTables& rt, int n_nodes,
+                         const int32_t* node_ptr, const int32_t* node_slots, double* slot_buf, double* S, double* E,
+                         int* err, cudaStream_t s) {
+    if (g4.n)
+        FX_LAUNCH(k_node_stress<4>, (unsigned)(((int64_t)g4.n * 4 + 127) / 128), 128, 0, s, g4.n, g4.conn, g4.mat, X,
+                  u, tinit, tcur, md, rt, slot_buf, err);
+    if (g20.n)
+        FX_LAUNCH(k_node_stress<20>, (unsigned)(((int64_t)g20.n * 20 + 127) / 128), 128, 0, s, g20.n, g20.conn,
+                  g20.mat, X, u, tinit, tcur, md, rt, slot_buf + (size_t)g4.n * 4 * 12, err);
+    if (n_nodes) FX_LAUNCH(k_node_average12, (n_nodes + 255) / 256, 256, 0, s, n_nodes, node_ptr, node_slots, slot_buf, S, E);
 }
 
 // ------------------------------------------------------------------ launchers

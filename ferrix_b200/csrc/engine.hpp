@@ -3,6 +3,7 @@
 #pragma once
 
 #include <memory>
+#include <new>
 #include <string>
 
 #include "kernels.hpp"
@@ -76,6 +77,24 @@ struct fx_model {
     fx::SolverTime timer;
     fx::ModelDev dev;
 };
+
+// Runs an entry point's body: fx::Error and standard exceptions become status
+// codes, with the message stored as the context's last error.
+template <typename F>
+inline int guarded(fx_ctx* ctx, F&& f) {
+    try {
+        return f();
+    } catch (const fx::Error& e) {
+        if (ctx) ctx->last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->last_error = "host allocation failed";
+        return FX_GENERIC;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->last_error = e.what();
+        return FX_GENERIC;
+    }
+}
 
 namespace fx {
 

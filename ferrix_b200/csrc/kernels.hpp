@@ -18,7 +18,7 @@ struct ElemView {
 };
 
 struct DeviceTables {
-    DBuf<double> n20_d, dn20_d, w20;
+    DBuf<double> n20_d, dn20_d, w20, dn20_nodes;
     DBuf<float> n20_f, dn20_f;
     DBuf<uint8_t> pair20;
     void init(cudaStream_t s);
@@ -35,6 +35,11 @@ void launch_apply(const ElemView& g4, const ElemView& g20, const double* X, cons
                   const RuleTables& rt, double* fe, int* err, cudaStream_t s);
 void launch_node_gather(int n_nodes, const int32_t* ptr, const int32_t* slots, const double* fe, double* out,
                         cudaStream_t s);
+// nodal-averaged stress and mechanical strain (6 Voigt components each, per node)
+void launch_nodal_stress(const ElemView& g4, const ElemView& g20, const double* X, const double* u,
+                         const double* tinit, const double* tcur, const MatDev& md, const RuleTables& rt, int n_nodes,
+                         const int32_t* node_ptr, const int32_t* node_slots, double* slot_buf, double* S, double* E,
+                         int* err, cudaStream_t s);
 
 // ---- BSR3 structure (assembly.cu)
 // Block row i holds cnt_i = row_ptr[i+1]-row_ptr[i] blocks sorted by column,

@@ -200,6 +200,22 @@ int fx_profile_spmv(fx_model* model, int precision, int reps, double* ms, double
  * support for the FX_PRECOND_AMG path. */
 int fx_profile_smoother(fx_model* model, int precision, int reps, double* ms, double* bytes);
 
+/* ---- result fields ---------------------------------------------------- */
+/* StaticStep::calculate_stress_strain (src/solver/step/static_step.rs:271-379):
+ * nodal-averaged stress and mechanical strain of the current state, 6 Voigt
+ * components per node (xx, yy, zz, xy, yz, zx; engineering shear strains), in
+ * node-index order; strain = B at each element's nodes on the undeformed mesh
+ * minus the thermal strain change, stress = D(E(T), nu(T)) at the node's current
+ * temperature; nodes of no element get zeros. S or E may be NULL. */
+int fx_nodal_stress_strain(fx_model* model, double* S, double* E);
+/* VtkWriter::write_increment (src/solver/io/vtk.rs:72-319) for the current
+ * state: legacy ASCII VTK unstructured grid with POINTS, CELLS (C3D4 as
+ * VTK_TETRA, C3D20 as VTK_QUADRATIC_HEXAHEDRON), U, S, E, NT, MISES, TRESCA.
+ * Cells are written per element type in ascending element id (the reference
+ * follows its hash-map order). The series file and directory layout stay
+ * with the caller. */
+int fx_write_vtk(fx_model* model, const char* path);
+
 /* ---- batched decks ---------------------------------------------------- */
 /* Runs the first step of every model (each fx_state_initialize'd) with all
  * linear solves of the batch advanced together; per-model status in status[]. */

@@ -131,3 +131,42 @@ def test_parser_errors_and_quirks():
     assert [(b.node_id, b.dof) for b in s.bcs] == [(1, 0), (1, 1), (1, 2), (2, 0), (2, 1), (2, 2)]
     # nset CLOAD gives the full value to every node; second *CLOAD continues after *NODE PRINT
     assert [(l.node_id, l.dof, l.value) for l in s.loads] == [(1, 2, 5.0), (2, 2, 5.0), (2, 0, 1.0)]
+
+
+# ---- result fields (oracle/stress.py) ------------------------------------------------------------
+
+def test_stress_oracle_c3d20_derivatives_match_the_c_restatement():
+    from oracle import elem, stress
+    rng = np.random.default_rng(3)
+    pts = list(stress.C3D20_NODES) + list(rng.uniform(-1, 1, size=(5, 3)))
+    for q in pts:
+        g = stress.c3d20_local_derivatives(np.asarray(q, dtype=np.float64))
+        _, dn = elem.shape_c3d20(*q)
+        assert np.abs(g - dn).max() < 1e-14
+        assert np.abs(g.sum(axis=1)).max() < 1e-14  # partition of unity
+
+
+@pytest.mark.parametrize("npe", [4, 20])
+def test_stress_oracle_reproduces_a_uniform_strain_field(npe):
+    """Patch test: u = G x gives the strain sym(G) (engineering shear) at every node, stress = D strain."""
+    from ferrix_b200 import decks
+    from oracle import inp, stress
+    text = decks.c3d4_cantilever(2, 2, 3) if npe == 4 else decks.c3d20_box(2, 2, 2)
+    p = inp.parse_inp_text(text)
+    xyz = np.asarray([p.nodes[i] for i in p.index_to_node_id])
+    G = np.array([[1e-3, 2e-4, -3e-4], [5e-4, -2e-3, 1e-4], [-1e-4, 3e-4, 4e-4]])
+    u = (xyz @ G.T).ravel()
+    t = np.full(len(xyz), 20.0)
+    S, E = stress.nodal_stress_strain(p, u, t, t)
+    want = np.array([G[0, 0], G[1, 1], G[2, 2], G[0, 1] + G[1, 0], G[1, 2] + G[2, 1], G[0, 2] + G[2, 0]])
+    assert np.abs(E - want).max() < 1e-12
+    mat = p.materials[0]
+    D = stress._d_matrix(mat.youngs_modulus.interpolate(20.0), mat.poisson_ratio.interpolate(20.0))
+    assert np.abs(S - D @ want).max() < 1e-7 * np.abs(D @ want).max()
+
+
+def test_mises_and_tresca_closed_forms():
+    from oracle import stress
+    S = np.array([[100.0, 0, 0, 0, 0, 0], [0, 0, 0, 50.0, 0, 0], [10.0, 10.0, 10.0, 0, 0, 0]])
+    assert np.allclose(stress.mises(S), [100.0, np.sqrt(3.0) * 50.0, 0.0])
+    assert np.allclose(stress.tresca(S), [100.0, 100.0, 0.0])
