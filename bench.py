@@ -137,6 +137,26 @@ def run_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_once(args, rank: int, local: int) -> None:
+    """--mode once: parse the C3D20 box (--cells) and run one step with the default solver options
+    and --precision / --preconditioner; prints the step statistics (for profiler runs)."""
+    import ferrix_b200 as fx
+    from ferrix_b200 import decks
+    nx, ny, nz = (int(v) for v in args.cells.split(","))
+    prec = {"fp64": fx.PREC_FP64, "mixed": fx.PREC_MIXED, "fp64_csr": fx.PREC_FP64_CSR}[args.precision]
+    pc = {"amg": fx.PRECOND_AMG, "bj": fx.PRECOND_BLOCK_JACOBI}[args.preconditioner]
+    ctx = fx.Context(local)
+    p = fx.Project.from_inp_text(decks.c3d20_box(nx, ny, nz), ctx)
+    st = fx.SolutionState(p.num_dofs, p.num_nodes)
+    st.initialize(p)
+    s = p.steps[0].solve(1, p, st, opts=fx.solve_opts(precision=prec, preconditioner=pc))
+    print(json.dumps({"mode": "once", "dofs": p.num_dofs, **{k: s[k] for k in (
+        "pcg_iterations", "amg_levels", "amg_setup_ms", "t_assembly_ms", "t_pcg_ms", "t_total_ms", "bsr_blocks")}}),
+          flush=True)
+    p.close()
+    ctx.close()
+
+
 def _serve_summary(res):
     return {k: res[k] for k in ("rate_per_s", "requests", "completed", "slots", "p50_ms", "p99_ms", "mean_ms",
                                 "solves_per_s", "mean_dofs")}
@@ -335,7 +355,8 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="serve mode: requests per rate")
     ap.add_argument("--slots", type=int, default=4, help="serve mode: concurrent requests on the GPU")
     ap.add_argument("--decks", type=int, default=256, help="batch mode: number of decks")
-    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "serve", "batch", "nlgeom"],
+    ap.add_argument("--cells", default="20,20,80", help="once mode: C3D20 box cells nx,ny,nz")
+    ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "serve", "batch", "nlgeom", "once"],
                     help="spmv: only assemble and time REPS standalone SpMV launches (profiling case)")
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
@@ -344,6 +365,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.mode == "once":
+        return run_once(args, rank, local)
     if args.mode == "serve":
         return run_serve(args, rank, local)
     if args.mode == "batch":
@@ -541,9 +564,14 @@ def main():
         try:
             import re
             prof = open(os.path.join(ROOT, "profiles", prof_name)).read()
-            m = re.search(r"traffic_bytes_per_launch[^|]*\|\s*([\d,]+)\s*\|\s*([\d,]+)", prof)
-            if m:
-                traffic = int((m.group(2) if prec == fx.PREC_MIXED else m.group(1)).replace(",", ""))
+            if use_amg:  # one row per precision: traffic_bytes_per_launch_<precision> | N
+                m = re.search(r"traffic_bytes_per_launch_%s[^|]*\|\s*([\d,]+)" % args.precision, prof)
+                if m:
+                    traffic = int(m.group(1).replace(",", ""))
+            else:
+                m = re.search(r"traffic_bytes_per_launch[^|]*\|\s*([\d,]+)\s*\|\s*([\d,]+)", prof)
+                if m:
+                    traffic = int((m.group(2) if prec == fx.PREC_MIXED else m.group(1)).replace(",", ""))
         except OSError:
             pass
         plain = arms.get("plain_fp64_csr_jacobi", {}).get("ms")
