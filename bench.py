@@ -257,24 +257,32 @@ def run_batch(args, rank: int, local: int) -> None:
 
     Arms: one fx_batch_solve over all decks (mixed block-Jacobi PCG, all systems in
     one launch sequence per iteration block), the same decks one after another, and
-    the request loop (4 slots, multigrid) fed with all decks at once."""
-    if rank != 0:
-        return
+    the request loop (4 slots, multigrid) fed with all decks at once. Under torchrun
+    the decks are partitioned across the ranks by DOF count (footprint), no
+    collective on the data path; solves/s = all decks / max-over-ranks time."""
     import numpy as np
     import torch
     import ferrix_b200 as fx
-    from ferrix_b200 import decks
+    from ferrix_b200 import decks, multi
     from oracle import inp, static_step
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     t0 = time.perf_counter()
     pop = decks.batch_population(args.decks, seed=7, dof_lo=2e3, dof_hi=6e4, c3d20_fraction=0.0)
     gen_s = time.perf_counter() - t0
-    texts = [t for t, _ in pop]
-    dofs = np.array([d for _, d in pop])
+    all_dofs = [d for _, d in pop]
+    mine = multi.partition_by_footprint(all_dofs, world)[rank]
+    texts = [pop[i][0] for i in mine]
+    dofs = np.array([pop[i][1] for i in mine])
     ctx = fx.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
     out = {"mode": "batch", "metric": "batched linear static solves/s (C3D4 decks, mixed precision, 1e-8)",
-           "decks": len(texts), "total_dofs": int(dofs.sum()), "mean_dofs": float(dofs.mean()),
-           "deck_generation_s": gen_s, "arms": {}}
+           "decks": len(pop), "n_gpus": world, "total_dofs": int(np.sum(all_dofs)),
+           "mean_dofs": float(np.mean(all_dofs)), "deck_generation_s": gen_s, "arms": {}}
 
     def projects():
         ps = [fx.Project.from_inp_text(t, ctx) for t in texts]
@@ -305,8 +313,10 @@ def run_batch(args, rank: int, local: int) -> None:
             u_batch.append(s.displacements)
         for p in ps:
             p.close()
-    out["arms"]["fx_batch_solve_mixed_bj"] = {"solves_per_s": len(texts) / dev_s, "device_s": dev_s,
-                                              "wall_s": wall_s, "failed": int(np.sum(st != 0)),
+    dev_max = multi.max_over_ranks(dev_s, device="cuda")
+    out["arms"]["fx_batch_solve_mixed_bj"] = {"solves_per_s": len(pop) / dev_max, "device_s": dev_max,
+                                              "wall_s": wall_s,
+                                              "failed": int(multi.sum_over_ranks(float(np.sum(st != 0)), "cuda")),
                                               "pcg_iterations_max": int(max(s["pcg_iterations"] for s in stats))}
     ps = projects()
 
@@ -321,15 +331,18 @@ def run_batch(args, rank: int, local: int) -> None:
     bad, dev_s, wall_s = timed(seq)
     for p in ps:
         p.close()
-    out["arms"]["sequential_mixed_bj"] = {"solves_per_s": len(texts) / dev_s, "device_s": dev_s, "wall_s": wall_s,
-                                          "failed": bad}
+    dev_max = multi.max_over_ranks(dev_s, device="cuda")
+    out["arms"]["sequential_mixed_bj"] = {"solves_per_s": len(pop) / dev_max, "device_s": dev_max, "wall_s": wall_s,
+                                          "failed": int(multi.sum_over_ranks(float(bad), "cuda"))}
     ctx.close()
     from ferrix_b200 import serving
     res = serving.run_stream(texts, 1e6, len(texts), fx.solve_opts(precision=fx.PREC_MIXED,
                                                                   preconditioner=fx.PRECOND_AMG, rtol=1e-8),
                              device=local, slots=4, seed=1)
-    out["arms"]["request_loop_mixed_amg_4_slots"] = {"solves_per_s": res["solves_per_s"], "wall_s": res["span_s"],
-                                                     "failed": len(texts) - res["completed"]}
+    span = multi.max_over_ranks(res["span_s"], device="cuda")
+    out["arms"]["request_loop_mixed_amg_4_slots"] = {"solves_per_s": len(pop) / span, "wall_s": span,
+                                                     "failed": int(multi.sum_over_ranks(
+                                                         float(len(texts) - res["completed"]), "cuda"))}
     # accuracy of the batched result on the first decks against the oracle's direct solve
     errs = []
     for k in range(min(4, len(texts))):
@@ -338,7 +351,11 @@ def run_batch(args, rank: int, local: int) -> None:
         ref = static_step.Runner(o).run().displacements
         errs.append(float(np.linalg.norm(u_batch[k] - ref) / np.linalg.norm(ref)))
     out["rel_err_vs_oracle_first4"] = errs
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():
@@ -443,9 +460,8 @@ def main():
     launches = ctx.kernel_launches - launches0
     u_gpu = state.displacements
     if dist:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+        from ferrix_b200 import multi
+        elapsed = multi.max_over_ranks(elapsed, device="cuda")
         dist.barrier()
 
     # dominant kernel, timed standalone with CUDA events on the context stream:
