@@ -174,18 +174,38 @@ def run_serve(args, rank: int, local: int) -> None:
            "pool": "16 seeded boxes, 60% C3D4 / 40% C3D20, DOF log-uniform [5k, 500k]", "arms": {}}
     arms = (("mixed_amg", fx.solve_opts(precision=fx.PREC_MIXED, preconditioner=fx.PRECOND_AMG), rates),
             ("plain_fp64_csr_jacobi", fx.solve_opts(precision=fx.PREC_FP64_CSR), rates[:2]))
+    import numpy as np
+    from oracle import inp, static_step
+    smallest = [int(i) for i in np.argsort([len(t) for t in pool])[:3]]
+    refs = {}
     for name, o, rs in arms:
-        out["arms"][name] = [_serve_summary(serving.run_stream(pool, r, args.requests, o, device=local,
-                                                               slots=args.slots, seed=int(r)))
-                             for r in rs]
+        out["arms"][name] = []
+        for r in rs:
+            res = serving.run_stream(pool, r, args.requests, o, device=local, slots=args.slots, seed=int(r),
+                                     keep=smallest)
+            line = _serve_summary(res)
+            # accuracy of served results (the smallest pool decks that were drawn) against the oracle
+            errs = {}
+            for i, u in res["kept"].items():
+                if i not in refs:
+                    q = inp.parse_inp_text(pool[i])
+                    q.default_initial_temperature = 20.0
+                    refs[i] = static_step.Runner(q).run().displacements
+                errs[i] = float(np.linalg.norm(u - refs[i]) / np.linalg.norm(refs[i]))
+            line["rel_err_vs_oracle"] = errs
+            out["arms"][name].append(line)
     print(json.dumps(out), flush=True)
+
+
+NLGEOM_FULL = (100, 20, 20)  # 240,000 C3D4, 133,623 DOF
+NLGEOM_MID = (50, 10, 10)    # 30,000 C3D4, 16,833 DOF: same beam, coarser, for the oracle
 
 
 def _oracle_nlgeom_job(out_path: str, q) -> None:
     import numpy as np
     from ferrix_b200 import decks
     from oracle import inp, static_step
-    text = decks.c3d4_nlgeom_beam()
+    text = decks.c3d4_nlgeom_beam(*NLGEOM_MID)
     t0 = time.perf_counter()
     p = inp.parse_inp_text(text)
     p.default_initial_temperature = 20.0
@@ -193,61 +213,76 @@ def _oracle_nlgeom_job(out_path: str, q) -> None:
     st = r.run()
     dt = time.perf_counter() - t0
     np.save(out_path, st.displacements)
-    q.put({"seconds": dt, "increments": len(r.log), "cores": os.cpu_count(),
-           "phases": {k: round(v, 3) for k, v in vars(r.t).items()}})
+    q.put({"seconds": dt, "increments": len(r.log), "newton_iterations": sum(len(l.residuals) - 1 for l in r.log),
+           "cores": os.cpu_count(), "phases": {k: round(v, 3) for k, v in vars(r.t).items()}})
 
 
 def run_nlgeom(args, rank: int, local: int) -> None:
-    """--mode nlgeom: the C3D4 NLGEOM beam (240,000 C3D4, 133,623 DOF, E(T), thermal gradient,
-    amplitude ramp over 10 increments): whole-step time on the GPU, both preconditioners, and the
-    oracle's FP64 Cholesky Newton run on the host cores for accuracy and the CPU time."""
+    """--mode nlgeom: the C3D4 NLGEOM beam (E(T), initial temperature gradient, amplitude
+    ramp over 10 increments) at full size (240,000 C3D4, 133,623 DOF): whole-step device time
+    for three solvers, their agreement with each other; the same beam at 30,000 C3D4 against
+    the oracle's FP64 Cholesky Newton run (spawned on the host cores; a full-size oracle run
+    takes most of an hour)."""
     if rank != 0:
         return
     import numpy as np
     ctxmp = mp.get_context("spawn")
     q = ctxmp.Queue()
     out_path = os.path.join("/tmp", f"u_oracle_nl_{os.getpid()}.npy")
-    proc = ctxmp.Process(target=_oracle_nlgeom_job, args=(out_path, q), daemon=True)
-    proc.start()
+    proc = None
+    if not args.no_oracle:
+        proc = ctxmp.Process(target=_oracle_nlgeom_job, args=(out_path, q), daemon=True)
+        proc.start()
     import torch
     import ferrix_b200 as fx
     from ferrix_b200 import decks
-    text = decks.c3d4_nlgeom_beam()
     ctx = fx.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    p = fx.Project.from_inp_text(text, ctx)
-    p.default_initial_temperature = 20.0
-    st = fx.SolutionState(p.num_dofs, p.num_nodes)
-    out = {"mode": "nlgeom", "metric": "C3D4 NLGEOM step time (ms) and accuracy vs FP64 oracle",
-           "dofs": p.num_dofs, "arms": {}}
-    for name, o in (("mixed_amg", fx.solve_opts()),
-                    ("mixed_blockjacobi", fx.solve_opts(preconditioner=fx.PRECOND_BLOCK_JACOBI)),
-                    ("fp64_blockjacobi", fx.solve_opts(precision=fx.PREC_FP64,
-                                                       preconditioner=fx.PRECOND_BLOCK_JACOBI))):
-        best = None
-        for _ in range(2):
-            st.initialize(p)
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            s = p.steps[0].solve(1, p, st, opts=o)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1)
-            best = ms if best is None else min(best, ms)
-        out["arms"][name] = {"ms": best, "increments": s["increments"], "newton_iterations": s["newton_iterations"],
-                             "linear_solves": s["linear_solves"], "pcg_iterations": s["pcg_iterations"],
-                             "u": st.displacements}
-    res = q.get(timeout=3600)
-    proc.join(timeout=60)
-    u_ref = np.load(out_path)
-    for a in out["arms"].values():
-        a["rel_err_vs_oracle"] = float(np.linalg.norm(a.pop("u") - u_ref) / np.linalg.norm(u_ref))
-    out["cpu_oracle"] = {"seconds": res["seconds"], "increments": res["increments"], "cores": res["cores"],
-                         "phases_s": res["phases"]}
-    os.remove(out_path)
-    p.close()
+    solvers = (("mixed_amg", fx.solve_opts()),
+               ("mixed_blockjacobi", fx.solve_opts(preconditioner=fx.PRECOND_BLOCK_JACOBI)),
+               ("fp64_blockjacobi", fx.solve_opts(precision=fx.PREC_FP64, preconditioner=fx.PRECOND_BLOCK_JACOBI)))
+    out = {"mode": "nlgeom", "metric": "C3D4 NLGEOM step: device time (ms) and accuracy vs FP64 oracle",
+           "full": {}, "mid": {}}
+    for size, key, reps in ((NLGEOM_FULL, "full", 2), (NLGEOM_MID, "mid", 1)):
+        p = fx.Project.from_inp_text(decks.c3d4_nlgeom_beam(*size), ctx)
+        p.default_initial_temperature = 20.0
+        st = fx.SolutionState(p.num_dofs, p.num_nodes)
+        out[key]["dofs"] = p.num_dofs
+        for name, o in solvers:
+            best = None
+            for _ in range(reps):
+                st.initialize(p)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s = p.steps[0].solve(1, p, st, opts=o)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            out[key][name] = {"ms": best, "increments": s["increments"], "newton_iterations": s["newton_iterations"],
+                              "linear_solves": s["linear_solves"], "pcg_iterations": s["pcg_iterations"],
+                              "u": st.displacements}
+        u64 = out[key]["fp64_blockjacobi"]["u"]
+        for name, _ in solvers:
+            a = out[key][name]
+            a["rel_diff_vs_fp64_blockjacobi"] = float(np.linalg.norm(a["u"] - u64) / np.linalg.norm(u64))
+        p.close()
+    if proc is not None:
+        res = q.get(timeout=7200)
+        proc.join(timeout=60)
+        u_ref = np.load(out_path)
+        for name, _ in solvers:
+            a = out["mid"][name]
+            a["rel_err_vs_oracle"] = float(np.linalg.norm(a["u"] - u_ref) / np.linalg.norm(u_ref))
+        out["mid"]["cpu_oracle"] = {"seconds": res["seconds"], "increments": res["increments"],
+                                    "newton_iterations": res["newton_iterations"], "cores": res["cores"],
+                                    "phases_s": res["phases"]}
+        os.remove(out_path)
+    for key in ("full", "mid"):
+        for name, _ in solvers:
+            out[key][name].pop("u")
     ctx.close()
     print(json.dumps(out), flush=True)
 

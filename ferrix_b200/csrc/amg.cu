@@ -729,20 +729,32 @@ __device__ __forceinline__ void cta_dot_finalize(double v, double v2, int mode, 
 }
 
 #ifndef FX_L0_MIN_BLOCKS
-#define FX_L0_MIN_BLOCKS 3
+#define FX_L0_MIN_BLOCKS 2
 #endif
-constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per SM (3: at most 85 registers)
+constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per SM (2: at most 128 registers)
+
+#ifndef FX_L0_LANES
+#define FX_L0_LANES 8
+#endif
+constexpr int kL0Lanes = FX_L0_LANES;          // lanes per block row (8 or 4)
+constexpr int kL0RowsPerWarp = 32 / kL0Lanes;
+constexpr int kL0LaneShift = kL0Lanes == 8 ? 3 : 2;
+#ifndef FX_L0_UNROLL
+#define FX_L0_UNROLL 2
+#endif
+constexpr int kL0Unroll = FX_L0_UNROLL;  // groups of a row in flight per lane
 
 template <typename VT, int MODE>
 __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
-    const int sub = threadIdx.x & 7;
-    const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const int rows_per_grid = (gridDim.x * blockDim.x) >> 3;
-    const int nb = ((o.n + 3) / 4) * 4;  // uniform trip count per warp (4 rows per warp)
+    const int sub = threadIdx.x & (kL0Lanes - 1);
+    const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> kL0LaneShift;
+    const int rows_per_grid = (gridDim.x * blockDim.x) >> kL0LaneShift;
+    // uniform trip count per warp: the warp's rows share one base
+    const int nb = ((o.n + kL0RowsPerWarp - 1) / kL0RowsPerWarp) * kL0RowsPerWarp;
     const double* __restrict__ v = o.v;
     double dsum = 0.0, dsum2 = 0.0;
-    for (int base = row0 - (row0 & 3); base < nb; base += rows_per_grid) {
-        const int row = base + (row0 & 3);
+    for (int base = row0 - (row0 & (kL0RowsPerWarp - 1)); base < nb; base += rows_per_grid) {
+        const int row = base + (row0 & (kL0RowsPerWarp - 1));
         const bool valid = row < o.n;
         const int g0 = valid ? o.goff[row] : 0;
         const int ng = valid ? o.goff[row + 1] - g0 : 0;
@@ -772,7 +784,8 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
             }
         }
         double acc[3] = {0.0, 0.0, 0.0};
-        for (int g = sub; g < ng; g += 8) {
+#pragma unroll kL0Unroll
+        for (int g = sub; g < ng; g += kL0Lanes) {
             const int4 cc = __ldg(reinterpret_cast<const int4*>(o.cols) + g0 + g);
             const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
             double xv[4][3];
@@ -796,7 +809,7 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
             }
         }
 #pragma unroll
-        for (int s = 4; s > 0; s >>= 1)
+        for (int s = kL0Lanes / 2; s > 0; s >>= 1)
 #pragma unroll
             for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], s);
         // epilogue: lane c of the row's 8 handles component c
@@ -1072,7 +1085,7 @@ static unsigned l0_grid(int n) {
         cached_cap = std::max(1, sms * std::max(1, per_sm));
         cached_dev = dev;
     }
-    return (unsigned)std::min<int64_t>(grid_for((int64_t)n * 8), cached_cap);
+    return (unsigned)std::min<int64_t>(grid_for((int64_t)n * kL0Lanes), cached_cap);
 }
 
 template <typename VT>
