@@ -657,6 +657,10 @@ struct L0Op {
     double* part;
     int* counter;
     double* S;
+    // FP32 smoother vectors (mixed precision): the gathered vector as float4 per
+    // node (x, y, z, 0) and the new direction written into the same layout
+    const float4* v4;
+    float* d4_out;
 };
 
 __device__ __forceinline__ void ld4v(const float* p, float o[4]) {
@@ -744,7 +748,10 @@ constexpr int kL0LaneShift = kL0Lanes == 8 ? 3 : 2;
 #endif
 constexpr int kL0Unroll = FX_L0_UNROLL;  // groups of a row in flight per lane
 
-template <typename VT, int MODE>
+// G32: gathers from o.v4 (FP32, 16 B per node) and writes the direction into
+// o.d4_out; the row's own FP64 values still come from o.v where the mode needs
+// them (Cheb0: the iterate), else from o.v4.
+template <typename VT, int MODE, bool G32 = false>
 __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
     const int sub = threadIdx.x & (kL0Lanes - 1);
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> kL0LaneShift;
@@ -771,7 +778,12 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
                     src3[kk] = src[o3 + kk];
                     Dr[kk] = o.dinv[9 * (int64_t)row + 3 * c + kk];
                 }
-                vc = v[o3 + c];
+                if (G32 && MODE == kL0ChebK) {
+                    const float* own = reinterpret_cast<const float*>(o.v4 + row);
+                    vc = (double)own[c];
+                } else {
+                    vc = v[o3 + c];
+                }
                 if (MODE == kL0ChebK) xoc = o.xo[o3 + c];
                 if (o.dot) bc = o.b[o3 + c];
                 if (o.dot && o.zold) zoc = o.zold[o3 + c];
@@ -789,10 +801,20 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
             const int4 cc = __ldg(reinterpret_cast<const int4*>(o.cols) + g0 + g);
             const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
             double xv[4][3];
+            if (G32) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+                for (int q = 0; q < 4; ++q) {
+                    const float4 t = __ldg(o.v4 + cj[q]);
+                    xv[q][0] = (double)t.x;
+                    xv[q][1] = (double)t.y;
+                    xv[q][2] = (double)t.z;
+                }
+            } else {
 #pragma unroll
-                for (int k = 0; k < 3; ++k) xv[q][k] = __ldg(v + 3 * (int64_t)cj[q] + k);
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) xv[q][k] = __ldg(v + 3 * (int64_t)cj[q] + k);
+            }
             const VT* vb = o.vals + ((int64_t)g0 * 9 + g) * 4;
             const int64_t pl = (int64_t)ng * 4;
 #pragma unroll
@@ -828,7 +850,8 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
             const double z = Dr[0] * rr[0] + Dr[1] * rr[1] + Dr[2] * rr[2];
             o.r[o3 + c] = c == 0 ? rr[0] : (c == 1 ? rr[1] : rr[2]);
             const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * vc) + o.c2 * z;
-            o.d_out[o3 + c] = dn;
+            if (G32) o.d4_out[4 * (int64_t)row + c] = (float)dn;
+            else o.d_out[o3 + c] = dn;
             const double xn = (MODE == kL0Cheb0 ? vc : xoc) + dn;
             o.xo[o3 + c] = xn;
             if (o.dot) {
@@ -1006,20 +1029,42 @@ __global__ void k_cheb_start(int n, int bs, const double* __restrict__ dinv, con
 }
 
 // first pre-smoothing step from x = 0: d = c2 D^-1 b; x = d; r = b
+// (d4 != null: the direction as float4 per node instead of d)
 __global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const double* __restrict__ b,
-                                double* __restrict__ r, double* __restrict__ d, double* __restrict__ x, double c2) {
+                                double* __restrict__ r, double* __restrict__ d, float4* __restrict__ d4,
+                                double* __restrict__ x, double c2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t o3 = 3 * (int64_t)i;
     const double bb[3] = {b[o3], b[o3 + 1], b[o3 + 2]};
     const double* D = dinv + 9 * (int64_t)i;
+    double t[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const double t = c2 * (D[3 * c] * bb[0] + D[3 * c + 1] * bb[1] + D[3 * c + 2] * bb[2]);
+        t[c] = c2 * (D[3 * c] * bb[0] + D[3 * c + 1] * bb[1] + D[3 * c + 2] * bb[2]);
         r[o3 + c] = bb[c];
-        d[o3 + c] = t;
-        x[o3 + c] = t;
+        x[o3 + c] = t[c];
     }
+    if (d4) d4[i] = make_float4((float)t[0], (float)t[1], (float)t[2], 0.0f);
+    else
+        for (int c = 0; c < 3; ++c) d[o3 + c] = t[c];
+}
+
+// fine level: x += Q xc (3 rows per node) and the FP32 copy of x for the smoother gathers
+__global__ void k_prolong0(int n, const int32_t* __restrict__ agg, const double* __restrict__ Q,
+                           const double* __restrict__ xc, double* __restrict__ xf, float4* __restrict__ x4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* x = xc + (int64_t)agg[i] * 6;
+    double out[3];
+    for (int k = 0; k < 3; ++k) {
+        const double* q = Q + (3 * (int64_t)i + k) * 6;
+        double t = 0.0;
+        for (int c = 0; c < 6; ++c) t += q[c] * x[c];
+        out[k] = xf[3 * (int64_t)i + k] + t;
+        xf[3 * (int64_t)i + k] = out[k];
+    }
+    x4[i] = make_float4((float)out[0], (float)out[1], (float)out[2], 0.0f);
 }
 
 // x += alpha p, r -= alpha q; r.D^-1 r reduced by the last CTA into S[2]
@@ -1172,6 +1217,11 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         const int64_t nd = (int64_t)l.n * l.bs;
         for (DBuf<double>* v : {&l.x, &l.b, &l.r, &l.d, &l.t}) v->alloc(nd, s);
         if (lev > 0) l.xs.alloc(nd, s);
+        if (lev == 0)
+            for (DBuf<float>* v : {&l.d4a, &l.d4b, &l.x4}) {
+                v->alloc(4 * (size_t)l.n, s);
+                v->zero(s);  // the fourth component stays 0
+            }
         if (lev > 0) {
             l.dinv.alloc((size_t)l.n * 36, s);
             FX_LAUNCH(k_block_inv6, grid_for(l.n, 128), 128, 0, s, l.n, l.row_ptr.ptr, l.cols.ptr, l.vals.ptr,
@@ -1454,52 +1504,64 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     const int64_t nd = (int64_t)l.n * 3;
     const ChebCoef k = cheb_coef(l.lmax, degree_);
     const unsigned grid = l0_grid(l.n);
+    // FP32 values: the smoother's gathered vectors are FP32 too (float4 per node)
+    constexpr bool g32 = sizeof(VT) == 4;
     double* dA = l.d.ptr;
     double* dB = l.t.ptr;
-    FX_LAUNCH(k_l0_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.dinv0, b, l.r.ptr, dA, l.x.ptr, k.c2_start);
-    L0Op<VT> o = l0_op<VT>(l, vals);
+    float4* dA4 = reinterpret_cast<float4*>(l.d4a.ptr);
+    float4* dB4 = reinterpret_cast<float4*>(l.d4b.ptr);
+    float4* x4 = reinterpret_cast<float4*>(l.x4.ptr);
+    FX_LAUNCH(k_l0_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.dinv0, b, l.r.ptr, dA, g32 ? dA4 : nullptr, l.x.ptr,
+              k.c2_start);
+    auto op = [&]() {
+        L0Op<VT> o = l0_op<VT>(l, vals);
+        return o;
+    };
     for (int st = 1; st < degree_; ++st) {
+        L0Op<VT> o = op();
         o.v = dA;
+        o.v4 = dA4;
         o.r = l.r.ptr;
         o.d_out = dB;
+        o.d4_out = reinterpret_cast<float*>(dB4);
         o.xo = l.x.ptr;
         o.c1 = k.c1[st];
         o.c2 = k.c2[st];
-        FX_LAUNCH((k_l0_op<VT, kL0ChebK>), grid, 256, 0, s, o);
+        FX_LAUNCH((k_l0_op<VT, kL0ChebK, g32>), grid, 256, 0, s, o);
         std::swap(dA, dB);
+        std::swap(dA4, dB4);
     }
-    o = l0_op<VT>(l, vals);
-    o.v = dA;
-    o.r = l.r.ptr;
-    FX_LAUNCH((k_l0_op<VT, kL0RUpd>), grid, 256, 0, s, o);  // r = b - A x
+    {
+        L0Op<VT> o = op();
+        o.v = dA;
+        o.v4 = dA4;
+        o.r = l.r.ptr;
+        FX_LAUNCH((k_l0_op<VT, kL0RUpd, g32>), grid, 256, 0, s, o);  // r = b - A x
+    }
     FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
               l.Q.ptr, l.r.ptr, c.b.ptr);
     coarse(1, s);
-    FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr);
-    o = l0_op<VT>(l, vals);
-    o.v = l.x.ptr;
-    o.b = b;
-    o.r = l.r.ptr;
-    o.d_out = dA;
-    o.xo = z;
-    o.c2 = k.c2_start;
-    if (degree_ == 1 && S) {
-        o.dot = 2;
-        o.zold = zold;
-        o.part = part;
-        o.counter = counter;
-        o.S = S;
-    }
-    FX_LAUNCH((k_l0_op<VT, kL0Cheb0>), grid, 256, 0, s, o);
-    for (int st = 1; st < degree_; ++st) {
-        o = l0_op<VT>(l, vals);
-        o.v = dA;
+    if (g32) FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4);
+    else FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr);
+    for (int st = 0; st < degree_; ++st) {
+        L0Op<VT> o = op();
         o.b = b;
         o.r = l.r.ptr;
-        o.d_out = dB;
         o.xo = z;
-        o.c1 = k.c1[st];
-        o.c2 = k.c2[st];
+        if (st == 0) {  // from the iterate: r = b - A x, d = D^-1 r / theta, z = x + d
+            o.v = l.x.ptr;
+            o.v4 = x4;
+            o.d_out = dA;
+            o.d4_out = reinterpret_cast<float*>(dA4);
+            o.c2 = k.c2_start;
+        } else {
+            o.v = dA;
+            o.v4 = dA4;
+            o.d_out = dB;
+            o.d4_out = reinterpret_cast<float*>(dB4);
+            o.c1 = k.c1[st];
+            o.c2 = k.c2[st];
+        }
         if (st == degree_ - 1 && S) {
             o.dot = 2;
             o.zold = zold;
@@ -1507,8 +1569,12 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
             o.counter = counter;
             o.S = S;
         }
-        FX_LAUNCH((k_l0_op<VT, kL0ChebK>), grid, 256, 0, s, o);
-        std::swap(dA, dB);
+        if (st == 0) FX_LAUNCH((k_l0_op<VT, kL0Cheb0, g32>), grid, 256, 0, s, o);
+        else {
+            FX_LAUNCH((k_l0_op<VT, kL0ChebK, g32>), grid, 256, 0, s, o);
+            std::swap(dA, dB);
+            std::swap(dA4, dB4);
+        }
     }
 }
 
@@ -1535,6 +1601,13 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
         b->alloc(nd, s);
         FX_LAUNCH(k_fill_hash, grid_for(nd), 256, 0, s, nd, b->ptr);
     }
+    DBuf<float> v4, d4;  // FP32 smoother vectors (float4 per node), as in the V-cycle
+    if (fp32) {
+        v4.alloc(4 * (size_t)n, s);
+        d4.alloc(4 * (size_t)n, s);
+        v4.zero(s);
+        d4.zero(s);
+    }
     AmgLevel l;
     l.n = n;
     l.S0 = &S;
@@ -1545,12 +1618,14 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
         if (fp32) {
             L0Op<float> o = l0_op<float>(l, v32.ptr);
             o.v = v.ptr;
+            o.v4 = reinterpret_cast<const float4*>(v4.ptr);
             o.r = r.ptr;
             o.d_out = d.ptr;
+            o.d4_out = d4.ptr;
             o.xo = xo.ptr;
             o.c1 = 0.5;
             o.c2 = 1e-9;
-            FX_LAUNCH((k_l0_op<float, kL0ChebK>), grid, 256, 0, s, o);
+            FX_LAUNCH((k_l0_op<float, kL0ChebK, true>), grid, 256, 0, s, o);
         } else {
             L0Op<double> o = l0_op<double>(l, vals64);
             o.v = v.ptr;
@@ -1568,9 +1643,9 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
     for (int k = 0; k < reps; ++k) launch();
     const double ms = t.stop_ms(s) / reps;
     // compulsory bytes: matrix values + column indices once, row offsets, and per
-    // node the gathered direction (24 B), r read+write (48), new direction (24),
-    // iterate read+write (48) and the 3x3 block inverse (72)
-    *bytes = (double)S.n_blocks * (9.0 * (fp32 ? 4.0 : 8.0) + 4.0) + 4.0 * (n + 1) + 216.0 * n;
+    // node the gathered direction (24 B FP64 / 16 B float4), r read+write (48), the
+    // new direction (24 / 16), iterate read+write (48) and the 3x3 block inverse (72)
+    *bytes = (double)S.n_blocks * (9.0 * (fp32 ? 4.0 : 8.0) + 4.0) + 4.0 * (n + 1) + (fp32 ? 200.0 : 216.0) * n;
     return ms;
 }
 

@@ -45,6 +45,8 @@ struct AmgLevel {
     int n_agg = 0;
     // work vectors (n * bs); xs: pre-smoothed iterate of the coarse-level cycle
     DBuf<double> x, b, r, d, t, xs;
+    // fine level with FP32 smoother values: directions and the iterate as float4 per node
+    DBuf<float> d4a, d4b, x4;
     // coarsest level: dense inverse (n*bs)^2
     bool coarsest = false;
     DBuf<double> dense_inv;
