@@ -337,7 +337,7 @@ def run_batch(args, rank: int, local: int) -> None:
         torch.cuda.synchronize()
         return r, e0.elapsed_time(e1) / 1e3, time.perf_counter() - w0
 
-    o_bj = fx.solve_opts(precision=fx.PREC_MIXED, rtol=1e-8)
+    o_bj = fx.solve_opts(precision=fx.PREC_MIXED, rtol=1e-8, preconditioner=fx.PRECOND_BLOCK_JACOBI)
     for rep in range(2):  # the first pass also loads kernels and builds graphs
         ps = projects()
         (st, stats), dev_s, wall_s = timed(lambda: fx.batch_solve(ctx, ps, o_bj))
@@ -353,6 +353,16 @@ def run_batch(args, rank: int, local: int) -> None:
                                               "wall_s": wall_s,
                                               "failed": int(multi.sum_over_ranks(float(np.sum(st != 0)), "cuda")),
                                               "pcg_iterations_max": int(max(s["pcg_iterations"] for s in stats))}
+    o_amg = fx.solve_opts(rtol=1e-8)  # default: mixed multigrid (solved one system at a time inside the rounds)
+    for rep in range(2):
+        ps = projects()
+        (st_a, _), dev_s, wall_s = timed(lambda: fx.batch_solve(ctx, ps, o_amg))
+        for p in ps:
+            p.close()
+    dev_max = multi.max_over_ranks(dev_s, device="cuda")
+    out["arms"]["fx_batch_solve_mixed_amg"] = {"solves_per_s": len(pop) / dev_max, "device_s": dev_max,
+                                               "wall_s": wall_s,
+                                               "failed": int(multi.sum_over_ranks(float(np.sum(st_a != 0)), "cuda"))}
     ps = projects()
 
     def seq():

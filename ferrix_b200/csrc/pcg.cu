@@ -88,8 +88,15 @@ __device__ __forceinline__ bool cta_running(const int* status) {
 }
 
 // (A) q = K p_new, p_new = z + beta p_old (fused), partial p_new . q
+// residency and column groups in flight per lane: FP32 rows are short in bytes and
+// favour 2 CTAs of 64 registers; FP64 rows favour 1 CTA with 2 groups in flight
 template <typename T>
-__global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __restrict__ chunks,
+constexpr int pcg_min_blocks() {
+    return sizeof(T) == 8 ? 1 : 2;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSpmvThreads, pcg_min_blocks<T>()) k_pcg_spmv(const ChunkDev* __restrict__ chunks,
                                                            const InstDev<T>* __restrict__ insts, int parity) {
     __shared__ double sh[4 * 32];
     const ChunkDev ck = chunks[blockIdx.x];
@@ -110,6 +117,7 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
         const int g0 = valid ? I.goff[row] : 0;
         const int ng = valid ? I.goff[row + 1] - g0 : 0;
         T a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll(sizeof(T) == 8 ? 2 : 1)
         for (int g = sub; g < ng; g += 8) {
             int4 cc = __ldcs(reinterpret_cast<const int4*>(I.cols) + g0 + g);
             T v[9][4];

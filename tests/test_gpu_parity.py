@@ -231,6 +231,18 @@ def test_iterative_solver_reference_semantics(ctx, golden_dir):
     assert e.value.kind == "ConvergenceError"
 
 
+@pytest.mark.parametrize("case", ["one_c3d4", "one_c3d20", "c3d4_box"])
+@pytest.mark.parametrize("pc", [fx.PRECOND_BLOCK_JACOBI, fx.PRECOND_AMG])
+def test_tiny_decks_solve(ctx, case, pc):
+    """Single-element and few-element decks through the default solver and block-Jacobi (the
+    multigrid hierarchy degenerates to one aggregate, i.e. a direct solve on the rigid-body modes)."""
+    text = SMALL[case]()
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    p.steps[0].solve(1, p, st, opts=fx.solve_opts(preconditioner=pc, precision=fx.PREC_FP64))
+    assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref)
+
+
 AMG_CASES = {
     "c3d4_cantilever": lambda: decks.c3d4_cantilever(),
     "c3d20_box": lambda: decks.c3d20_box(4, 4, 16, lengths=(20.0, 20.0, 80.0)),
