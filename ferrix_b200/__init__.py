@@ -95,7 +95,8 @@ class Context:
 def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 50000, poll_interval: int = 32,
                reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
                reference_iterative: bool = False, preconditioner: int = PRECOND_AMG,
-               amg_aggregate_nodes: int = 40, amg_smoother_degree: int = 2, amg_cycle: int = 0) -> SolveOpts:
+               amg_aggregate_nodes: int = 40, amg_smoother_degree: int = 2, amg_cycle: int = 0,
+               amg_smoother: int = 0) -> SolveOpts:
     o = SolveOpts()
     _lib.load().fx_default_solve_opts(C.byref(o))
     o.precision = precision
@@ -110,6 +111,7 @@ def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 
     o.amg_aggregate_nodes = int(amg_aggregate_nodes)
     o.amg_smoother_degree = int(amg_smoother_degree)
     o.amg_cycle = int(amg_cycle)
+    o.amg_smoother = int(amg_smoother)
     return o
 
 

@@ -29,7 +29,8 @@ class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("rtol", C.c_double), ("max_iter", C.c_int), ("poll_interval", C.c_int),
                 ("reliable_delta", C.c_double), ("use_graphs", C.c_int), ("verbose", C.c_int),
                 ("reference_iterative", C.c_int), ("preconditioner", C.c_int),
-                ("amg_aggregate_nodes", C.c_int), ("amg_smoother_degree", C.c_int), ("amg_cycle", C.c_int)]
+                ("amg_aggregate_nodes", C.c_int), ("amg_smoother_degree", C.c_int), ("amg_cycle", C.c_int),
+                ("amg_smoother", C.c_int)]
 
 
 class StepStats(C.Structure):

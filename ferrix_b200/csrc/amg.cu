@@ -1386,7 +1386,21 @@ struct ChebCoef {
     double c2_start;
     double c1[8], c2[8];
 };
-static ChebCoef cheb_coef(double lmax, int degree) {
+// kind 1: fourth-kind Chebyshev smoother (Lottes, "Optimal polynomial smoothers
+// for multigrid V-cycles", Numer. Linear Algebra Appl. 2023): d_1 = 4/(3 rho)
+// D^-1 r_0, d_k = (2k-3)/(2k+1) d_{k-1} + (8k-4)/((2k+1) rho) D^-1 r_{k-1}, rho =
+// the lambda_max estimate; no lower eigenvalue bound needed.
+static ChebCoef cheb_coef(double lmax, int degree, int kind) {
+    if (kind == 1) {
+        ChebCoef k{};
+        k.c2_start = 4.0 / (3.0 * lmax);
+        for (int s = 1; s < degree; ++s) {
+            const int i = s + 1;  // step index of the recurrence (the start is step 1)
+            k.c1[s] = (2.0 * i - 3.0) / (2.0 * i + 1.0);
+            k.c2[s] = (8.0 * i - 4.0) / ((2.0 * i + 1.0) * lmax);
+        }
+        return k;
+    }
     const double lmin = lmax / 30.0;
     const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
     const double sigma = theta / delta;
@@ -1424,7 +1438,7 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
         return;
     }
     AmgLevel& c = L[lev + 1];
-    const ChebCoef k = cheb_coef(l.lmax, degree_);
+    const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_);
     const unsigned grid = grid_for((int64_t)l.n * 32);
     double* dA = l.d.ptr;
     double* dB = l.t.ptr;
@@ -1502,7 +1516,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     AmgLevel& l = L[0];
     AmgLevel& c = L[1];
     const int64_t nd = (int64_t)l.n * 3;
-    const ChebCoef k = cheb_coef(l.lmax, degree_);
+    const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_);
     const unsigned grid = l0_grid(l.n);
     // FP32 values: the smoother's gathered vectors are FP32 too (float4 per node)
     constexpr bool g32 = sizeof(VT) == 4;
@@ -1665,6 +1679,7 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     }
     amg.set_smoother(opt.amg_degree, v32);
     amg.set_cycle(opt.amg_kcycle);
+    amg.set_smoother_kind(opt.amg_cheb_kind);
     r_.alloc(nd, s);
     z_.alloc(nd, s);
     p_.alloc(nd, s);

@@ -74,6 +74,8 @@ class Amg {
     }
     // K-cycle at the first coarse level (true) or V-cycles throughout.
     void set_cycle(bool kcycle) { kcycle_ = kcycle; }
+    // Chebyshev smoother: 0 = first kind on [lmax/30, lmax], 1 = fourth kind
+    void set_smoother_kind(int kind) { cheb_kind_ = kind; }
     bool kcycle() const { return kcycle_; }
     // z = cycle(r), FP64 vectors of 3 * n_nodes. With S != null the last
     // smoothing step also reduces r.z (and r.zold when zold != null, for the
@@ -89,6 +91,7 @@ class Amg {
     void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
                  const double* zold, cudaStream_t s);
     bool kcycle_ = false;
+    int cheb_kind_ = 0;
     int degree_ = 2;
     const float* vals0_f32_ = nullptr;
     DBuf<uint8_t> tmp_;

@@ -54,6 +54,7 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->amg_aggregate_nodes = 40;
     o->amg_smoother_degree = 2;
     o->amg_cycle = 0;  // V-cycle
+    o->amg_smoother = 0;
 }
 
 int fx_ctx_create(int device, fx_ctx** out) {

@@ -543,6 +543,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         po.amg_degree = rs[0]->o.amg_smoother_degree > 0 ? rs[0]->o.amg_smoother_degree : 2;
         po.amg_fp32 = rs[0]->o.precision == FX_PREC_MIXED;
         po.amg_kcycle = rs[0]->o.amg_cycle == 1;
+        po.amg_cheb_kind = rs[0]->o.amg_smoother == 1 ? 1 : 0;
     }
     while (true) {
         bool any = false;

@@ -91,6 +91,7 @@ struct PcgOptions {
     int amg_degree = 2;       // Chebyshev smoothing steps per pre/post smoothing
     bool amg_fp32 = false;    // FP32 fine-matrix values in the level-0 smoother
     bool amg_kcycle = false;  // K-cycle at the first coarse level (flexible outer CG)
+    int amg_cheb_kind = 0;    // 0: Chebyshev of the first kind on [lmax/30, lmax], 1: fourth kind
 };
 
 template <typename T>

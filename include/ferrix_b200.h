@@ -86,6 +86,8 @@ typedef struct {
     int amg_smoother_degree; /* FX_PRECOND_AMG: Chebyshev steps per pre/post smoothing, 1..8; 0 = 2 */
     int amg_cycle;           /* FX_PRECOND_AMG: 0 = V-cycle, 1 = K-cycle at the first coarse level (two
                                 flexible-CG steps per coarse correction; the outer CG is then flexible) */
+    int amg_smoother;        /* FX_PRECOND_AMG: 0 = Chebyshev of the first kind on [lmax/30, lmax],
+                                1 = Chebyshev of the fourth kind (Lottes 2023) */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */

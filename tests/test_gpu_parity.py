@@ -264,14 +264,14 @@ def test_amg_preconditioned_solve(ctx, case, prec):
     assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref), stats
 
 
-@pytest.mark.parametrize("degree,cycle", [(1, 0), (3, 0), (2, 1), (1, 1)])
-def test_amg_smoother_degree_and_cycle(ctx, degree, cycle):
-    """Chebyshev degree and V- / K-cycle (flexible outer CG) variants against the oracle."""
+@pytest.mark.parametrize("degree,cycle,kind", [(1, 0, 0), (3, 0, 0), (2, 1, 0), (1, 1, 0), (2, 0, 1), (3, 1, 1)])
+def test_amg_smoother_degree_and_cycle(ctx, degree, cycle, kind):
+    """Chebyshev degree and kind, V- / K-cycle (flexible outer CG) variants against the oracle."""
     text = AMG_CASES["c3d20_box_3_levels"]()
     ref, _ = _oracle_run(text)
     p, st = _project(ctx, text)
     opts = fx.solve_opts(preconditioner=fx.PRECOND_AMG, amg_smoother_degree=degree, amg_aggregate_nodes=60,
-                         amg_cycle=cycle)
+                         amg_cycle=cycle, amg_smoother=kind)
     stats = p.steps[0].solve(1, p, st, opts=opts)
     assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref), stats
 
