@@ -19,6 +19,7 @@
 
 #include <charconv>
 #include <string_view>
+#include <thread>
 
 #include "common.hpp"
 #include "model.hpp"
@@ -282,8 +283,76 @@ const std::unordered_set<std::string>& keywords() {
     return k;
 }
 
+// Data blocks of *NODE and *ELEMENT (TYPE=C3D4 / C3D20), parsed ahead of the
+// keyword state machine by several threads. The state machine then applies a
+// block's rows in line order, exactly as it would apply the lines one by one; a
+// block with any line that does not parse is left to the line-by-line path,
+// which reports the error as before.
+struct PreBlock {
+    size_t begin = 0, end = 0;  // line range of the data lines
+    int npe = 0;                // 0: *NODE, 4 / 20: *ELEMENT of that type
+    bool ok = true;
+    std::vector<int64_t> ids;
+    std::vector<double> xyz;     // *NODE: 3 per line
+    std::vector<int64_t> conn;   // *ELEMENT: npe per line
+};
+
+static void preparse_block(const std::vector<std::string>& lines, PreBlock& b) {
+    const size_t n = b.end - b.begin;
+    b.ids.resize(n);
+    if (b.npe == 0) b.xyz.resize(3 * n);
+    else b.conn.resize((size_t)b.npe * n);
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nthreads = std::min<size_t>(hw, std::max<size_t>(1, n / 4096));
+    std::vector<uint8_t> bad(nthreads, 0);
+    std::vector<size_t> rows(nthreads, 0);  // non-empty lines seen per chunk
+    auto work = [&](size_t t) {
+        std::vector<std::string_view> f;
+        const size_t a = n * t / nthreads, e = n * (t + 1) / nthreads;
+        for (size_t k = a; k < e; ++k) {
+            const std::string& line = lines[b.begin + k];
+            size_t s = 0, z = line.size();
+            while (s < z && is_ws(line[s])) ++s;
+            if (s == z) {  // blank lines are skipped by the state machine: keep the block exact
+                bad[t] = 1;
+                return;
+            }
+            split_views(line, ',', f);
+            if (b.npe == 0) {
+                if (f.size() != 4 || !parse_usize_sv(f[0], &b.ids[k]) || !parse_f64_sv(f[1], &b.xyz[3 * k]) ||
+                    !parse_f64_sv(f[2], &b.xyz[3 * k + 1]) || !parse_f64_sv(f[3], &b.xyz[3 * k + 2])) {
+                    bad[t] = 1;
+                    return;
+                }
+            } else {
+                if ((int)f.size() != b.npe + 1 || !parse_usize_sv(f[0], &b.ids[k])) {
+                    bad[t] = 1;
+                    return;
+                }
+                for (int a2 = 0; a2 < b.npe; ++a2)
+                    if (!parse_usize_sv(f[a2 + 1], &b.conn[(size_t)b.npe * k + a2])) {
+                        bad[t] = 1;
+                        return;
+                    }
+            }
+            ++rows[t];
+        }
+    };
+    if (nthreads == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < nthreads; ++t) th.emplace_back(work, t);
+        for (auto& x : th) x.join();
+    }
+    for (size_t t = 0; t < nthreads; ++t)
+        if (bad[t]) b.ok = false;
+}
+
 struct Parser {
     std::vector<std::string> lines;
+    std::vector<PreBlock> blocks;  // sorted by begin
+    size_t next_block = 0;
     size_t pos = 0;
     Project p;
     std::string kw;  // current keyword ("" = none)
@@ -327,9 +396,39 @@ struct Parser {
 
     int64_t origin() const { return in_step ? step_counter : 0; }
 
+    // Applies a pre-parsed block if the state machine is in the matching keyword
+    // (what data() would do line by line); false = parse the lines one by one.
+    bool apply_block(const PreBlock& b) {
+        if (b.npe == 0) {
+            if (kw != "NODE") return false;
+            for (size_t k = 0; k < b.ids.size(); ++k)
+                p.nodes[b.ids[k]] = {b.xyz[3 * k], b.xyz[3 * k + 1], b.xyz[3 * k + 2]};
+            return true;
+        }
+        if (kw != "ELEMENT" || !has_elem_type) return false;
+        if (!((b.npe == 4 && elem_type == "C3D4") || (b.npe == 20 && elem_type == "C3D20"))) return false;
+        const ElemType t = b.npe == 4 ? ElemType::C3D4 : ElemType::C3D20;
+        auto* eset = has_elset && !elset_name.empty() ? &p.element_sets[elset_name] : nullptr;
+        for (size_t k = 0; k < b.ids.size(); ++k) {
+            if (eset) eset->push_back(b.ids[k]);
+            ElementRec r;
+            r.type = t;
+            r.nodes.assign(b.conn.begin() + (size_t)b.npe * k, b.conn.begin() + (size_t)b.npe * (k + 1));
+            p.elements[b.ids[k]] = std::move(r);
+        }
+        return true;
+    }
+
     void run() {
         while (pos < lines.size()) {
             line_nr = (int64_t)pos + 1;
+            while (next_block < blocks.size() && blocks[next_block].begin < pos) ++next_block;
+            if (next_block < blocks.size() && blocks[next_block].begin == pos && blocks[next_block].ok &&
+                apply_block(blocks[next_block])) {
+                pos = blocks[next_block].end;
+                ++next_block;
+                continue;
+            }
             const std::string& line = lines[pos++];
             if (!line.empty() && line[0] == '*') {
                 keyword(line);
@@ -670,6 +769,31 @@ Project parse_inp(const std::string& text) {
         if (nl == std::string::npos) break;
         start = nl + 1;
     }
+    // *NODE / *ELEMENT data blocks: keyword line followed by data lines up to the next keyword
+    for (size_t i = 0; i < ps.lines.size(); ++i) {
+        const std::string& l = ps.lines[i];
+        if (l.empty() || l[0] != '*') continue;
+        size_t e = i + 1;
+        while (e < ps.lines.size() && !(!ps.lines[e].empty() && ps.lines[e][0] == '*')) ++e;
+        if (e - i - 1 < 1024) continue;  // small blocks: line by line
+        std::string name = trim(l.substr(1, l.find(',') == std::string::npos ? std::string::npos : l.find(',') - 1));
+        std::replace(name.begin(), name.end(), ' ', '_');
+        PreBlock b;
+        b.begin = i + 1;
+        b.end = e;
+        if (name == "NODE") {
+            b.npe = 0;
+        } else if (name == "ELEMENT") {
+            KwArgs ka = keyword_arguments(l);
+            const std::string* t = kw_value(ka, "TYPE");
+            if (!t || (*t != "C3D4" && *t != "C3D20")) continue;
+            b.npe = *t == "C3D4" ? 4 : 20;
+        } else {
+            continue;
+        }
+        ps.blocks.push_back(std::move(b));
+    }
+    for (auto& b : ps.blocks) preparse_block(ps.lines, b);
     ps.run();
     return std::move(ps.p);
 }

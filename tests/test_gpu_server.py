@@ -85,3 +85,42 @@ def test_failed_request_reports_its_error_and_the_loop_continues():
         assert r["status"] == 0 and np.all(np.isfinite(u))
     finally:
         srv.close()
+
+
+def test_wait_with_a_short_limit_reports_not_finished():
+    """Failure detection on the host: a wait that runs out returns FX_TIMEOUT and the ticket stays valid."""
+    srv = fx.Server(0, slots=1)
+    try:
+        big = _host_project(decks.c3d20_box(10, 10, 40))
+        t = srv.submit(big)
+        with pytest.raises(fx.FerrixError) as e:
+            srv.wait(t, timeout=0.0)
+        assert e.value.kind == "Timeout"
+        u, r = srv.wait(t, timeout=600.0)
+        assert r["status"] == 0 and np.all(np.isfinite(u))
+    finally:
+        srv.close()
+    big.close()
+
+
+def test_closing_the_server_cancels_queued_requests_and_models_stay_usable():
+    texts = _pool()[:6]
+    projs = [_host_project(t) for t in texts]
+    srv = fx.Server(0, slots=1)
+    for p in projs:
+        srv.submit(p)
+    srv.close()  # finishes the running request, cancels the rest
+    # every model is unbound again and can be served by a new loop
+    out = _serve_projects(projs, 2)
+    assert all(r["status"] == 0 for _, r in out)
+    for p in projs:
+        p.close()
+
+
+def _serve_projects(projs, slots):
+    srv = fx.Server(0, slots=slots)
+    try:
+        tickets = [srv.submit(p) for p in projs]
+        return [srv.wait(t, timeout=600.0) for t in tickets]
+    finally:
+        srv.close()
