@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""Benchmark of the linear-static C3D20 solve (the north-star workload).
+"""Benchmark of the linear-static C3D20 solve (the headline workload); further modes
+time batched decks, the serving loop and the NLGEOM beam.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64|fp64_csr]
                     [--preconditioner amg|bj]
