@@ -969,23 +969,30 @@ __global__ void __launch_bounds__(256) k_ln_op(LnOp o) {
             src6[0] = o.r[o6 + c];
         }
     }
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int blk = o.row_ptr[row] + lane; blk < o.row_ptr[row + 1]; blk += 32) {
-        const double* vb = o.vals + (int64_t)blk * 36;
-        const double* xx = o.v + 6 * (int64_t)o.cols[blk];
-        double xv[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) xv[k] = xx[k];
-#pragma unroll
-        for (int r = 0; r < 6; ++r) {
-            double t = 0.0;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) t += vb[r * 6 + k] * xv[k];
-            acc[r] += t;
+    // 30 lanes walk (block, block row) items: lane l always handles block row l % 6
+    // of blocks l / 6 + 5 m, so consecutive lanes read consecutive 48-B block rows
+    const int b0 = o.row_ptr[row], items = 6 * (o.row_ptr[row + 1] - b0);
+    double t = 0.0;
+    if (lane < 30)
+        for (int it = lane; it < items; it += 30) {
+            const int kb = it / 6;
+            const int64_t blk = b0 + kb;
+            const double2* vr = reinterpret_cast<const double2*>(o.vals + blk * 36 + (it - 6 * kb) * 6);
+            const double* xx = o.v + 6 * (int64_t)o.cols[blk];
+            const double2 a0 = vr[0], a1 = vr[1], a2 = vr[2];
+            t += a0.x * xx[0] + a0.y * xx[1] + a1.x * xx[2] + a1.y * xx[3] + a2.x * xx[4] + a2.y * xx[5];
         }
-    }
+    // lanes r, r+6, ..., r+24 hold block-row r partial sums: fixed-order tree into lanes 0..5
+    // (a source lane past 31 returns the caller's own value, hence the lane conditions)
+    double u = __shfl_down_sync(0xffffffffu, t, 24);
+    if (lane < 8) t += u;  // lanes 0..5 += 24..29 (6, 7 += 30, 31, which carry 0)
+    u = __shfl_down_sync(0xffffffffu, t, 12);
+    if (lane < 12) t += u;  // lanes 0..11 += 12..23
+    u = __shfl_down_sync(0xffffffffu, t, 6);
+    if (lane < 6) t += u;  // lanes 0..5 += 6..11
+    double acc[6];
 #pragma unroll
-    for (int r = 0; r < 6; ++r) acc[r] = warp_sum(acc[r]);
+    for (int r = 0; r < 6; ++r) acc[r] = __shfl_sync(0xffffffffu, t, r);
     double axc = acc[0];
 #pragma unroll
     for (int r = 1; r < 6; ++r)
