@@ -499,11 +499,12 @@ __global__ void __launch_bounds__(256) k_panel_trailing(int nd, int k0, int b, d
     for (int j0 = 0; j0 < nd; j0 += 32) {  // uniform trip count: all lanes reach the shuffles
         const int j = j0 + lane;
         const bool valid = j < nd && !(j >= k0 && j < k0 + b);
+        double pk[kPanel];  // the panel rows' column j, all loads issued before the sum
+#pragma unroll
+        for (int t = 0; t < kPanel; ++t) pk[t] = (valid && t < b) ? A[(int64_t)(k0 + t) * nd + j] : 0.0;
         double acc = 0.0;
-        for (int t = 0; t < b; ++t) {
-            const double at = __shfl_sync(0xffffffffu, a, t);
-            if (valid) acc += at * A[(int64_t)(k0 + t) * nd + j];
-        }
+#pragma unroll
+        for (int t = 0; t < kPanel; ++t) acc += __shfl_sync(0xffffffffu, a, t) * pk[t];  // a = 0 for t >= b
         if (valid) Ai[j] -= acc;
     }
     double acc = 0.0;
@@ -1174,14 +1175,22 @@ static void dot_dev(const double* a, const double* b, int64_t n, DBuf<double>& r
 
 // Largest eigenvalue of D^-1 A by 12 power iterations from a fixed hashed start
 // vector, normalised on the device; one host read at the end.
-static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s) {
+// (vals32: FP32 copy of the fine matrix, used for the products at level 0 when given)
+static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const float* vals32) {
     const int64_t nd = (int64_t)l.n * l.bs;
     const int nb = 296;
     FX_LAUNCH(k_fill_hash, grid_for(nd), 256, 0, s, nd, l.x.ptr);
     dot_dev(l.x.ptr, l.x.ptr, nd, red, s);
     FX_LAUNCH(k_normalize, grid_for(nd), 256, 0, s, nd, red.ptr + nb, l.x.ptr, l.x.ptr);
     for (int it = 0; it < 12; ++it) {
-        level_spmv(l, l.x.ptr, nullptr, l.t.ptr, s);  // t = A x, |x| = 1
+        if (l.S0 && vals32) {  // t = A x, |x| = 1
+            L0Op<float> o = l0_op<float>(l, vals32);
+            o.v = l.x.ptr;
+            o.y = l.t.ptr;
+            FX_LAUNCH((k_l0_op<float, kL0Resid>), l0_grid(l.n), 256, 0, s, o);
+        } else {
+            level_spmv(l, l.x.ptr, nullptr, l.t.ptr, s);
+        }
         FX_LAUNCH(k_cheb_init, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv_ptr(), l.t.ptr, l.d.ptr, l.r.ptr, 1.0,
                   1);  // d = D^-1 A x
         dot_dev(l.d.ptr, l.d.ptr, nd, red, s);
@@ -1253,7 +1262,7 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
             stream_wait(s, "amg coarse inverse");
             break;
         }
-        estimate_lmax(l, red_, s);
+        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr);
         // ---- aggregation by cells
         DBuf<uint64_t> keys, keys_s;
         DBuf<int32_t> ids, ids_s, head, rank1;
@@ -1676,7 +1685,6 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     const int n = S.n_rows;
     const int64_t nd = 3 * (int64_t)n;
     if (opt.amg_degree < 1 || opt.amg_degree > 8) fail(FX_INVALID_ARGUMENT, "multigrid smoother degree must be 1..8");
-    amg.setup(S, vals64, dinv64, xyz, n, cell0, s, st);
     const float* v32 = nullptr;
     if (opt.amg_fp32) {
         const int64_t nv = (int64_t)S.n_groups * 36;
@@ -1684,7 +1692,8 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         FX_LAUNCH(k_f64_to_f32, 148 * 8, 256, 0, s, nv, vals64, vals32_.ptr);
         v32 = vals32_.ptr;
     }
-    amg.set_smoother(opt.amg_degree, v32);
+    amg.set_smoother(opt.amg_degree, v32);  // before setup: its eigenvalue estimate uses v32
+    amg.setup(S, vals64, dinv64, xyz, n, cell0, s, st);
     amg.set_cycle(opt.amg_kcycle);
     amg.set_smoother_kind(opt.amg_cheb_kind);
     r_.alloc(nd, s);
