@@ -164,8 +164,8 @@ void fx_model_destroy(fx_model* m) {
 
 int fx_model_sizes(const fx_model* m, int64_t* nn, int64_t* ne, int* ns, int* nm) {
     if (!m) return FX_INVALID_ARGUMENT;
-    if (nn) *nn = (int64_t)m->project.nodes.size();
-    if (ne) *ne = (int64_t)m->project.elements.size();
+    if (nn) *nn = m->project.n_nodes();
+    if (ne) *ne = m->project.n_elements();
     if (ns) *ns = (int)m->project.steps.size();
     if (nm) *nm = (int)m->project.materials.size();
     return FX_OK;

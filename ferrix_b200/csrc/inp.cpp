@@ -97,7 +97,7 @@ static bool parse_usize(const std::string& s, int64_t* out) {
 
 // Allocation-free forms for the bulk data lines (*NODE, *ELEMENT): fields as
 // views into the line, trimmed like trim().
-static void split_views(const std::string& s, char sep, std::vector<std::string_view>& out) {
+static void split_views(std::string_view s, char sep, std::vector<std::string_view>& out) {
     out.clear();
     size_t start = 0;
     for (size_t i = 0; i <= s.size(); ++i) {
@@ -220,36 +220,85 @@ double Record::eval(const SolverTime& t, int64_t current_step) const {  // ampli
 
 // ------------------------------------------------------------------ preprocess
 
-std::string preprocess_inp(const std::string& text) {  // parser.rs:903-921
-    std::string out;
-    out.resize(text.size() + 1);
-    size_t w = 0;  // write position (the output is never longer than the input plus one)
-    size_t start = 0;
-    const size_t n = text.size();
-    while (start <= n) {
-        size_t nl = text.find('\n', start);
-        size_t end = nl == std::string::npos ? n : nl;
-        if (nl == std::string::npos && start == n) break;
-        size_t a = start, b = end;
+// Trimmed, comment-free, upper-cased lines of text[begin, end) (a range of
+// whole lines) appended at out + w; a line ending in ',' is joined to the next
+// by a space. Returns the new write position.
+static size_t preprocess_range(const std::string& text, size_t begin, size_t end, char* out, size_t w) {
+    size_t start = begin;
+    while (start < end) {
+        const void* hit = std::memchr(text.data() + start, '\n', end - start);
+        const size_t nl = hit ? (size_t)((const char*)hit - text.data()) : end;
+        size_t a = start, b = nl;
         while (a < b && is_ws(text[a])) ++a;
         while (b > a && is_ws(text[b - 1])) --b;
-        if (a < b) {
-            bool comment = b - a >= 2 && text[a] == '*' && text[a + 1] == '*';
-            if (!comment) {
-                for (size_t k = a; k < b; ++k) {
-                    const char c = text[k];
-                    out[w++] = (c >= 'a' && c <= 'z') ? (char)(c - 'a' + 'A') : c;  // ASCII to_uppercase
-                }
-                out[w++] = text[b - 1] == ',' ? ' ' : '\n';
+        if (a < b && !(b - a >= 2 && text[a] == '*' && text[a + 1] == '*')) {
+            const char* src = text.data() + a;
+            char* dst = out + w;
+            const size_t len = b - a;
+            for (size_t k = 0; k < len; ++k) {  // ASCII to_uppercase (a loop the compiler vectorises)
+                const char c = src[k];
+                dst[k] = (c >= 'a' && c <= 'z') ? (char)(c - 'a' + 'A') : c;
             }
+            w += len;
+            out[w++] = text[b - 1] == ',' ? ' ' : '\n';
         }
-        if (nl == std::string::npos) break;
         start = nl + 1;
     }
-    out.resize(w);
-    // substitute_ccx_solvers (parser.rs:930-942)
+    return w;
+}
+
+std::string preprocess_inp(const std::string& text) {  // parser.rs:903-921
+    // Lines are independent: chunks of whole lines are processed on several
+    // threads into separate buffers and concatenated in order.
+    const size_t n = text.size();
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nthreads = std::min<size_t>(hw, std::max<size_t>(1, n / (1u << 20)));
+    std::vector<size_t> cut(nthreads + 1, n);
+    cut[0] = 0;
+    for (size_t t = 1; t < nthreads; ++t) {  // chunk t starts after the first newline at or past n t / nthreads
+        size_t c = std::max(cut[t - 1], n * t / nthreads);
+        const void* hit = c < n ? std::memchr(text.data() + c, '\n', n - c) : nullptr;
+        cut[t] = hit ? (size_t)((const char*)hit - text.data()) + 1 : n;
+    }
+    // Chunk t writes its output at its own input offset cut[t] (a chunk's output
+    // is never longer than its input, except the last one's by the final
+    // newline); the chunks are then moved down to close the gaps.
+    std::string out;
+    out.resize(n + 1);
+    // substitute_ccx_solvers (parser.rs:930-942) patterns: looked for per chunk
+    // (and across the chunk seams below); replaced only where present.
     static const char* pats[] = {"ITERATIVE CHOLESKY", "ITERATIVE SCALING", "PASTIX", "PARDISO", "SPOOLES"};
     static const char* reps[] = {"ITERATIVE", "ITERATIVE", "DIRECT", "DIRECT", "DIRECT"};
+    constexpr size_t kMaxPat = 18;
+    std::vector<size_t> len(nthreads, 0);
+    std::vector<uint8_t> hit_pat(nthreads, 0);
+    auto work = [&](size_t t) {
+        len[t] = preprocess_range(text, cut[t], cut[t + 1], &out[0], cut[t]) - cut[t];
+        const std::string_view v(out.data() + cut[t], len[t]);
+        for (const char* q : pats)
+            if (v.find(q) != std::string_view::npos) hit_pat[t] = 1;
+    };
+    if (nthreads == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (size_t t = 1; t < nthreads; ++t) th.emplace_back(work, t);
+        work(0);
+        for (auto& x : th) x.join();
+    }
+    bool any = hit_pat[0] != 0;
+    size_t w = len[0];
+    for (size_t t = 1; t < nthreads; ++t) {
+        if (w != cut[t]) std::memmove(&out[w], &out[cut[t]], len[t]);
+        const size_t a = w > kMaxPat ? w - kMaxPat : 0;  // a pattern may span the seam at w
+        w += len[t];
+        const std::string_view seam(out.data() + a, std::min(w, a + 2 * kMaxPat) - a);
+        for (const char* q : pats)
+            if (seam.find(q) != std::string_view::npos) any = true;
+        if (hit_pat[t]) any = true;
+    }
+    out.resize(w);
+    if (!any) return out;
     for (int k = 0; k < 5; ++k) {
         if (out.find(pats[k]) == std::string::npos) continue;  // nothing to replace: keep the string
         std::string r;
@@ -297,7 +346,7 @@ struct PreBlock {
     std::vector<int64_t> conn;   // *ELEMENT: npe per line
 };
 
-static void preparse_block(const std::vector<std::string>& lines, PreBlock& b) {
+static void preparse_block(const std::vector<std::string_view>& lines, PreBlock& b) {
     const size_t n = b.end - b.begin;
     b.ids.resize(n);
     if (b.npe == 0) b.xyz.resize(3 * n);
@@ -310,7 +359,7 @@ static void preparse_block(const std::vector<std::string>& lines, PreBlock& b) {
         std::vector<std::string_view> f;
         const size_t a = n * t / nthreads, e = n * (t + 1) / nthreads;
         for (size_t k = a; k < e; ++k) {
-            const std::string& line = lines[b.begin + k];
+            const std::string_view line = lines[b.begin + k];
             size_t s = 0, z = line.size();
             while (s < z && is_ws(line[s])) ++s;
             if (s == z) {  // blank lines are skipped by the state machine: keep the block exact
@@ -350,7 +399,15 @@ static void preparse_block(const std::vector<std::string>& lines, PreBlock& b) {
 }
 
 struct Parser {
-    std::vector<std::string> lines;
+    // Lines of the preprocessed text as views; a line becomes a std::string only
+    // when the state machine reads it (not for pre-parsed *NODE / *ELEMENT blocks).
+    std::string text;
+    std::vector<std::string_view> views;
+    std::vector<std::string> cache;
+    const std::string& line_at(size_t i) {
+        if (cache[i].size() != views[i].size()) cache[i].assign(views[i]);
+        return cache[i];
+    }
     std::vector<PreBlock> blocks;  // sorted by begin
     size_t next_block = 0;
     size_t pos = 0;
@@ -369,7 +426,7 @@ struct Parser {
     [[noreturn]] void perr(const std::string& msg) {
         fail(FX_PARSE, "Parsing error at line " + std::to_string(line_nr) + ": " + msg);
     }
-    const std::string* peek() const { return pos < lines.size() ? &lines[pos] : nullptr; }
+    const std::string* peek() { return pos < views.size() ? &line_at(pos) : nullptr; }
 
     void finish_step() {
         cur.loads = step_loads;
@@ -401,26 +458,29 @@ struct Parser {
     bool apply_block(const PreBlock& b) {
         if (b.npe == 0) {
             if (kw != "NODE") return false;
-            for (size_t k = 0; k < b.ids.size(); ++k)
-                p.nodes[b.ids[k]] = {b.xyz[3 * k], b.xyz[3 * k + 1], b.xyz[3 * k + 2]};
+            p.node_line_ids.insert(p.node_line_ids.end(), b.ids.begin(), b.ids.end());
+            const size_t at = p.node_line_xyz.size();
+            p.node_line_xyz.resize(at + b.ids.size());
+            std::memcpy(p.node_line_xyz[at].data(), b.xyz.data(), b.xyz.size() * sizeof(double));
             return true;
         }
         if (kw != "ELEMENT" || !has_elem_type) return false;
         if (!((b.npe == 4 && elem_type == "C3D4") || (b.npe == 20 && elem_type == "C3D20"))) return false;
-        const ElemType t = b.npe == 4 ? ElemType::C3D4 : ElemType::C3D20;
-        auto* eset = has_elset && !elset_name.empty() ? &p.element_sets[elset_name] : nullptr;
-        for (size_t k = 0; k < b.ids.size(); ++k) {
-            if (eset) eset->push_back(b.ids[k]);
-            ElementRec r;
-            r.type = t;
-            r.nodes.assign(b.conn.begin() + (size_t)b.npe * k, b.conn.begin() + (size_t)b.npe * (k + 1));
-            p.elements[b.ids[k]] = std::move(r);
+        if (has_elset && !elset_name.empty()) {
+            auto& eset = p.element_sets[elset_name];
+            eset.insert(eset.end(), b.ids.begin(), b.ids.end());
         }
+        const int64_t off0 = (int64_t)p.elem_line_conn.size();
+        p.elem_line_ids.insert(p.elem_line_ids.end(), b.ids.begin(), b.ids.end());
+        p.elem_line_npe.insert(p.elem_line_npe.end(), b.ids.size(), (uint8_t)b.npe);
+        p.elem_line_off.reserve(p.elem_line_off.size() + b.ids.size());
+        for (size_t k = 0; k < b.ids.size(); ++k) p.elem_line_off.push_back(off0 + (int64_t)(b.npe * k));
+        p.elem_line_conn.insert(p.elem_line_conn.end(), b.conn.begin(), b.conn.end());
         return true;
     }
 
     void run() {
-        while (pos < lines.size()) {
+        while (pos < views.size()) {
             line_nr = (int64_t)pos + 1;
             while (next_block < blocks.size() && blocks[next_block].begin < pos) ++next_block;
             if (next_block < blocks.size() && blocks[next_block].begin == pos && blocks[next_block].ok &&
@@ -429,7 +489,7 @@ struct Parser {
                 ++next_block;
                 continue;
             }
-            const std::string& line = lines[pos++];
+            const std::string& line = line_at(pos++);
             if (!line.empty() && line[0] == '*') {
                 keyword(line);
                 continue;
@@ -444,13 +504,7 @@ struct Parser {
             data(t);
         }
         if (in_step) finish_step();
-        std::vector<int64_t> ids;
-        ids.reserve(p.nodes.size());
-        for (auto& kv : p.nodes) ids.push_back(kv.first);
-        std::sort(ids.begin(), ids.end());
-        p.index_to_node_id = ids;
-        p.node_id_to_index.reserve(ids.size());
-        for (size_t i = 0; i < ids.size(); ++i) p.node_id_to_index[ids[i]] = (int64_t)i;
+        p.resolve_mesh();
     }
 
     void keyword(const std::string& line) {
@@ -510,7 +564,7 @@ struct Parser {
             if (midx < 0) fail(FX_MATERIAL_NOT_FOUND, "Material " + *mn + " not found");
             auto it = p.element_sets.find(*es);
             if (it == p.element_sets.end()) fail(FX_ELSET_NOT_FOUND, "Elset " + *es + " not found");
-            for (int64_t eid : it->second) p.element_materials[eid] = midx;
+            for (int64_t eid : it->second) p.elem_material_lines.emplace_back(eid, midx);
         } else if (key == "STEP") {
             if (step_counter == 0) {
                 step_loads = p.initial_loads;
@@ -659,7 +713,8 @@ struct Parser {
             if (fields.size() != 4 || !parse_usize_sv(fields[0], &id) || !parse_f64_sv(fields[1], &x[0]) ||
                 !parse_f64_sv(fields[2], &x[1]) || !parse_f64_sv(fields[3], &x[2]))
                 perr("Invalid node definition: " + line);
-            p.nodes[id] = x;
+            p.node_line_ids.push_back(id);
+            p.node_line_xyz.push_back(x);
         } else if (kw == "ELEMENT") {
             if (!has_elem_type) return;
             split_views(line, ',', fields);
@@ -671,18 +726,17 @@ struct Parser {
                 nums.push_back(v);
             }
             int npe;
-            ElemType t;
-            if (elem_type == "C3D4") { npe = 4; t = ElemType::C3D4; }
-            else if (elem_type == "C3D20") { npe = 20; t = ElemType::C3D20; }
+            if (elem_type == "C3D4") npe = 4;
+            else if (elem_type == "C3D20") npe = 20;
             else fail(FX_PARSE, "Parsing error at line 0: Unknown element definition: " + elem_type);
             if ((int)nums.size() - 1 != npe)
                 fail(FX_PARSE, "Parsing error at line 0: Wrong node count for " + elem_type);
             int64_t eid = nums[0];
             if (has_elset && !elset_name.empty()) p.element_sets[elset_name].push_back(eid);
-            ElementRec r;
-            r.type = t;
-            r.nodes.assign(nums.begin() + 1, nums.end());
-            p.elements[eid] = std::move(r);
+            p.elem_line_ids.push_back(eid);
+            p.elem_line_npe.push_back((uint8_t)npe);
+            p.elem_line_off.push_back((int64_t)p.elem_line_conn.size());
+            p.elem_line_conn.insert(p.elem_line_conn.end(), nums.begin() + 1, nums.end());
         } else if (kw == "NSET" || kw == "ELSET") {
             if (!has_set || is_generate) return;
             std::vector<int64_t> ids;
@@ -756,27 +810,31 @@ struct Parser {
 }  // namespace
 
 Project parse_inp(const std::string& text) {
-    std::string pre = preprocess_inp(text);
     Parser ps;
+    ps.text = preprocess_inp(text);
     // str::lines semantics
+    const std::string& pre = ps.text;
     size_t start = 0;
     while (start < pre.size()) {
-        size_t nl = pre.find('\n', start);
-        size_t end = nl == std::string::npos ? pre.size() : nl;
-        std::string l = pre.substr(start, end - start);
-        if (!l.empty() && l.back() == '\r') l.pop_back();
-        ps.lines.push_back(std::move(l));
-        if (nl == std::string::npos) break;
-        start = nl + 1;
+        const void* hit = std::memchr(pre.data() + start, '\n', pre.size() - start);
+        size_t end = hit ? (size_t)((const char*)hit - pre.data()) : pre.size();
+        size_t e2 = end;
+        if (e2 > start && pre[e2 - 1] == '\r') --e2;
+        ps.views.emplace_back(pre.data() + start, e2 - start);
+        if (!hit) break;
+        start = end + 1;
     }
+    ps.cache.resize(ps.views.size());
     // *NODE / *ELEMENT data blocks: keyword line followed by data lines up to the next keyword
-    for (size_t i = 0; i < ps.lines.size(); ++i) {
-        const std::string& l = ps.lines[i];
+    const auto& V = ps.views;
+    for (size_t i = 0; i < V.size(); ++i) {
+        const std::string_view l = V[i];
         if (l.empty() || l[0] != '*') continue;
         size_t e = i + 1;
-        while (e < ps.lines.size() && !(!ps.lines[e].empty() && ps.lines[e][0] == '*')) ++e;
+        while (e < V.size() && !(!V[e].empty() && V[e][0] == '*')) ++e;
         if (e - i - 1 < 1024) continue;  // small blocks: line by line
-        std::string name = trim(l.substr(1, l.find(',') == std::string::npos ? std::string::npos : l.find(',') - 1));
+        const std::string kl(l);
+        std::string name = trim(kl.substr(1, kl.find(',') == std::string::npos ? std::string::npos : kl.find(',') - 1));
         std::replace(name.begin(), name.end(), ' ', '_');
         PreBlock b;
         b.begin = i + 1;
@@ -784,7 +842,7 @@ Project parse_inp(const std::string& text) {
         if (name == "NODE") {
             b.npe = 0;
         } else if (name == "ELEMENT") {
-            KwArgs ka = keyword_arguments(l);
+            KwArgs ka = keyword_arguments(kl);
             const std::string* t = kw_value(ka, "TYPE");
             if (!t || (*t != "C3D4" && *t != "C3D20")) continue;
             b.npe = *t == "C3D4" ? 4 : 20;
@@ -793,41 +851,113 @@ Project parse_inp(const std::string& text) {
         }
         ps.blocks.push_back(std::move(b));
     }
-    for (auto& b : ps.blocks) preparse_block(ps.lines, b);
+    for (auto& b : ps.blocks) preparse_block(ps.views, b);
     ps.run();
     return std::move(ps.p);
 }
 
+void IdIndex::build(const std::vector<int64_t>& ids) {
+    table.clear();
+    map.clear();
+    count = (int64_t)ids.size();
+    base = ids.empty() ? 0 : ids.front();
+    if (ids.empty() || ids.back() - base == count - 1) {  // ascending and unique: consecutive
+        mode = 0;
+        return;
+    }
+    const int64_t span = ids.back() - base + 1;
+    if (span <= 8 * count + 4096) {
+        mode = 1;
+        table.assign((size_t)span, -1);
+        for (int64_t i = 0; i < count; ++i) table[(size_t)(ids[(size_t)i] - base)] = (int32_t)i;
+        return;
+    }
+    mode = 2;
+    map.reserve((size_t)count);
+    for (int64_t i = 0; i < count; ++i) map[ids[(size_t)i]] = i;
+}
+
+// Ascending unique ids of `line_ids` with, for each, the last line that defines
+// it (what repeated map inserts in line order leave behind).
+static void last_definitions(const std::vector<int64_t>& line_ids, std::vector<int64_t>& ids,
+                             std::vector<int64_t>& line) {
+    const size_t n = line_ids.size();
+    bool ascending = true;
+    for (size_t i = 1; i < n && ascending; ++i) ascending = line_ids[i] > line_ids[i - 1];
+    ids.clear();
+    line.clear();
+    if (ascending) {
+        ids = line_ids;
+        line.resize(n);
+        for (size_t i = 0; i < n; ++i) line[i] = (int64_t)i;
+        return;
+    }
+    std::vector<int64_t> perm(n);
+    for (size_t i = 0; i < n; ++i) perm[i] = (int64_t)i;
+    std::stable_sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return line_ids[a] < line_ids[b]; });
+    ids.reserve(n);
+    line.reserve(n);
+    for (size_t k = 0; k < n; ++k) {
+        const int64_t id = line_ids[(size_t)perm[k]];
+        if (!ids.empty() && ids.back() == id) line.back() = perm[k];  // a later line of the same id
+        else {
+            ids.push_back(id);
+            line.push_back(perm[k]);
+        }
+    }
+}
+
+void Project::resolve_mesh() {
+    std::vector<int64_t> nline;
+    last_definitions(node_line_ids, index_to_node_id, nline);
+    node_xyz.resize(nline.size());
+    if (nline.size() == node_line_xyz.size()) node_xyz.swap(node_line_xyz);  // no repeats: identity
+    else
+        for (size_t i = 0; i < nline.size(); ++i) node_xyz[i] = node_line_xyz[(size_t)nline[i]];
+    node_index.build(index_to_node_id);
+    last_definitions(elem_line_ids, elem_ids, elem_line);
+}
+
 DenseModel build_dense(const Project& p) {
     DenseModel d;
-    d.n_nodes = (int64_t)p.index_to_node_id.size();
+    d.n_nodes = p.n_nodes();
     d.xyz.resize(3 * d.n_nodes);
-    for (int64_t i = 0; i < d.n_nodes; ++i) {
-        const auto& x = p.nodes.at(p.index_to_node_id[i]);
-        d.xyz[3 * i] = x[0];
-        d.xyz[3 * i + 1] = x[1];
-        d.xyz[3 * i + 2] = x[2];
+    if (d.n_nodes) std::memcpy(d.xyz.data(), p.node_xyz.data(), d.xyz.size() * sizeof(double));
+    // material of every element (ascending id order): the last assignment wins
+    const int64_t ne = p.n_elements();
+    IdIndex eindex;
+    eindex.build(p.elem_ids);
+    std::vector<int32_t> mat((size_t)ne, -1);
+    for (const auto& em : p.elem_material_lines) {
+        const int64_t k = eindex.find(em.first);
+        if (k >= 0) mat[(size_t)k] = em.second;
     }
-    std::vector<int64_t> ids;
-    ids.reserve(p.elements.size());
-    for (auto& kv : p.elements) ids.push_back(kv.first);
-    std::sort(ids.begin(), ids.end());
     d.g4.npe = 4;
     d.g20.npe = 20;
-    for (int64_t eid : ids) {
-        const ElementRec& r = p.elements.at(eid);
-        ElemGroup& g = r.type == ElemType::C3D4 ? d.g4 : d.g20;
-        g.elem_ids.push_back(eid);
-        for (int64_t nid : r.nodes) {
-            int64_t idx = p.index_of(nid);
+    int64_t n4 = 0;
+    for (int64_t k = 0; k < ne; ++k) n4 += p.elem_line_npe[(size_t)p.elem_line[(size_t)k]] == 4;
+    for (ElemGroup* g : {&d.g4, &d.g20}) {
+        const int64_t m = g == &d.g4 ? n4 : ne - n4;
+        g->elem_ids.reserve((size_t)m);
+        g->conn.reserve((size_t)m * g->npe);
+        g->mat.reserve((size_t)m);
+    }
+    for (int64_t k = 0; k < ne; ++k) {
+        const size_t line = (size_t)p.elem_line[(size_t)k];
+        const int npe = p.elem_line_npe[line];
+        ElemGroup& g = npe == 4 ? d.g4 : d.g20;
+        g.elem_ids.push_back(p.elem_ids[(size_t)k]);
+        const int64_t* nodes = &p.elem_line_conn[(size_t)p.elem_line_off[line]];
+        for (int a = 0; a < npe; ++a) {
+            const int64_t nid = nodes[a];
+            const int64_t idx = p.index_of(nid);
             if (idx < 0 && d.missing_node_id < 0) {
                 d.missing_node_id = nid;
                 d.missing_node_error = "Node " + std::to_string(nid) + " not found in mesh";
             }
             g.conn.push_back((int32_t)(idx < 0 ? 0 : idx));
         }
-        auto it = p.element_materials.find(eid);
-        g.mat.push_back(it == p.element_materials.end() ? -1 : it->second);
+        g.mat.push_back(mat[(size_t)k]);
     }
     // mesh volume: tets exactly; bricks as 6 Kuhn tets of their 8 corner nodes
     auto tet_vol = [&](int a, int b, int c, int e) {

@@ -69,32 +69,53 @@ struct StaticStep {
     bool nlgeom = false;
 };
 
-enum class ElemType : int { C3D4 = 4, C3D20 = 20 };
-
-struct ElementRec {
-    ElemType type;
-    std::vector<int64_t> nodes;
+// Id -> position in an ascending list of unique ids: arithmetic when the ids
+// are consecutive, a direct table when they are dense enough, a hash map
+// otherwise. -1 when absent.
+struct IdIndex {
+    int64_t base = 0, count = 0;
+    int mode = 0;  // 0 consecutive, 1 table, 2 map
+    std::vector<int32_t> table;
+    std::unordered_map<int64_t, int64_t> map;
+    void build(const std::vector<int64_t>& sorted_ids);
+    int64_t find(int64_t id) const {
+        if (mode == 0) return id >= base && id - base < count ? id - base : -1;
+        if (mode == 1) return id >= base && id - base < (int64_t)table.size() ? table[(size_t)(id - base)] : -1;
+        auto it = map.find(id);
+        return it == map.end() ? -1 : it->second;
+    }
 };
 
 struct Project {
-    std::unordered_map<int64_t, std::array<double, 3>> nodes;
-    std::unordered_map<int64_t, ElementRec> elements;
+    // *NODE / *ELEMENT lines in deck order. A line whose id was seen before
+    // replaces the earlier definition (the reference inserts into maps keyed by
+    // id); resolve_mesh() applies that and sorts by id.
+    std::vector<int64_t> node_line_ids;
+    std::vector<std::array<double, 3>> node_line_xyz;
+    std::vector<int64_t> elem_line_ids;
+    std::vector<uint8_t> elem_line_npe;  // 4 (C3D4) or 20 (C3D20)
+    std::vector<int64_t> elem_line_off;  // first node of the line in elem_line_conn
+    std::vector<int64_t> elem_line_conn;
+    // *SOLID_SECTION assignments (element id, material index) in deck order; the last one wins.
+    std::vector<std::pair<int64_t, int>> elem_material_lines;
     std::unordered_map<std::string, std::vector<int64_t>> node_sets, element_sets;
     std::vector<Material> materials;
-    std::unordered_map<int64_t, int> element_materials;
     std::vector<StaticStep> steps;
     std::vector<Record> initial_loads, initial_bcs;
     std::unordered_map<int64_t, double> initial_temperatures;
     double default_initial_temperature = 0.0;
     std::vector<std::string> nodal_output, element_output;
     std::unordered_map<std::string, std::shared_ptr<const Amplitude>> amplitudes;
-    // Mesh::build_node_mappings (mesh.rs:35-50)
+    // Resolved mesh (Mesh::build_node_mappings, mesh.rs:35-50): node index =
+    // rank of the node id; elements in ascending id with their defining line.
     std::vector<int64_t> index_to_node_id;
-    std::unordered_map<int64_t, int64_t> node_id_to_index;
-    int64_t index_of(int64_t id) const {
-        auto it = node_id_to_index.find(id);
-        return it == node_id_to_index.end() ? -1 : it->second;
-    }
+    std::vector<std::array<double, 3>> node_xyz;
+    std::vector<int64_t> elem_ids, elem_line;
+    IdIndex node_index;
+    int64_t index_of(int64_t id) const { return node_index.find(id); }
+    int64_t n_nodes() const { return (int64_t)index_to_node_id.size(); }
+    int64_t n_elements() const { return (int64_t)elem_ids.size(); }
+    void resolve_mesh();
 };
 
 // Preprocess + parse (parser.rs:111-147, 903-942). Throws fx::Error.

@@ -68,6 +68,74 @@ def test_parser_matches_oracle_on_synthetic_decks():
     _compare(decks.c3d4_nlgeom_beam(4, 2, 2))
 
 
+def _relabel(text, node_id, elem_id, seed):
+    """The same deck with node / element ids mapped through node_id / elem_id, the
+    *NODE and *ELEMENT lines shuffled, one node and one element defined twice (the
+    later definition must win) and the volume elset assigned a material twice."""
+    rng = np.random.default_rng(seed)
+    out, block, kw = [], [], None
+
+    def flush():
+        if kw in ("NODE", "ELEMENT") and block:
+            order = rng.permutation(len(block))
+            rows = [block[i] for i in order]
+            first = rows[0].split(",")
+            if kw == "NODE":  # redefine a node: moved by 1e-3 in x
+                rows.append(", ".join([first[0], repr(float(first[1]) + 1e-3)] + first[2:]))
+            else:  # redefine an element with its nodes rotated (C3D4: 1, 2, 3, 4 -> 1, 3, 4, 2)
+                f = [x.strip() for x in first]
+                rows.append(", ".join(f[:2] + f[3:5] + [f[2]] + f[5:]))
+            out.extend(rows)
+        else:
+            out.extend(block)
+        block.clear()
+
+    for line in text.splitlines():
+        if line.startswith("*"):
+            flush()
+            kw = line[1:].split(",")[0].strip().upper() if not line.startswith("**") else kw
+            out.append(line)
+            if line.upper().startswith("*SOLID SECTION"):
+                out.append(line)
+            continue
+        f = [x.strip() for x in line.split(",")]
+        if kw == "NODE":
+            f[0] = str(node_id(int(f[0])))
+        elif kw == "ELEMENT":
+            f = [str(elem_id(int(f[0])))] + [str(node_id(int(x))) for x in f[1:] if x]
+        elif kw == "NSET":
+            f = [str(node_id(int(x))) if x.isdigit() else x for x in f if x]
+        elif kw == "ELSET":
+            f = [str(elem_id(int(x))) if x.isdigit() else x for x in f if x]
+        block.append(", ".join(f))
+    flush()
+    return "\n".join(out) + "\n"
+
+
+@pytest.mark.parametrize("node_id,elem_id", [
+    (lambda i: i, lambda e: e),                      # consecutive ids, shuffled lines
+    (lambda i: 3 * i + 5, lambda e: 2 * e + 1),      # gaps: direct table
+    (lambda i: 100003 * i, lambda e: 7919 * e),      # sparse: hash map
+], ids=["consecutive", "gaps", "sparse"])
+def test_parser_id_layouts_match_oracle(node_id, elem_id):
+    """Bulk *NODE / *ELEMENT blocks (over 1,024 lines) with shuffled, gapped and
+    repeated ids parse to the oracle's arrays (nodes by ascending id, later
+    definitions winning)."""
+    text = _relabel(decks.c3d4_cantilever(8, 8, 40), node_id, elem_id, seed=3)
+    p, o = _compare(text)
+    assert p.num_nodes == 9 * 9 * 41 and p.num_elements == 8 * 8 * 40 * 6
+
+
+def test_preprocess_chunks_match_oracle():
+    """A deck of several MB (the preprocessor splits it into chunks on several
+    threads) with a solver name to substitute at its very end."""
+    text = decks.c3d20_box(14, 14, 30)
+    assert len(text) > 2 << 20
+    text = text.replace("*Static, Solver=Spooles", "*Static, Solver=Iterative Cholesky")
+    p, o = _compare(text)
+    assert p.steps[0].info.solver == "ITERATIVE"
+
+
 QUIRKS = """** comment
 *Heading
 title line
