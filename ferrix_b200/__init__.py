@@ -211,7 +211,7 @@ class Project:
     @classmethod
     def from_inp_text(cls, text: str, ctx: Optional[Context] = None) -> "Project":
         lib = _lib.load()
-        raw = text.encode()
+        raw = bytes(text) if isinstance(text, (bytes, bytearray, memoryview)) else text.encode()
         h = C.c_void_p()
         _check(lib.fx_model_from_inp(ctx.handle if ctx else None, raw, len(raw), C.byref(h)), ctx)
         return cls(h, ctx)

@@ -247,76 +247,117 @@ static size_t preprocess_range(const std::string& text, size_t begin, size_t end
     return w;
 }
 
-std::string preprocess_inp(const std::string& text) {  // parser.rs:903-921
-    // Lines are independent: chunks of whole lines are processed on several
-    // threads into separate buffers and concatenated in order.
+// substitute_ccx_solvers (parser.rs:930-942)
+static const char* const kSolverPats[] = {"ITERATIVE CHOLESKY", "ITERATIVE SCALING", "PASTIX", "PARDISO", "SPOOLES"};
+static const char* const kSolverReps[] = {"ITERATIVE", "ITERATIVE", "DIRECT", "DIRECT", "DIRECT"};
+
+// Replaces every solver name in buf[0, len) in pattern order, in place (no
+// replacement is longer than its pattern); returns the new length.
+static size_t substitute_solvers(char* buf, size_t len) {
+    for (int k = 0; k < 5; ++k) {
+        const std::string_view pat(kSolverPats[k]), rep(kSolverReps[k]);
+        size_t r = std::string_view(buf, len).find(pat);
+        if (r == std::string_view::npos) continue;
+        size_t w = r;
+        while (r != std::string_view::npos) {
+            std::memmove(buf + w, rep.data(), rep.size());
+            w += rep.size();
+            size_t from = r + pat.size();
+            r = std::string_view(buf, len).find(pat, from);
+            const size_t stop = r == std::string_view::npos ? len : r;
+            std::memmove(buf + w, buf + from, stop - from);
+            w += stop - from;
+        }
+        len = w;
+    }
+    return len;
+}
+
+// Appends the str::lines views of text[a, b) (trailing '\r' dropped) to `lines`.
+static void split_lines(const char* text, size_t a, size_t b, std::string_view* lines) {
+    size_t k = 0;
+    while (a < b) {
+        const void* hit = std::memchr(text + a, '\n', b - a);
+        const size_t end = hit ? (size_t)((const char*)hit - text) : b;
+        size_t e2 = end;
+        if (e2 > a && text[e2 - 1] == '\r') --e2;
+        lines[k++] = std::string_view(text + a, e2 - a);
+        a = end + 1;
+    }
+}
+
+static size_t count_lines(const char* text, size_t a, size_t b) {
+    size_t k = 0;
+    while (a < b) {
+        const void* hit = std::memchr(text + a, '\n', b - a);
+        ++k;
+        if (!hit) break;
+        a = (size_t)((const char*)hit - text) + 1;
+    }
+    return k;
+}
+
+// True when the input line ending at the newline `nl` is kept by the
+// preprocessor (not blank, not a comment) and does not end in ',' (so no
+// logical line continues past it).
+static bool ends_logical_line(const std::string& text, size_t lo, size_t nl) {
+    size_t a = nl;
+    while (a > lo && text[a - 1] != '\n') --a;
+    size_t b = nl;
+    while (a < b && is_ws(text[a])) ++a;
+    while (b > a && is_ws(text[b - 1])) --b;
+    if (a == b) return false;
+    if (b - a >= 2 && text[a] == '*' && text[a + 1] == '*') return false;
+    return text[b - 1] != ',';
+}
+
+// Lines of the preprocessed text (parser.rs:903-942 followed by str::lines) as
+// views into `store`. The input is cut into chunks only after lines that end a
+// logical line, so every output line, and every solver name, lies inside one
+// chunk: each thread preprocesses its chunk into its own region of `store`,
+// substitutes the solver names there, and then indexes that region's lines.
+static void preprocess_lines(const std::string& text, std::unique_ptr<char[]>& store,
+                             std::vector<std::string_view>& lines) {
     const size_t n = text.size();
     const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     const size_t nthreads = std::min<size_t>(hw, std::max<size_t>(1, n / (1u << 20)));
     std::vector<size_t> cut(nthreads + 1, n);
     cut[0] = 0;
-    for (size_t t = 1; t < nthreads; ++t) {  // chunk t starts after the first newline at or past n t / nthreads
-        size_t c = std::max(cut[t - 1], n * t / nthreads);
-        const void* hit = c < n ? std::memchr(text.data() + c, '\n', n - c) : nullptr;
-        cut[t] = hit ? (size_t)((const char*)hit - text.data()) + 1 : n;
-    }
-    // Chunk t writes its output at its own input offset cut[t] (a chunk's output
-    // is never longer than its input, except the last one's by the final
-    // newline); the chunks are then moved down to close the gaps.
-    std::string out;
-    out.resize(n + 1);
-    // substitute_ccx_solvers (parser.rs:930-942) patterns: looked for per chunk
-    // (and across the chunk seams below); replaced only where present.
-    static const char* pats[] = {"ITERATIVE CHOLESKY", "ITERATIVE SCALING", "PASTIX", "PARDISO", "SPOOLES"};
-    static const char* reps[] = {"ITERATIVE", "ITERATIVE", "DIRECT", "DIRECT", "DIRECT"};
-    constexpr size_t kMaxPat = 18;
-    std::vector<size_t> len(nthreads, 0);
-    std::vector<uint8_t> hit_pat(nthreads, 0);
-    auto work = [&](size_t t) {
-        len[t] = preprocess_range(text, cut[t], cut[t + 1], &out[0], cut[t]) - cut[t];
-        const std::string_view v(out.data() + cut[t], len[t]);
-        for (const char* q : pats)
-            if (v.find(q) != std::string_view::npos) hit_pat[t] = 1;
-    };
-    if (nthreads == 1) {
-        work(0);
-    } else {
-        std::vector<std::thread> th;
-        for (size_t t = 1; t < nthreads; ++t) th.emplace_back(work, t);
-        work(0);
-        for (auto& x : th) x.join();
-    }
-    bool any = hit_pat[0] != 0;
-    size_t w = len[0];
     for (size_t t = 1; t < nthreads; ++t) {
-        if (w != cut[t]) std::memmove(&out[w], &out[cut[t]], len[t]);
-        const size_t a = w > kMaxPat ? w - kMaxPat : 0;  // a pattern may span the seam at w
-        w += len[t];
-        const std::string_view seam(out.data() + a, std::min(w, a + 2 * kMaxPat) - a);
-        for (const char* q : pats)
-            if (seam.find(q) != std::string_view::npos) any = true;
-        if (hit_pat[t]) any = true;
-    }
-    out.resize(w);
-    if (!any) return out;
-    for (int k = 0; k < 5; ++k) {
-        if (out.find(pats[k]) == std::string::npos) continue;  // nothing to replace: keep the string
-        std::string r;
-        r.reserve(out.size());
-        size_t pos = 0, plen = std::strlen(pats[k]);
-        while (true) {
-            size_t f = out.find(pats[k], pos);
-            if (f == std::string::npos) {
-                r.append(out, pos, std::string::npos);
+        size_t c = std::max(cut[t - 1], n * t / nthreads);
+        cut[t] = n;
+        while (c < n) {
+            const void* hit = std::memchr(text.data() + c, '\n', n - c);
+            if (!hit) break;
+            const size_t nl = (size_t)((const char*)hit - text.data());
+            if (ends_logical_line(text, cut[t - 1], nl)) {
+                cut[t] = nl + 1;
                 break;
             }
-            r.append(out, pos, f - pos);
-            r.append(reps[k]);
-            pos = f + plen;
+            c = nl + 1;
         }
-        out.swap(r);
     }
-    return out;
+    store.reset(new char[n + 1]);  // a chunk's output is never longer than its input (+1 for the last)
+    char* out = store.get();
+    std::vector<size_t> len(nthreads, 0), nlines(nthreads, 0), first(nthreads + 1, 0);
+    auto run = [&](auto&& fn) {
+        if (nthreads == 1) {
+            fn((size_t)0);
+            return;
+        }
+        std::vector<std::thread> th;
+        for (size_t t = 1; t < nthreads; ++t) th.emplace_back(fn, t);
+        fn((size_t)0);
+        for (auto& x : th) x.join();
+    };
+    run([&](size_t t) {
+        len[t] = preprocess_range(text, cut[t], cut[t + 1], out, cut[t]) - cut[t];
+        len[t] = substitute_solvers(out + cut[t], len[t]);
+        nlines[t] = count_lines(out, cut[t], cut[t] + len[t]);
+    });
+    for (size_t t = 0; t < nthreads; ++t) first[t + 1] = first[t] + nlines[t];
+    lines.resize(first[nthreads]);
+    run([&](size_t t) { split_lines(out, cut[t], cut[t] + len[t], lines.data() + first[t]); });
 }
 
 // ------------------------------------------------------------------ parser
@@ -341,15 +382,15 @@ struct PreBlock {
     size_t begin = 0, end = 0;  // line range of the data lines
     int npe = 0;                // 0: *NODE, 4 / 20: *ELEMENT of that type
     bool ok = true;
-    std::vector<int64_t> ids;
-    std::vector<double> xyz;     // *NODE: 3 per line
-    std::vector<int64_t> conn;   // *ELEMENT: npe per line
+    RawVec<int64_t> ids;
+    RawVec<std::array<double, 3>> xyz;  // *NODE
+    RawVec<int64_t> conn;               // *ELEMENT: npe per line
 };
 
 static void preparse_block(const std::vector<std::string_view>& lines, PreBlock& b) {
     const size_t n = b.end - b.begin;
     b.ids.resize(n);
-    if (b.npe == 0) b.xyz.resize(3 * n);
+    if (b.npe == 0) b.xyz.resize(n);
     else b.conn.resize((size_t)b.npe * n);
     const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     const size_t nthreads = std::min<size_t>(hw, std::max<size_t>(1, n / 4096));
@@ -368,8 +409,8 @@ static void preparse_block(const std::vector<std::string_view>& lines, PreBlock&
             }
             split_views(line, ',', f);
             if (b.npe == 0) {
-                if (f.size() != 4 || !parse_usize_sv(f[0], &b.ids[k]) || !parse_f64_sv(f[1], &b.xyz[3 * k]) ||
-                    !parse_f64_sv(f[2], &b.xyz[3 * k + 1]) || !parse_f64_sv(f[3], &b.xyz[3 * k + 2])) {
+                if (f.size() != 4 || !parse_usize_sv(f[0], &b.ids[k]) || !parse_f64_sv(f[1], &b.xyz[k][0]) ||
+                    !parse_f64_sv(f[2], &b.xyz[k][1]) || !parse_f64_sv(f[3], &b.xyz[k][2])) {
                     bad[t] = 1;
                     return;
                 }
@@ -401,12 +442,13 @@ static void preparse_block(const std::vector<std::string_view>& lines, PreBlock&
 struct Parser {
     // Lines of the preprocessed text as views; a line becomes a std::string only
     // when the state machine reads it (not for pre-parsed *NODE / *ELEMENT blocks).
-    std::string text;
+    std::unique_ptr<char[]> store;
     std::vector<std::string_view> views;
-    std::vector<std::string> cache;
+    std::unordered_map<size_t, std::string> cache;  // references stay valid as it grows
     const std::string& line_at(size_t i) {
-        if (cache[i].size() != views[i].size()) cache[i].assign(views[i]);
-        return cache[i];
+        auto it = cache.find(i);
+        if (it == cache.end()) it = cache.emplace(i, std::string(views[i])).first;
+        return it->second;
     }
     std::vector<PreBlock> blocks;  // sorted by begin
     size_t next_block = 0;
@@ -455,13 +497,16 @@ struct Parser {
 
     // Applies a pre-parsed block if the state machine is in the matching keyword
     // (what data() would do line by line); false = parse the lines one by one.
-    bool apply_block(const PreBlock& b) {
+    bool apply_block(PreBlock& b) {
         if (b.npe == 0) {
             if (kw != "NODE") return false;
-            p.node_line_ids.insert(p.node_line_ids.end(), b.ids.begin(), b.ids.end());
-            const size_t at = p.node_line_xyz.size();
-            p.node_line_xyz.resize(at + b.ids.size());
-            std::memcpy(p.node_line_xyz[at].data(), b.xyz.data(), b.xyz.size() * sizeof(double));
+            if (p.node_line_ids.empty()) {  // the usual single *NODE block: take the arrays
+                p.node_line_ids.swap(b.ids);
+                p.node_line_xyz.swap(b.xyz);
+            } else {
+                p.node_line_ids.insert(p.node_line_ids.end(), b.ids.begin(), b.ids.end());
+                p.node_line_xyz.insert(p.node_line_xyz.end(), b.xyz.begin(), b.xyz.end());
+            }
             return true;
         }
         if (kw != "ELEMENT" || !has_elem_type) return false;
@@ -471,11 +516,17 @@ struct Parser {
             eset.insert(eset.end(), b.ids.begin(), b.ids.end());
         }
         const int64_t off0 = (int64_t)p.elem_line_conn.size();
-        p.elem_line_ids.insert(p.elem_line_ids.end(), b.ids.begin(), b.ids.end());
-        p.elem_line_npe.insert(p.elem_line_npe.end(), b.ids.size(), (uint8_t)b.npe);
-        p.elem_line_off.reserve(p.elem_line_off.size() + b.ids.size());
-        for (size_t k = 0; k < b.ids.size(); ++k) p.elem_line_off.push_back(off0 + (int64_t)(b.npe * k));
-        p.elem_line_conn.insert(p.elem_line_conn.end(), b.conn.begin(), b.conn.end());
+        const size_t m = b.ids.size(), at = p.elem_line_off.size();
+        p.elem_line_npe.insert(p.elem_line_npe.end(), m, (uint8_t)b.npe);
+        p.elem_line_off.resize(at + m);
+        for (size_t k = 0; k < m; ++k) p.elem_line_off[at + k] = off0 + (int64_t)(b.npe * k);
+        if (p.elem_line_ids.empty()) {  // the first bulk *ELEMENT block: take the arrays
+            p.elem_line_ids.swap(b.ids);
+            p.elem_line_conn.swap(b.conn);
+        } else {
+            p.elem_line_ids.insert(p.elem_line_ids.end(), b.ids.begin(), b.ids.end());
+            p.elem_line_conn.insert(p.elem_line_conn.end(), b.conn.begin(), b.conn.end());
+        }
         return true;
     }
 
@@ -811,20 +862,7 @@ struct Parser {
 
 Project parse_inp(const std::string& text) {
     Parser ps;
-    ps.text = preprocess_inp(text);
-    // str::lines semantics
-    const std::string& pre = ps.text;
-    size_t start = 0;
-    while (start < pre.size()) {
-        const void* hit = std::memchr(pre.data() + start, '\n', pre.size() - start);
-        size_t end = hit ? (size_t)((const char*)hit - pre.data()) : pre.size();
-        size_t e2 = end;
-        if (e2 > start && pre[e2 - 1] == '\r') --e2;
-        ps.views.emplace_back(pre.data() + start, e2 - start);
-        if (!hit) break;
-        start = end + 1;
-    }
-    ps.cache.resize(ps.views.size());
+    preprocess_lines(text, ps.store, ps.views);
     // *NODE / *ELEMENT data blocks: keyword line followed by data lines up to the next keyword
     const auto& V = ps.views;
     for (size_t i = 0; i < V.size(); ++i) {
@@ -879,7 +917,7 @@ void IdIndex::build(const std::vector<int64_t>& ids) {
 
 // Ascending unique ids of `line_ids` with, for each, the last line that defines
 // it (what repeated map inserts in line order leave behind).
-static void last_definitions(const std::vector<int64_t>& line_ids, std::vector<int64_t>& ids,
+static void last_definitions(const RawVec<int64_t>& line_ids, std::vector<int64_t>& ids,
                              std::vector<int64_t>& line) {
     const size_t n = line_ids.size();
     bool ascending = true;
@@ -887,7 +925,7 @@ static void last_definitions(const std::vector<int64_t>& line_ids, std::vector<i
     ids.clear();
     line.clear();
     if (ascending) {
-        ids = line_ids;
+        ids.assign(line_ids.begin(), line_ids.end());
         line.resize(n);
         for (size_t i = 0; i < n; ++i) line[i] = (int64_t)i;
         return;

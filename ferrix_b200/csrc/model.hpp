@@ -10,9 +10,35 @@
 #include <memory>
 #include <string>
 #include <unordered_map>
+#include <utility>
 #include <vector>
 
 namespace fx {
+
+// Allocator whose resize() leaves new elements default-initialised (not
+// zeroed): bulk arrays are sized by one thread and filled by several, each
+// touching its own pages first.
+template <class T>
+struct RawAlloc : std::allocator<T> {
+    using value_type = T;
+    template <class U>
+    struct rebind {
+        using other = RawAlloc<U>;
+    };
+    RawAlloc() = default;
+    template <class U>
+    RawAlloc(const RawAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using RawVec = std::vector<T, RawAlloc<T>>;
 
 // TemperatureDependentLUT (material.rs:14-69): sorted (T, v) pairs.
 struct Lut {
@@ -90,12 +116,12 @@ struct Project {
     // *NODE / *ELEMENT lines in deck order. A line whose id was seen before
     // replaces the earlier definition (the reference inserts into maps keyed by
     // id); resolve_mesh() applies that and sorts by id.
-    std::vector<int64_t> node_line_ids;
-    std::vector<std::array<double, 3>> node_line_xyz;
-    std::vector<int64_t> elem_line_ids;
-    std::vector<uint8_t> elem_line_npe;  // 4 (C3D4) or 20 (C3D20)
-    std::vector<int64_t> elem_line_off;  // first node of the line in elem_line_conn
-    std::vector<int64_t> elem_line_conn;
+    RawVec<int64_t> node_line_ids;
+    RawVec<std::array<double, 3>> node_line_xyz;
+    RawVec<int64_t> elem_line_ids;
+    RawVec<uint8_t> elem_line_npe;  // 4 (C3D4) or 20 (C3D20)
+    RawVec<int64_t> elem_line_off;  // first node of the line in elem_line_conn
+    RawVec<int64_t> elem_line_conn;
     // *SOLID_SECTION assignments (element id, material index) in deck order; the last one wins.
     std::vector<std::pair<int64_t, int>> elem_material_lines;
     std::unordered_map<std::string, std::vector<int64_t>> node_sets, element_sets;
@@ -109,7 +135,7 @@ struct Project {
     // Resolved mesh (Mesh::build_node_mappings, mesh.rs:35-50): node index =
     // rank of the node id; elements in ascending id with their defining line.
     std::vector<int64_t> index_to_node_id;
-    std::vector<std::array<double, 3>> node_xyz;
+    RawVec<std::array<double, 3>> node_xyz;
     std::vector<int64_t> elem_ids, elem_line;
     IdIndex node_index;
     int64_t index_of(int64_t id) const { return node_index.find(id); }
@@ -119,7 +145,6 @@ struct Project {
 };
 
 // Preprocess + parse (parser.rs:111-147, 903-942). Throws fx::Error.
-std::string preprocess_inp(const std::string& text);
 Project parse_inp(const std::string& text);
 
 // Dense form: node index = rank of node id; one group per element type.
