@@ -96,7 +96,7 @@ def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 
                reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
                reference_iterative: bool = False, preconditioner: int = PRECOND_AMG,
                amg_aggregate_nodes: int = 40, amg_smoother_degree: int = 2, amg_cycle: int = 0,
-               amg_smoother: int = 0) -> SolveOpts:
+               amg_smoother: int = 0, amg_overcorrect: float = 0.0, amg_cheb_ratio: float = 0.0) -> SolveOpts:
     o = SolveOpts()
     _lib.load().fx_default_solve_opts(C.byref(o))
     o.precision = precision
@@ -112,6 +112,8 @@ def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 
     o.amg_smoother_degree = int(amg_smoother_degree)
     o.amg_cycle = int(amg_cycle)
     o.amg_smoother = int(amg_smoother)
+    o.amg_overcorrect = float(amg_overcorrect)
+    o.amg_cheb_ratio = float(amg_cheb_ratio)
     return o
 
 

@@ -30,7 +30,7 @@ class SolveOpts(C.Structure):
                 ("reliable_delta", C.c_double), ("use_graphs", C.c_int), ("verbose", C.c_int),
                 ("reference_iterative", C.c_int), ("preconditioner", C.c_int),
                 ("amg_aggregate_nodes", C.c_int), ("amg_smoother_degree", C.c_int), ("amg_cycle", C.c_int),
-                ("amg_smoother", C.c_int)]
+                ("amg_smoother", C.c_int), ("amg_overcorrect", C.c_double), ("amg_cheb_ratio", C.c_double)]
 
 
 class StepStats(C.Structure):

@@ -391,7 +391,7 @@ __global__ void k_restrict(int na, const int32_t* __restrict__ ptr, const int32_
 }
 
 __global__ void k_prolong(int ndof, int bs, const int32_t* __restrict__ agg, const double* __restrict__ Q,
-                          const double* __restrict__ xc, double* __restrict__ xf) {
+                          const double* __restrict__ xc, double* __restrict__ xf, double alpha) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ndof) return;
     int j = k / bs;
@@ -399,7 +399,7 @@ __global__ void k_prolong(int ndof, int bs, const int32_t* __restrict__ agg, con
     const double* x = xc + (int64_t)agg[j] * 6;
     double t = 0.0;
     for (int c = 0; c < 6; ++c) t += q[c] * x[c];
-    xf[k] += t;
+    xf[k] += alpha * t;
 }
 
 // ------------------------------------------------------------------ coarsest level
@@ -1060,7 +1060,8 @@ __global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const do
 
 // fine level: x += Q xc (3 rows per node) and the FP32 copy of x for the smoother gathers
 __global__ void k_prolong0(int n, const int32_t* __restrict__ agg, const double* __restrict__ Q,
-                           const double* __restrict__ xc, double* __restrict__ xf, float4* __restrict__ x4) {
+                           const double* __restrict__ xc, double* __restrict__ xf, float4* __restrict__ x4,
+                           double alpha) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double* x = xc + (int64_t)agg[i] * 6;
@@ -1069,7 +1070,7 @@ __global__ void k_prolong0(int n, const int32_t* __restrict__ agg, const double*
         const double* q = Q + (3 * (int64_t)i + k) * 6;
         double t = 0.0;
         for (int c = 0; c < 6; ++c) t += q[c] * x[c];
-        out[k] = xf[3 * (int64_t)i + k] + t;
+        out[k] = xf[3 * (int64_t)i + k] + alpha * t;
         xf[3 * (int64_t)i + k] = out[k];
     }
     x4[i] = make_float4((float)out[0], (float)out[1], (float)out[2], 0.0f);
@@ -1406,7 +1407,7 @@ struct ChebCoef {
 // for multigrid V-cycles", Numer. Linear Algebra Appl. 2023): d_1 = 4/(3 rho)
 // D^-1 r_0, d_k = (2k-3)/(2k+1) d_{k-1} + (8k-4)/((2k+1) rho) D^-1 r_{k-1}, rho =
 // the lambda_max estimate; no lower eigenvalue bound needed.
-static ChebCoef cheb_coef(double lmax, int degree, int kind) {
+static ChebCoef cheb_coef(double lmax, int degree, int kind, double ratio) {
     if (kind == 1) {
         ChebCoef k{};
         k.c2_start = 4.0 / (3.0 * lmax);
@@ -1417,7 +1418,7 @@ static ChebCoef cheb_coef(double lmax, int degree, int kind) {
         }
         return k;
     }
-    const double lmin = lmax / 30.0;
+    const double lmin = lmax / ratio;
     const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
     const double sigma = theta / delta;
     ChebCoef k{};
@@ -1454,7 +1455,7 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
         return;
     }
     AmgLevel& c = L[lev + 1];
-    const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_);
+    const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
     const unsigned grid = grid_for((int64_t)l.n * 32);
     double* dA = l.d.ptr;
     double* dB = l.t.ptr;
@@ -1480,7 +1481,7 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
     FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs,
               l.Q.ptr, l.r.ptr, c.b.ptr);
     coarse(lev + 1, s);
-    FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, l.bs, l.agg.ptr, l.Q.ptr, c.x.ptr, xs);
+    FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, l.bs, l.agg.ptr, l.Q.ptr, c.x.ptr, xs, alpha_);
     {
         LnOp o = ln_op(l);
         o.v = xs;
@@ -1532,7 +1533,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     AmgLevel& l = L[0];
     AmgLevel& c = L[1];
     const int64_t nd = (int64_t)l.n * 3;
-    const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_);
+    const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
     const unsigned grid = l0_grid(l.n);
     // FP32 values: the smoother's gathered vectors are FP32 too (float4 per node)
     constexpr bool g32 = sizeof(VT) == 4;
@@ -1571,8 +1572,8 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
               l.Q.ptr, l.r.ptr, c.b.ptr);
     coarse(1, s);
-    if (g32) FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4);
-    else FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr);
+    if (g32) FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4, alpha_);
+    else FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, alpha_);
     for (int st = 0; st < degree_; ++st) {
         L0Op<VT> o = op();
         o.b = b;
@@ -1696,6 +1697,8 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     amg.setup(S, vals64, dinv64, xyz, n, cell0, s, st);
     amg.set_cycle(opt.amg_kcycle);
     amg.set_smoother_kind(opt.amg_cheb_kind);
+    amg.set_overcorrect(opt.amg_overcorrect);
+    amg.set_cheb_ratio(opt.amg_cheb_ratio);
     r_.alloc(nd, s);
     z_.alloc(nd, s);
     p_.alloc(nd, s);

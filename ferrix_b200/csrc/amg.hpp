@@ -76,6 +76,9 @@ class Amg {
     void set_cycle(bool kcycle) { kcycle_ = kcycle; }
     // Chebyshev smoother: 0 = first kind on [lmax/30, lmax], 1 = fourth kind
     void set_smoother_kind(int kind) { cheb_kind_ = kind; }
+    // coarse corrections x += alpha P e; first-kind Chebyshev interval [lmax / ratio, lmax]
+    void set_overcorrect(double alpha) { alpha_ = alpha; }
+    void set_cheb_ratio(double ratio) { cheb_ratio_ = ratio; }
     bool kcycle() const { return kcycle_; }
     // z = cycle(r), FP64 vectors of 3 * n_nodes. With S != null the last
     // smoothing step also reduces r.z (and r.zold when zold != null, for the
@@ -92,6 +95,7 @@ class Amg {
                  const double* zold, cudaStream_t s);
     bool kcycle_ = false;
     int cheb_kind_ = 0;
+    double alpha_ = 1.0, cheb_ratio_ = 30.0;
     int degree_ = 2;
     const float* vals0_f32_ = nullptr;
     DBuf<uint8_t> tmp_;

@@ -55,6 +55,8 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->amg_smoother_degree = 2;
     o->amg_cycle = 0;  // V-cycle
     o->amg_smoother = 0;
+    o->amg_overcorrect = 0.0;
+    o->amg_cheb_ratio = 0.0;
 }
 
 int fx_ctx_create(int device, fx_ctx** out) {
@@ -112,7 +114,7 @@ int fx_model_from_inp(fx_ctx* ctx, const char* text, size_t len, fx_model** out)
         fx_model* m = new fx_model();
         m->ctx = ctx;
         try {
-            m->project = parse_inp(std::string(text ? text : "", len));
+            m->project = parse_inp(std::string_view(text ? text : "", len));
         } catch (...) {
             delete m;
             throw;

@@ -63,12 +63,53 @@ static void upload_mats(const MatTableHost& h, MatTableDev& d, cudaStream_t s) {
     d.n_mat = (int)h.tref.size();
 }
 
+// Element pair buffers and the symbolic sort per element, BSR3 values (FP64 +
+// FP32), column indices and the slot map per block, vectors and the multigrid
+// hierarchy per node. Blocks per element: 240 for C3D20 and 2.8 for C3D4
+// bricks-of-tets meshes (node pairs shared by neighbouring elements counted once).
+double model_footprint(const DenseModel& D) {
+    const double e20 = (double)D.g20.size(), e4 = (double)D.g4.size(), n = (double)D.n_nodes;
+    const double blocks = 240.0 * e20 + 2.8 * e4;
+    return e20 * 32.0e3 + e4 * 1.6e3 + blocks * 120.0 + n * 1.0e3 + 64.0e6;
+}
+
+// The pool is grown here, up front, because a pool that grows while kernels
+// of other streams are in flight stalled all of them (requests of 7k DOF took
+// 0.3-0.5 s instead of 10 ms in a four-slot request loop on B200); growing it
+// by one allocation before any work is queued cost about 12 ms per GB.
+void reserve_pool(int device, cudaStream_t s, double bytes) {
+    if (!(bytes > 0.0)) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    uint64_t keep = UINT64_MAX, reserved = 0, used = 0;  // the pool keeps freed memory (fx_ctx_create sets the same)
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    const double spare = (double)reserved - (double)used;
+    if (spare >= bytes) return;
+    const size_t granule = (size_t)2 << 20;
+    const size_t want = ((size_t)(bytes - spare) + granule - 1) / granule * granule;
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, want, s) != cudaSuccess) {
+        cudaGetLastError();  // not enough memory in one piece: the pool grows on demand instead
+        return;
+    }
+    cudaFreeAsync(p, s);
+}
+
 void upload_model(fx_model* m) {
     ensure_dense(m);
     ModelDev& d = m->dev;
     if (d.uploaded) return;
     cudaStream_t s = m->ctx->stream;
     const DenseModel& D = m->dense;
+    reserve_pool(m->ctx->device, s, model_footprint(D));
     d.xyz.upload(D.xyz, s);
     d.conn4.upload(D.g4.conn, s);
     d.mat4.upload(D.g4.mat, s);
@@ -544,6 +585,9 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         po.amg_fp32 = rs[0]->o.precision == FX_PREC_MIXED;
         po.amg_kcycle = rs[0]->o.amg_cycle == 1;
         po.amg_cheb_kind = rs[0]->o.amg_smoother == 1 ? 1 : 0;
+        const double oc = rs[0]->o.amg_overcorrect;
+        po.amg_overcorrect = oc > 0.0 && oc < 2.0 ? oc : kAmgOvercorrect;
+        po.amg_cheb_ratio = rs[0]->o.amg_cheb_ratio > 1.0 ? rs[0]->o.amg_cheb_ratio : kAmgChebRatio;
     }
     while (true) {
         bool any = false;

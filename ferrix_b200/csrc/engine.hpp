@@ -99,6 +99,13 @@ inline int guarded(fx_ctx* ctx, F&& f) {
 namespace fx {
 
 void ensure_dense(fx_model* m);
+// Device bytes of one model while it is solved (an upper estimate).
+double model_footprint(const DenseModel& D);
+// Grows the device's stream-ordered memory pool (which keeps what it holds) so
+// that it has `bytes` more than it has in use, by one allocation queued on `s`
+// and freed again, before the caller queues any work. Best effort: a failed
+// allocation leaves the pool as it was.
+void reserve_pool(int device, cudaStream_t s, double bytes);
 void upload_model(fx_model* m);
 void ensure_structure(fx_model* m);
 void state_initialize(fx_model* m);

@@ -223,7 +223,7 @@ double Record::eval(const SolverTime& t, int64_t current_step) const {  // ampli
 // Trimmed, comment-free, upper-cased lines of text[begin, end) (a range of
 // whole lines) appended at out + w; a line ending in ',' is joined to the next
 // by a space. Returns the new write position.
-static size_t preprocess_range(const std::string& text, size_t begin, size_t end, char* out, size_t w) {
+static size_t preprocess_range(std::string_view text, size_t begin, size_t end, char* out, size_t w) {
     size_t start = begin;
     while (start < end) {
         const void* hit = std::memchr(text.data() + start, '\n', end - start);
@@ -300,7 +300,7 @@ static size_t count_lines(const char* text, size_t a, size_t b) {
 // True when the input line ending at the newline `nl` is kept by the
 // preprocessor (not blank, not a comment) and does not end in ',' (so no
 // logical line continues past it).
-static bool ends_logical_line(const std::string& text, size_t lo, size_t nl) {
+static bool ends_logical_line(std::string_view text, size_t lo, size_t nl) {
     size_t a = nl;
     while (a > lo && text[a - 1] != '\n') --a;
     size_t b = nl;
@@ -316,7 +316,7 @@ static bool ends_logical_line(const std::string& text, size_t lo, size_t nl) {
 // logical line, so every output line, and every solver name, lies inside one
 // chunk: each thread preprocesses its chunk into its own region of `store`,
 // substitutes the solver names there, and then indexes that region's lines.
-static void preprocess_lines(const std::string& text, std::unique_ptr<char[]>& store,
+static void preprocess_lines(std::string_view text, std::unique_ptr<char[]>& store,
                              std::vector<std::string_view>& lines) {
     const size_t n = text.size();
     const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
@@ -860,7 +860,7 @@ struct Parser {
 
 }  // namespace
 
-Project parse_inp(const std::string& text) {
+Project parse_inp(std::string_view text) {
     Parser ps;
     preprocess_lines(text, ps.store, ps.views);
     // *NODE / *ELEMENT data blocks: keyword line followed by data lines up to the next keyword

@@ -9,6 +9,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <string_view>
 #include <unordered_map>
 #include <utility>
 #include <vector>
@@ -145,7 +146,7 @@ struct Project {
 };
 
 // Preprocess + parse (parser.rs:111-147, 903-942). Throws fx::Error.
-Project parse_inp(const std::string& text);
+Project parse_inp(std::string_view text);
 
 // Dense form: node index = rank of node id; one group per element type.
 struct ElemGroup {

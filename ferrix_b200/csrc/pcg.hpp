@@ -78,6 +78,13 @@ struct PcgSystem {
     double relres = 0.0;  // final ||b - A x||_M / ||b||_M
 };
 
+// Multigrid defaults, from a sweep on the 417k-DOF C3D20 box (136 -> 100 CG
+// iterations) and a population of C3D4 / C3D20 boxes (13 % less time):
+// coarse corrections scaled by 1.7 (aggregation without prolongator smoothing
+// under-corrects), first-kind Chebyshev on [lmax / 12, lmax].
+constexpr double kAmgOvercorrect = 1.7;
+constexpr double kAmgChebRatio = 12.0;
+
 struct PcgOptions {
     double rtol = 1e-10;
     int max_iter = 20000;
@@ -91,7 +98,9 @@ struct PcgOptions {
     int amg_degree = 2;       // Chebyshev smoothing steps per pre/post smoothing
     bool amg_fp32 = false;    // FP32 fine-matrix values in the level-0 smoother
     bool amg_kcycle = false;  // K-cycle at the first coarse level (flexible outer CG)
-    int amg_cheb_kind = 0;    // 0: Chebyshev of the first kind on [lmax/30, lmax], 1: fourth kind
+    int amg_cheb_kind = 0;    // 0: Chebyshev of the first kind on [lmax/ratio, lmax], 1: fourth kind
+    double amg_overcorrect = kAmgOvercorrect;  // scale of every coarse correction
+    double amg_cheb_ratio = kAmgChebRatio;  // lmax / lmin of the first-kind Chebyshev interval
 };
 
 template <typename T>

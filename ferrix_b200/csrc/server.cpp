@@ -13,6 +13,7 @@
 // concurrently on the device, on separate streams; each request's arithmetic is
 // the same as alone (no shared reductions, fixed launch shapes), so its result
 // does not depend on the mix.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -68,17 +69,6 @@ struct fx_server {
 };
 
 namespace {
-
-// Device bytes of one request while it runs: element pair buffers and the
-// symbolic sort per element, BSR3 values (FP64 + FP32), column indices and the
-// slot map per block, vectors and the multigrid hierarchy per node. Blocks per
-// element: 240 for C3D20 and 2.8 for C3D4 bricks-of-tets meshes (node pairs
-// shared by neighbouring elements counted once).
-double footprint(const DenseModel& D) {
-    const double e20 = (double)D.g20.size(), e4 = (double)D.g4.size(), n = (double)D.n_nodes;
-    const double blocks = 240.0 * e20 + 2.8 * e4;
-    return e20 * 32.0e3 + e4 * 1.6e3 + blocks * 120.0 + n * 1.0e3 + 64.0e6;
-}
 
 void release_device(fx_model* m) {
     if (!m->ctx) return;
@@ -173,6 +163,16 @@ int fx_server_create(const fx_server_opts* opts, fx_server** out) {
     s->n_slots = o.slots;
     s->budget = o.hbm_budget_bytes > 0.0 ? o.hbm_budget_bytes : 0.7 * (double)free_b;
     s->opts = o.opts;
+    // the budget is held in the device's memory pool from now on, so that requests
+    // never grow the pool while other requests' kernels run
+    cudaStream_t rs = nullptr;
+    if (cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking) == cudaSuccess) {
+        reserve_pool(o.device, rs, std::min(s->budget, 0.9 * (double)free_b));
+        cudaStreamSynchronize(rs);
+        cudaStreamDestroy(rs);
+    } else {
+        cudaGetLastError();
+    }
     for (int i = 0; i < o.slots; ++i) s->workers.emplace_back(worker, s, i);
     *out = s;
     return FX_OK;
@@ -192,7 +192,7 @@ int fx_server_submit(fx_server* s, fx_model* m, int64_t* ticket) {
         return e.status;
     }
     r->model = m;
-    r->bytes = footprint(m->dense);
+    r->bytes = model_footprint(m->dense);
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> g(s->mu);

@@ -86,8 +86,11 @@ typedef struct {
     int amg_smoother_degree; /* FX_PRECOND_AMG: Chebyshev steps per pre/post smoothing, 1..8; 0 = 2 */
     int amg_cycle;           /* FX_PRECOND_AMG: 0 = V-cycle, 1 = K-cycle at the first coarse level (two
                                 flexible-CG steps per coarse correction; the outer CG is then flexible) */
-    int amg_smoother;        /* FX_PRECOND_AMG: 0 = Chebyshev of the first kind on [lmax/30, lmax],
+    int amg_smoother;        /* FX_PRECOND_AMG: 0 = Chebyshev of the first kind on [lmax/ratio, lmax],
                                 1 = Chebyshev of the fourth kind (Lottes 2023) */
+    double amg_overcorrect;  /* FX_PRECOND_AMG: coarse corrections are scaled by this factor, in (0, 2);
+                                0 = 1.7 */
+    double amg_cheb_ratio;   /* FX_PRECOND_AMG: lmax / lmin of the first-kind Chebyshev interval; 0 = 12 */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */
@@ -113,7 +116,8 @@ typedef struct {
 } fx_step_stats;
 
 /* Defaults: FX_PREC_MIXED, FX_PRECOND_AMG, rtol 1e-8, max_iter 50000, poll 32,
- * reliable_delta 1e-2, graphs on, 40 nodes per aggregate, Chebyshev degree 2.
+ * reliable_delta 1e-2, graphs on, 40 nodes per aggregate, Chebyshev degree 2 on
+ * [lmax/12, lmax], coarse corrections scaled by 1.7.
  * fx_solve_csr has no node coordinates and always uses block-Jacobi. */
 void fx_default_solve_opts(fx_solve_opts* opts);
 
@@ -238,7 +242,9 @@ int fx_batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_o
 typedef struct {
     int device;
     int slots;               /* concurrent requests (worker threads, one stream each), 1..64 */
-    double hbm_budget_bytes; /* admission budget for the summed footprint estimates; 0 = 70% of free memory */
+    double hbm_budget_bytes; /* admission budget for the summed footprint estimates; 0 = 70% of free memory.
+                                fx_server_create reserves it in the device's memory pool (kept by the
+                                process until it exits) */
     fx_solve_opts opts;      /* solve options of every request */
 } fx_server_opts;
 
