@@ -369,24 +369,59 @@ __global__ void k_cheb_init(int n, int bs, const double* __restrict__ dinv, cons
 }
 
 // bc = Q^T rf per aggregate: one warp per aggregate, lanes over member rows
+// Coarse Chebyshev start fused into the restriction (cs.dinv != null): with
+// b = R r the first pre-smoothing step of the coarse level from x = 0 is
+// d = c2 D^-1 b, xs = d, r = b (what k_cheb_start does there).
+// b_c = Q^T r_f, warp per aggregate; each lane's rows are loaded four at a time
+// before they are accumulated (in the same order as one row at a time).
 __global__ void k_restrict(int na, const int32_t* __restrict__ ptr, const int32_t* __restrict__ nodes, int bs,
-                           const double* __restrict__ Q, const double* __restrict__ rf, double* __restrict__ bc) {
+                           const double* __restrict__ Q, const double* __restrict__ rf, double* __restrict__ bc,
+                           CoarseStart cs) {
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (a >= na) return;  // warp-uniform
     const int p0 = ptr[a], rows = (ptr[a + 1] - p0) * bs;
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int r = lane; r < rows; r += 32) {
-        const int j = nodes[p0 + r / bs];
-        const int64_t row = (int64_t)j * bs + r % bs;
-        const double rv = rf[row];
-        const double* q = Q + row * 6;
+    for (int r0 = lane; r0 < rows; r0 += 128) {
+        double rv[4], qv[4][6];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) acc[c] += q[c] * rv;
+        for (int u = 0; u < 4; ++u) {
+            const int r = r0 + 32 * u;
+            rv[u] = 0.0;
+            if (r < rows) {
+                const int j = nodes[p0 + r / bs];
+                const int64_t row = (int64_t)j * bs + r % bs;
+                rv[u] = rf[row];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) qv[u][c] = Q[row * 6 + c];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (r0 + 32 * u < rows) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) acc[c] += qv[u][c] * rv[u];
+            }
     }
+    double t[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-        const double t = warp_sum(acc[c]);
-        if (lane == 0) bc[(int64_t)a * 6 + c] = t;
+    for (int c = 0; c < 6; ++c) t[c] = warp_sum(acc[c]);  // every lane holds the sums
+    if (lane < 6) {
+        const int64_t o = (int64_t)a * 6 + lane;
+        double tk = t[0];
+#pragma unroll
+        for (int c = 1; c < 6; ++c)
+            if (lane == c) tk = t[c];
+        bc[o] = tk;
+        if (cs.dinv) {
+            const double* Di = cs.dinv + (int64_t)a * 36 + lane * 6;
+            double v = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) v += Di[j] * t[j];
+            v *= cs.c2;
+            cs.d[o] = v;
+            cs.xs[o] = v;
+            cs.r[o] = tk;
+        }
     }
 }
 
@@ -1447,7 +1482,19 @@ static LnOp ln_op(const AmgLevel& l) {
 // Chebyshev pre-smoothing from x = 0 into the scratch iterate xs (start kernel,
 // then SpMVs fused with the updates), the residual, the coarse correction added
 // to xs, and post-smoothing that reads xs and writes the result into x.
-void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
+CoarseStart Amg::coarse_start(int m) const {
+    CoarseStart cs{};
+    const AmgLevel& c = L[m];
+    if (c.coarsest || (kcycle_ && m == 1)) return cs;  // dense solve; K-cycle calls the cycle on other vectors
+    cs.dinv = c.dinv.ptr;
+    cs.r = c.r.ptr;
+    cs.d = c.d.ptr;
+    cs.xs = c.xs.ptr;
+    cs.c2 = cheb_coef(c.lmax, degree_, cheb_kind_, cheb_ratio_).c2_start;
+    return cs;
+}
+
+void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s, bool started) {
     AmgLevel& l = L[lev];
     const int64_t nd = (int64_t)l.n * l.bs;
     if (l.coarsest) {
@@ -1460,7 +1507,8 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
     double* dA = l.d.ptr;
     double* dB = l.t.ptr;
     double* xs = l.xs.ptr;
-    FX_LAUNCH(k_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv.ptr, b, l.r.ptr, dA, xs, k.c2_start);
+    if (!started)
+        FX_LAUNCH(k_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.bs, l.dinv.ptr, b, l.r.ptr, dA, xs, k.c2_start);
     for (int st = 1; st < degree_; ++st) {
         LnOp o = ln_op(l);
         o.v = dA;
@@ -1479,7 +1527,7 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
         FX_LAUNCH(k_ln_op<kL0RUpd>, grid, 256, 0, s, o);  // r = b - A xs
     }
     FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs,
-              l.Q.ptr, l.r.ptr, c.b.ptr);
+              l.Q.ptr, l.r.ptr, c.b.ptr, coarse_start(lev + 1));
     coarse(lev + 1, s);
     FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, l.bs, l.agg.ptr, l.Q.ptr, c.x.ptr, xs, alpha_);
     {
@@ -1510,7 +1558,7 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s) {
 void Amg::coarse(int m, cudaStream_t s) {
     AmgLevel& l = L[m];
     if (!(kcycle_ && m == 1 && !l.coarsest)) {
-        cycle(m, l.b.ptr, l.x.ptr, s);
+        cycle(m, l.b.ptr, l.x.ptr, s, coarse_start(m).dinv != nullptr);
         return;
     }
     const int64_t nd = (int64_t)l.n * l.bs;
@@ -1570,7 +1618,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
         FX_LAUNCH((k_l0_op<VT, kL0RUpd, g32>), grid, 256, 0, s, o);  // r = b - A x
     }
     FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
-              l.Q.ptr, l.r.ptr, c.b.ptr);
+              l.Q.ptr, l.r.ptr, c.b.ptr, coarse_start(1));
     coarse(1, s);
     if (g32) FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4, alpha_);
     else FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, alpha_);
@@ -1742,6 +1790,9 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         amg.apply(r_.ptr, zn, sc_.ptr, part_.ptr, counter_.ptr, amg.kcycle() ? zo : nullptr, s);  // z, r.z, beta
         FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, zn, sc_.ptr, p_.ptr);
     };
+    // Four iterations per graph replay between host checks. (A device-side loop
+    // as a WHILE graph node, one or four iterations per body, measured 1-7 %
+    // slower per iteration on B200 than these host-polled replays.)
     const int per_poll = 4;
     cudaGraphExec_t gexec = nullptr;
     int64_t per_iter_launches = 0;

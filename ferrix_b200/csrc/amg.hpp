@@ -61,6 +61,13 @@ struct AmgStats {
     double setup_ms = 0.0;
 };
 
+// First smoothing step of a coarse level, done by the restriction kernel into it.
+struct CoarseStart {
+    const double* dinv;  // 6x6 block inverses of the coarse level
+    double *r, *d, *xs;
+    double c2;
+};
+
 class Amg {
    public:
     // xyz: FP64 node coordinates (device, 3 per node); dinv0: fine 3x3 block inverses.
@@ -88,7 +95,10 @@ class Amg {
     std::vector<AmgLevel> L;
 
    private:
-    void cycle(int l, const double* b, double* x, cudaStream_t s);
+    // started: the restriction into this level already did the first smoothing step
+    void cycle(int l, const double* b, double* x, cudaStream_t s, bool started = false);
+    // the start that the restriction into level m does (dinv null: none)
+    CoarseStart coarse_start(int m) const;
     void coarse(int m, cudaStream_t s);
     template <typename VT>
     void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
