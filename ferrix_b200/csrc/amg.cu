@@ -30,10 +30,32 @@ void cub_call(Op op, DBuf<uint8_t>& tmp, cudaStream_t s) {
 
 // ------------------------------------------------------------------ aggregation
 
-__global__ void k_cell_keys(int n, const double* __restrict__ c, double ox, double oy, double oz, double inv_cell,
+// org[0..2] = componentwise minimum of the n points c (one CTA)
+__global__ void __launch_bounds__(1024) k_min3(int n, const double* __restrict__ c, double* __restrict__ org) {
+    __shared__ double sh[3][32];
+    double m[3] = {1e300, 1e300, 1e300};
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) m[d] = fmin(m[d], c[3 * (int64_t)i + d]);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        for (int o = 16; o > 0; o >>= 1) m[d] = fmin(m[d], __shfl_xor_sync(0xffffffffu, m[d], o));
+        if (lane == 0) sh[d][w] = m[d];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 1e300;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v = fmin(v, sh[threadIdx.x][k]);
+        org[threadIdx.x] = v;
+    }
+}
+
+__global__ void k_cell_keys(int n, const double* __restrict__ c, const double* __restrict__ org, double inv_cell,
                             uint64_t* __restrict__ keys, int32_t* __restrict__ ids) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const double ox = org[0], oy = org[1], oz = org[2];
     auto cell = [&](double v, double o) {
         double f = floor((v - o) * inv_cell);
         f = f < 0.0 ? 0.0 : (f > 2097151.0 ? 2097151.0 : f);
@@ -523,25 +545,45 @@ __global__ void __launch_bounds__(128) k_panel_rows(int nd, int k0, int b, doubl
     }
 }
 
-// every row i outside K (one warp per row): A[i, j] -= A[i, K] A[K, j], then A[i, K] = -A[i, K] P
-__global__ void __launch_bounds__(256) k_panel_trailing(int nd, int k0, int b, double* __restrict__ A) {
+// A[i, j] -= A[i, K] A[K, j] for every i, j outside K: one 32 x 32 tile per CTA,
+// both factors staged in shared memory (k0 is a multiple of 32, so the panel's
+// rows and columns are whole tiles, which are skipped)
+__global__ void __launch_bounds__(256) k_panel_update(int nd, int k0, int b, double* __restrict__ A) {
+    __shared__ double Lt[32][33];  // A[i0 + r, k0 + t]
+    __shared__ double Rt[32][33];  // A[k0 + t, j0 + c]
+    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+    if (i0 == k0 || j0 == k0) return;  // CTA-uniform
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        const int i = i0 + r, j = j0 + tx;
+        Lt[r][tx] = (i < nd && tx < b) ? A[(int64_t)i * nd + k0 + tx] : 0.0;
+        Rt[r][tx] = (r < b && j < nd) ? A[(int64_t)(k0 + r) * nd + j] : 0.0;
+    }
+    __syncthreads();
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int t = 0; t < 32; ++t) {
+        const double rv = Rt[t][tx];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] += Lt[ty + 8 * u][t] * rv;
+    }
+    const int j = j0 + tx;
+    if (j >= nd) return;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int i = i0 + ty + 8 * u;
+        if (i < nd) A[(int64_t)i * nd + j] -= acc[u];
+    }
+}
+
+// after the update: A[i, K] = -A[i, K] P for every row i outside K (one warp per row)
+__global__ void __launch_bounds__(256) k_panel_cols(int nd, int k0, int b, double* __restrict__ A) {
     __shared__ double P[kPanel][kPanel];
     load_panel(nd, k0, b, A, P);
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i >= nd || (i >= k0 && i < k0 + b)) return;  // warp-uniform
     double* Ai = A + (int64_t)i * nd;
     const double a = lane < b ? Ai[k0 + lane] : 0.0;
-    for (int j0 = 0; j0 < nd; j0 += 32) {  // uniform trip count: all lanes reach the shuffles
-        const int j = j0 + lane;
-        const bool valid = j < nd && !(j >= k0 && j < k0 + b);
-        double pk[kPanel];  // the panel rows' column j, all loads issued before the sum
-#pragma unroll
-        for (int t = 0; t < kPanel; ++t) pk[t] = (valid && t < b) ? A[(int64_t)(k0 + t) * nd + j] : 0.0;
-        double acc = 0.0;
-#pragma unroll
-        for (int t = 0; t < kPanel; ++t) acc += __shfl_sync(0xffffffffu, a, t) * pk[t];  // a = 0 for t >= b
-        if (valid) Ai[j] -= acc;
-    }
     double acc = 0.0;
     for (int s = 0; s < b; ++s) acc += __shfl_sync(0xffffffffu, a, s) * P[s][lane];
     if (lane < b) Ai[k0 + lane] = -acc;
@@ -1254,15 +1296,12 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         l0.dinv0 = dinv0;
         l0.nblocks = S0.n_blocks;
     }
-    // host copy of the level-0 points' origin
-    std::vector<double> hx(3 * (size_t)n_nodes);
-    FX_CUDA_CHECK(cudaMemcpyAsync(hx.data(), xyz, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    stream_wait(s, "amg coords");
-    double o[3] = {1e300, 1e300, 1e300};
-    for (int i = 0; i < n_nodes; ++i)
-        for (int d = 0; d < 3; ++d) o[d] = std::min(o[d], hx[3 * (size_t)i + d]);
-    DBuf<double> coords, cent, Rprev, Rnext;
-    coords.upload(hx, s);
+    // the level-0 points and their origin (cell keys of every level are taken from it)
+    DBuf<double> coords, cent, Rprev, Rnext, org;
+    coords.alloc(3 * (size_t)n_nodes, s);
+    FX_CUDA_CHECK(cudaMemcpyAsync(coords.ptr, xyz, 3 * (size_t)n_nodes * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    org.alloc(3, s);
+    FX_LAUNCH(k_min3, 1, 1024, 0, s, n_nodes, coords.ptr, org.ptr);
     double cell = cell0;
     for (int lev = 0;; ++lev) {
         AmgLevel& l = L[lev];
@@ -1292,7 +1331,9 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
                 const int b = std::min<int>(kPanel, (int)nd - k0);
                 FX_LAUNCH(k_panel_inverse, 1, 1024, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
                 FX_LAUNCH(k_panel_rows, grid_for(nd, 128), 128, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
-                FX_LAUNCH(k_panel_trailing, grid_for(nd * 32), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+                const unsigned tiles = (unsigned)((nd + 31) / 32);
+                FX_LAUNCH(k_panel_update, dim3(tiles, tiles), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+                FX_LAUNCH(k_panel_cols, grid_for(nd * 32), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
             }
             FX_LAUNCH(k_dense_zero_dead, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
             stream_wait(s, "amg coarse inverse");
@@ -1306,7 +1347,7 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         keys_s.alloc(l.n, s);
         ids.alloc(l.n, s);
         ids_s.alloc(l.n, s);
-        FX_LAUNCH(k_cell_keys, grid_for(l.n), 256, 0, s, l.n, coords.ptr, o[0], o[1], o[2], 1.0 / cell, keys.ptr,
+        FX_LAUNCH(k_cell_keys, grid_for(l.n), 256, 0, s, l.n, coords.ptr, org.ptr, 1.0 / cell, keys.ptr,
                   ids.ptr);
         cub_call([&](void* t, size_t& b) {
             return cub::DeviceRadixSort::SortPairs(t, b, keys.ptr, keys_s.ptr, ids.ptr, ids_s.ptr, l.n, 0, 63, s);
