@@ -2,6 +2,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 
@@ -878,20 +879,23 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
         for (int g = sub; g < ng; g += kL0Lanes) {
             const int4 cc = __ldg(reinterpret_cast<const int4*>(o.cols) + g0 + g);
             const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
-            double xv[4][3];
+            // FP32 values with FP32 gathered vectors: the group's 4 blocks are summed in
+            // FP32 (no FP64 conversions of the 36 values) and added to the FP64 row sums
+            using GT = typename std::conditional<G32, float, double>::type;
+            GT xv[4][3];
             if (G32) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const float4 t = __ldg(o.v4 + cj[q]);
-                    xv[q][0] = (double)t.x;
-                    xv[q][1] = (double)t.y;
-                    xv[q][2] = (double)t.z;
+                    xv[q][0] = t.x;
+                    xv[q][1] = t.y;
+                    xv[q][2] = t.z;
                 }
             } else {
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) xv[q][k] = __ldg(v + 3 * (int64_t)cj[q] + k);
+                    for (int k = 0; k < 3; ++k) xv[q][k] = (GT)__ldg(v + 3 * (int64_t)cj[q] + k);
             }
             const VT* vb = o.vals + ((int64_t)g0 * 9 + g) * 4;
             const int64_t pl = (int64_t)ng * 4;
@@ -901,11 +905,11 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
                 ld4v(vb + (3 * r) * pl, m0);
                 ld4v(vb + (3 * r + 1) * pl, m1);
                 ld4v(vb + (3 * r + 2) * pl, m2);
-                double t = 0.0;
+                GT t = 0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    t += (double)m0[q] * xv[q][0] + (double)m1[q] * xv[q][1] + (double)m2[q] * xv[q][2];
-                acc[r] += t;
+                    t += (GT)m0[q] * xv[q][0] + (GT)m1[q] * xv[q][1] + (GT)m2[q] * xv[q][2];
+                acc[r] += (double)t;
             }
         }
 #pragma unroll
