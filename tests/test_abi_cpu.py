@@ -24,6 +24,34 @@ def test_library_exports_every_header_symbol():
     assert set(declared) == set(_lib.SIGNATURES), set(declared) ^ set(_lib.SIGNATURES)
 
 
+def _struct_fill_check(struct_type, fill_fn):
+    """fill_fn writes exactly sizeof(struct_type) bytes: a guard region after the
+    ctypes struct (sized from the Python field list) stays untouched, so the
+    Python layout is at least as long as the C one."""
+    import ctypes as C
+    n = C.sizeof(struct_type)
+    buf = (C.c_ubyte * (n + 64))(*([0xA5] * (n + 64)))
+    fill_fn(C.cast(buf, C.POINTER(struct_type)))
+    assert bytes(buf[n:]) == b"\xa5" * 64
+    return struct_type.from_buffer_copy(bytes(buf[:n]))
+
+
+def test_option_structs_match_the_header():
+    lib = _lib.load()
+    o = _struct_fill_check(_lib.SolveOpts, lib.fx_default_solve_opts)
+    assert o.precision == fx.PREC_MIXED and o.preconditioner == fx.PRECOND_AMG and o.rtol == 1e-8
+    assert o.amg_smoother_degree == 2 and o.amg_overcorrect == 0.0 and o.amg_cheb_ratio == 0.0
+    so = _struct_fill_check(_lib.ServerOpts, lib.fx_default_server_opts)
+    assert so.slots == 4 and so.opts.amg_aggregate_nodes == 40 and so.opts.amg_cheb_ratio == 0.0
+    # the last field of each struct as the header lists it
+    text = open(HEADER).read()
+    body = text[text.index("typedef struct {", text.index("fx_precision;")):text.index("} fx_solve_opts;")]
+    import re
+    body = re.sub(r"/\*.*?\*/", "", body[body.index("{") + 1:], flags=re.S)
+    names = [d.split()[-1] for d in body.split(";") if d.strip()]
+    assert names == [f[0] for f in _lib.SolveOpts._fields_], names
+
+
 def _compare(text):
     o = inp.parse_inp_text(text)
     m = inp.model_arrays(o) if o.nodes else None
