@@ -51,13 +51,14 @@ def _deck():
     return decks.c3d20_box()
 
 
-def _oracle_job(out_path: str, q, go) -> None:
+def _oracle_job(out_path: str, q, go=None) -> None:
     """CPU reference path (oracle restatement): parse, serial assembly, CSR, FP64 Cholesky, Newton check.
-    Starts when `go` is set, after the GPU measurements, so that neither perturbs the other."""
+    With `go`, it starts when `go` is set (after the GPU measurements, so that neither perturbs the other)."""
     import numpy as np
     from oracle import inp, static_step
     text = _deck()
-    go.wait()
+    if go is not None:
+        go.wait()
     t0 = time.perf_counter()
     p = inp.parse_inp_text(text)
     r = static_step.Runner(p)
