@@ -73,17 +73,19 @@ double model_footprint(const DenseModel& D) {
     return e20 * 32.0e3 + e4 * 1.6e3 + blocks * 120.0 + n * 1.0e3 + 64.0e6;
 }
 
+// Spare pool memory to hold before a model's work is queued: 50 % over the
+// footprint estimate plus 256 MB, which absorbs the fragmentation that
+// otherwise made each new model grow the pool by a few tens of MB.
+double model_slack(const DenseModel& D) { return 1.5 * model_footprint(D) + 256.0e6; }
+
 // The pool is grown here, up front and with slack, because growing it goes to
 // the driver's physical allocator, which on shared B200 hosts stalled for up to
 // 0.5 s at times (even for 40 MB), and a pool that grows while kernels of other
 // streams are in flight stalls those too (requests of 7k DOF took 0.3-0.5 s
 // instead of 10 ms in a four-slot request loop). One allocation before any work
-// is queued cost about 12 ms per GB; 50 % slack over the estimate (plus 256 MB)
-// absorbs the fragmentation that otherwise made each new model grow the pool
-// by a few tens of MB.
+// is queued cost about 12 ms per GB.
 void reserve_pool(int device, cudaStream_t s, double bytes) {
     if (!(bytes > 0.0)) return;
-    bytes = 1.5 * bytes + 256.0e6;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) {
         cudaGetLastError();
@@ -114,7 +116,7 @@ void upload_model(fx_model* m) {
     if (d.uploaded) return;
     cudaStream_t s = m->ctx->stream;
     const DenseModel& D = m->dense;
-    reserve_pool(m->ctx->device, s, model_footprint(D));
+    reserve_pool(m->ctx->device, s, model_slack(D));
     d.xyz.upload(D.xyz, s);
     d.conn4.upload(D.g4.conn, s);
     d.mat4.upload(D.g4.mat, s);
@@ -683,7 +685,7 @@ int step_solve(fx_model* m, int k, const fx_solve_opts& o, fx_step_stats* st) {
         ~Restore() { g_launch_counter = v; }
     } restore{saved};
     ensure_dense(m);
-    reserve_pool(ctx->device, ctx->stream, model_footprint(m->dense));
+    reserve_pool(ctx->device, ctx->stream, model_slack(m->dense));
     EventTimer tot;
     tot.start(ctx->stream);
     StepRunner r;

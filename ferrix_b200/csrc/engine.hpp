@@ -99,8 +99,10 @@ inline int guarded(fx_ctx* ctx, F&& f) {
 namespace fx {
 
 void ensure_dense(fx_model* m);
-// Device bytes of one model while it is solved (an upper estimate).
+// Device bytes of one model while it is solved (an upper estimate), and the
+// spare pool memory held for it (with slack for fragmentation).
 double model_footprint(const DenseModel& D);
+double model_slack(const DenseModel& D);
 // Grows the device's stream-ordered memory pool (which keeps what it holds) so
 // that it has `bytes` more than it has in use, by one allocation queued on `s`
 // and freed again, before the caller queues any work. Best effort: a failed

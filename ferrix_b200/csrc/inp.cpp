@@ -10,6 +10,7 @@
 // and BCs carry over between steps unless OP=NEW; unknown keywords are an
 // error. Case folding is ASCII (decks are ASCII).
 #include <algorithm>
+#include <atomic>
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -273,14 +274,17 @@ static size_t substitute_solvers(char* buf, size_t len) {
     return len;
 }
 
-// Appends the str::lines views of text[a, b) (trailing '\r' dropped) to `lines`.
-static void split_lines(const char* text, size_t a, size_t b, std::string_view* lines) {
+// Writes the str::lines views of text[a, b) (trailing '\r' dropped) to
+// lines[0..) and appends first + (index) of every keyword line ('*') to kw.
+static void split_lines(const char* text, size_t a, size_t b, std::string_view* lines, size_t first,
+                        std::vector<size_t>& kw) {
     size_t k = 0;
     while (a < b) {
         const void* hit = std::memchr(text + a, '\n', b - a);
         const size_t end = hit ? (size_t)((const char*)hit - text) : b;
         size_t e2 = end;
         if (e2 > a && text[e2 - 1] == '\r') --e2;
+        if (e2 > a && text[a] == '*') kw.push_back(first + k);
         lines[k++] = std::string_view(text + a, e2 - a);
         a = end + 1;
     }
@@ -317,7 +321,7 @@ static bool ends_logical_line(std::string_view text, size_t lo, size_t nl) {
 // chunk: each thread preprocesses its chunk into its own region of `store`,
 // substitutes the solver names there, and then indexes that region's lines.
 static void preprocess_lines(std::string_view text, std::unique_ptr<char[]>& store,
-                             std::vector<std::string_view>& lines) {
+                             std::vector<std::string_view>& lines, std::vector<size_t>& keyword_lines) {
     const size_t n = text.size();
     const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     const size_t nthreads = std::min<size_t>(hw, std::max<size_t>(1, n / (1u << 20)));
@@ -357,7 +361,10 @@ static void preprocess_lines(std::string_view text, std::unique_ptr<char[]>& sto
     });
     for (size_t t = 0; t < nthreads; ++t) first[t + 1] = first[t] + nlines[t];
     lines.resize(first[nthreads]);
-    run([&](size_t t) { split_lines(out, cut[t], cut[t] + len[t], lines.data() + first[t]); });
+    std::vector<std::vector<size_t>> kw(nthreads);
+    run([&](size_t t) { split_lines(out, cut[t], cut[t] + len[t], lines.data() + first[t], first[t], kw[t]); });
+    keyword_lines.clear();
+    for (auto& v : kw) keyword_lines.insert(keyword_lines.end(), v.begin(), v.end());
 }
 
 // ------------------------------------------------------------------ parser
@@ -387,56 +394,73 @@ struct PreBlock {
     RawVec<int64_t> conn;               // *ELEMENT: npe per line
 };
 
-static void preparse_block(const std::vector<std::string_view>& lines, PreBlock& b) {
-    const size_t n = b.end - b.begin;
-    b.ids.resize(n);
-    if (b.npe == 0) b.xyz.resize(n);
-    else b.conn.resize((size_t)b.npe * n);
+// Runs f(0..ntasks-1) on up to 16 threads, each task once (the calling thread works too).
+template <typename F>
+static void parallel_tasks(size_t ntasks, F&& f) {
     const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const size_t nthreads = std::min<size_t>(hw, std::max<size_t>(1, n / 4096));
-    std::vector<uint8_t> bad(nthreads, 0);
-    std::vector<size_t> rows(nthreads, 0);  // non-empty lines seen per chunk
-    auto work = [&](size_t t) {
+    const size_t nthreads = std::min<size_t>(hw, ntasks);
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t t; (t = next.fetch_add(1)) < ntasks;) f(t);
+    };
+    if (nthreads <= 1) {
+        work();
+        return;
+    }
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nthreads; ++t) th.emplace_back(work);
+    work();
+    for (auto& x : th) x.join();
+}
+
+// Parses every block's lines into its arrays: tasks of up to 2,048 lines of
+// any block, taken in turn by up to 16 threads (each writes only its lines'
+// slots). A block with a line that does not parse is marked not ok.
+static void preparse_blocks(const std::vector<std::string_view>& lines, std::vector<PreBlock>& blocks) {
+    constexpr size_t kTask = 2048;
+    struct Task {
+        size_t block, a, e;
+    };
+    std::vector<Task> tasks;
+    for (size_t bi = 0; bi < blocks.size(); ++bi) {
+        PreBlock& b = blocks[bi];
+        const size_t n = b.end - b.begin;
+        b.ids.resize(n);
+        if (b.npe == 0) b.xyz.resize(n);
+        else b.conn.resize((size_t)b.npe * n);
+        for (size_t a = 0; a < n; a += kTask) tasks.push_back({bi, a, std::min(n, a + kTask)});
+    }
+    std::vector<uint8_t> bad(tasks.size(), 0);
+    parallel_tasks(tasks.size(), [&](size_t ti) {
         std::vector<std::string_view> f;
-        const size_t a = n * t / nthreads, e = n * (t + 1) / nthreads;
-        for (size_t k = a; k < e; ++k) {
+        f.reserve(24);
+        const Task& t = tasks[ti];
+        PreBlock& b = blocks[t.block];
+        for (size_t k = t.a; k < t.e; ++k) {
             const std::string_view line = lines[b.begin + k];
             size_t s = 0, z = line.size();
             while (s < z && is_ws(line[s])) ++s;
             if (s == z) {  // blank lines are skipped by the state machine: keep the block exact
-                bad[t] = 1;
+                bad[ti] = 1;
                 return;
             }
             split_views(line, ',', f);
+            bool ok;
             if (b.npe == 0) {
-                if (f.size() != 4 || !parse_usize_sv(f[0], &b.ids[k]) || !parse_f64_sv(f[1], &b.xyz[k][0]) ||
-                    !parse_f64_sv(f[2], &b.xyz[k][1]) || !parse_f64_sv(f[3], &b.xyz[k][2])) {
-                    bad[t] = 1;
-                    return;
-                }
+                ok = f.size() == 4 && parse_usize_sv(f[0], &b.ids[k]) && parse_f64_sv(f[1], &b.xyz[k][0]) &&
+                     parse_f64_sv(f[2], &b.xyz[k][1]) && parse_f64_sv(f[3], &b.xyz[k][2]);
             } else {
-                if ((int)f.size() != b.npe + 1 || !parse_usize_sv(f[0], &b.ids[k])) {
-                    bad[t] = 1;
-                    return;
-                }
-                for (int a2 = 0; a2 < b.npe; ++a2)
-                    if (!parse_usize_sv(f[a2 + 1], &b.conn[(size_t)b.npe * k + a2])) {
-                        bad[t] = 1;
-                        return;
-                    }
+                ok = (int)f.size() == b.npe + 1 && parse_usize_sv(f[0], &b.ids[k]);
+                for (int a2 = 0; ok && a2 < b.npe; ++a2) ok = parse_usize_sv(f[a2 + 1], &b.conn[(size_t)b.npe * k + a2]);
             }
-            ++rows[t];
+            if (!ok) {
+                bad[ti] = 1;
+                return;
+            }
         }
-    };
-    if (nthreads == 1) {
-        work(0);
-    } else {
-        std::vector<std::thread> th;
-        for (size_t t = 0; t < nthreads; ++t) th.emplace_back(work, t);
-        for (auto& x : th) x.join();
-    }
-    for (size_t t = 0; t < nthreads; ++t)
-        if (bad[t]) b.ok = false;
+    });
+    for (size_t ti = 0; ti < tasks.size(); ++ti)
+        if (bad[ti]) blocks[tasks[ti].block].ok = false;
 }
 
 struct Parser {
@@ -862,14 +886,14 @@ struct Parser {
 
 Project parse_inp(std::string_view text) {
     Parser ps;
-    preprocess_lines(text, ps.store, ps.views);
+    std::vector<size_t> kwl;  // indices of the keyword lines
+    preprocess_lines(text, ps.store, ps.views, kwl);
     // *NODE / *ELEMENT data blocks: keyword line followed by data lines up to the next keyword
     const auto& V = ps.views;
-    for (size_t i = 0; i < V.size(); ++i) {
+    for (size_t q = 0; q < kwl.size(); ++q) {
+        const size_t i = kwl[q];
         const std::string_view l = V[i];
-        if (l.empty() || l[0] != '*') continue;
-        size_t e = i + 1;
-        while (e < V.size() && !(!V[e].empty() && V[e][0] == '*')) ++e;
+        const size_t e = q + 1 < kwl.size() ? kwl[q + 1] : V.size();
         if (e - i - 1 < 1024) continue;  // small blocks: line by line
         const std::string kl(l);
         std::string name = trim(kl.substr(1, kl.find(',') == std::string::npos ? std::string::npos : kl.find(',') - 1));
@@ -889,7 +913,7 @@ Project parse_inp(std::string_view text) {
         }
         ps.blocks.push_back(std::move(b));
     }
-    for (auto& b : ps.blocks) preparse_block(ps.views, b);
+    preparse_blocks(ps.views, ps.blocks);
     ps.run();
     return std::move(ps.p);
 }
@@ -972,32 +996,50 @@ DenseModel build_dense(const Project& p) {
     }
     d.g4.npe = 4;
     d.g20.npe = 20;
-    int64_t n4 = 0;
-    for (int64_t k = 0; k < ne; ++k) n4 += p.elem_line_npe[(size_t)p.elem_line[(size_t)k]] == 4;
+    // each element's slot in its group (ascending id within the group)
+    std::vector<int32_t> slot((size_t)ne);
+    int64_t n4 = 0, n20 = 0;
+    for (int64_t k = 0; k < ne; ++k)
+        slot[(size_t)k] = (int32_t)(p.elem_line_npe[(size_t)p.elem_line[(size_t)k]] == 4 ? n4++ : n20++);
     for (ElemGroup* g : {&d.g4, &d.g20}) {
-        const int64_t m = g == &d.g4 ? n4 : ne - n4;
-        g->elem_ids.reserve((size_t)m);
-        g->conn.reserve((size_t)m * g->npe);
-        g->mat.reserve((size_t)m);
+        const int64_t m = g == &d.g4 ? n4 : n20;
+        g->elem_ids.resize((size_t)m);
+        g->conn.resize((size_t)m * g->npe);
+        g->mat.resize((size_t)m);
     }
-    for (int64_t k = 0; k < ne; ++k) {
-        const size_t line = (size_t)p.elem_line[(size_t)k];
-        const int npe = p.elem_line_npe[line];
-        ElemGroup& g = npe == 4 ? d.g4 : d.g20;
-        g.elem_ids.push_back(p.elem_ids[(size_t)k]);
-        const int64_t* nodes = &p.elem_line_conn[(size_t)p.elem_line_off[line]];
-        for (int a = 0; a < npe; ++a) {
-            const int64_t nid = nodes[a];
-            const int64_t idx = p.index_of(nid);
-            if (idx < 0 && d.missing_node_id < 0) {
-                d.missing_node_id = nid;
-                d.missing_node_error = "Node " + std::to_string(nid) + " not found in mesh";
+    // connectivity as node indices, in tasks of 2,048 elements; the first unknown
+    // node in element order is the one reported (NodeNotFound)
+    constexpr int64_t kTask = 2048;
+    const size_t ntask = (size_t)((ne + kTask - 1) / kTask);
+    std::vector<int64_t> miss_k(ntask, -1), miss_id(ntask, 0);
+    parallel_tasks(ntask, [&](size_t t) {
+        for (int64_t k = (int64_t)t * kTask; k < std::min<int64_t>(ne, ((int64_t)t + 1) * kTask); ++k) {
+            const size_t line = (size_t)p.elem_line[(size_t)k];
+            const int npe = p.elem_line_npe[line];
+            ElemGroup& g = npe == 4 ? d.g4 : d.g20;
+            const size_t pos = (size_t)slot[(size_t)k];
+            g.elem_ids[pos] = p.elem_ids[(size_t)k];
+            g.mat[pos] = mat[(size_t)k];
+            const int64_t* nodes = &p.elem_line_conn[(size_t)p.elem_line_off[line]];
+            int32_t* c = &g.conn[pos * (size_t)npe];
+            for (int a = 0; a < npe; ++a) {
+                const int64_t idx = p.index_of(nodes[a]);
+                if (idx < 0 && miss_k[t] < 0) {
+                    miss_k[t] = k;
+                    miss_id[t] = nodes[a];
+                }
+                c[a] = (int32_t)(idx < 0 ? 0 : idx);
             }
-            g.conn.push_back((int32_t)(idx < 0 ? 0 : idx));
         }
-        g.mat.push_back(mat[(size_t)k]);
-    }
-    // mesh volume: tets exactly; bricks as 6 Kuhn tets of their 8 corner nodes
+    });
+    for (size_t t = 0; t < ntask; ++t)
+        if (miss_k[t] >= 0) {
+            d.missing_node_id = miss_id[t];
+            d.missing_node_error = "Node " + std::to_string(miss_id[t]) + " not found in mesh";
+            break;
+        }
+    // mesh volume: tets exactly; bricks as 6 Kuhn tets of their 8 corner nodes. The
+    // tet volumes are computed in parallel and summed in element order on one thread.
     auto tet_vol = [&](int a, int b, int c, int e) {
         const double* A = &d.xyz[3 * (size_t)a];
         const double* B = &d.xyz[3 * (size_t)b];
@@ -1012,15 +1054,25 @@ DenseModel build_dense(const Project& p) {
         return std::fabs(u[0] * (v[1] * w[2] - v[2] * w[1]) - u[1] * (v[0] * w[2] - v[2] * w[0]) +
                          u[2] * (v[0] * w[1] - v[1] * w[0])) / 6.0;
     };
-    for (int64_t e = 0; e < d.g4.size(); ++e) {
-        const int32_t* c = &d.g4.conn[4 * (size_t)e];
-        d.volume += tet_vol(c[0], c[1], c[2], c[3]);
-    }
     static const int kuhn[6][4] = {{0, 1, 2, 6}, {0, 2, 3, 6}, {0, 3, 7, 6}, {0, 7, 4, 6}, {0, 4, 5, 6}, {0, 5, 1, 6}};
-    for (int64_t e = 0; e < d.g20.size(); ++e) {
-        const int32_t* c = &d.g20.conn[20 * (size_t)e];
-        for (auto& t : kuhn) d.volume += tet_vol(c[t[0]], c[t[1]], c[t[2]], c[t[3]]);
-    }
+    RawVec<double> tv((size_t)(n4 + 6 * n20));
+    const size_t vt4 = (size_t)((n4 + kTask - 1) / kTask), vt20 = (size_t)((n20 + kTask - 1) / kTask);
+    parallel_tasks(vt4 + vt20, [&](size_t t) {
+        if (t < vt4) {
+            for (int64_t e = (int64_t)t * kTask; e < std::min<int64_t>(n4, ((int64_t)t + 1) * kTask); ++e) {
+                const int32_t* c = &d.g4.conn[4 * (size_t)e];
+                tv[(size_t)e] = tet_vol(c[0], c[1], c[2], c[3]);
+            }
+        } else {
+            const int64_t t20 = (int64_t)(t - vt4);
+            for (int64_t e = t20 * kTask; e < std::min<int64_t>(n20, (t20 + 1) * kTask); ++e) {
+                const int32_t* c = &d.g20.conn[20 * (size_t)e];
+                for (int q = 0; q < 6; ++q)
+                    tv[(size_t)(n4 + 6 * e + q)] = tet_vol(c[kuhn[q][0]], c[kuhn[q][1]], c[kuhn[q][2]], c[kuhn[q][3]]);
+            }
+        }
+    });
+    for (double v : tv) d.volume += v;
     MatTableHost& m = d.mats;
     for (const Material& mat : p.materials) {
         auto add = [&](bool has, const Lut& l, std::vector<int32_t>& off, std::vector<int32_t>& len) {

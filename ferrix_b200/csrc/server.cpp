@@ -61,6 +61,7 @@ struct fx_server {
     std::unordered_map<int64_t, Request*> reqs;
     double in_use = 0.0;
     int running = 0;
+    int started = 0;  // workers whose context creation has finished (or failed)
     int64_t next_ticket = 1;
     bool stop = false;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -82,10 +83,16 @@ void release_device(fx_model* m) {
 void worker(fx_server* srv, int slot) {
     fx_ctx* ctx = nullptr;
     const int rc = fx_ctx_create(srv->device, &ctx);
-    if (rc != FX_OK) {
+    {
         std::lock_guard<std::mutex> g(srv->mu);
-        srv->last_error = "slot context creation failed";
-        --srv->n_slots;
+        ++srv->started;
+        if (rc != FX_OK) {
+            srv->last_error = "slot context creation failed";
+            --srv->n_slots;
+        }
+    }
+    srv->cv_done.notify_all();
+    if (rc != FX_OK) {
         srv->cv_work.notify_all();
         return;
     }
@@ -174,6 +181,10 @@ int fx_server_create(const fx_server_opts* opts, fx_server** out) {
         cudaGetLastError();
     }
     for (int i = 0; i < o.slots; ++i) s->workers.emplace_back(worker, s, i);
+    {  // every slot has its context (stream, workspaces) before the first request
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_done.wait_for(lk, std::chrono::seconds(60), [&] { return s->started == o.slots; });
+    }
     *out = s;
     return FX_OK;
 }
