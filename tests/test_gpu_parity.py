@@ -276,6 +276,22 @@ def test_amg_smoother_degree_and_cycle(ctx, degree, cycle, kind):
     assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref), stats
 
 
+@pytest.mark.parametrize("overcorrect,ratio", [(1.0, 30.0), (1.7, 12.0), (1.95, 8.0), (1.3, 50.0)])
+def test_amg_coarse_correction_scale_and_interval(ctx, overcorrect, ratio):
+    """Coarse-correction scale in (0, 2) and Chebyshev interval [lmax/ratio, lmax] against the oracle
+    (1.0 / 30 is the unscaled cycle; 1.7 / 12 the default)."""
+    text = AMG_CASES["c3d20_box_3_levels"]()
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    opts = fx.solve_opts(preconditioner=fx.PRECOND_AMG, amg_overcorrect=overcorrect, amg_cheb_ratio=ratio)
+    stats = p.steps[0].solve(1, p, st, opts=opts)
+    assert np.linalg.norm(st.displacements - ref) <= 1e-8 * np.linalg.norm(ref), stats
+    if (overcorrect, ratio) == (1.7, 12.0):  # the defaults
+        st.initialize(p)
+        d = p.steps[0].solve(1, p, st, opts=fx.solve_opts(preconditioner=fx.PRECOND_AMG))
+        assert d["pcg_iterations"] == stats["pcg_iterations"]
+
+
 @pytest.mark.parametrize("name", ["C3D4_staticstep", "C3D20", "NLGEOM_test"])
 def test_amg_reference_decks(ctx, golden_dir, name):
     gold = json.load(open(os.path.join(golden_dir, "calculix.json")))[name]
