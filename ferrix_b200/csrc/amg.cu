@@ -1157,44 +1157,60 @@ __global__ void k_prolong0(int n, const int32_t* __restrict__ agg, const double*
     x4[i] = make_float4((float)out[0], (float)out[1], (float)out[2], 0.0f);
 }
 
-// x += alpha p, r -= alpha q; r.D^-1 r reduced by the last CTA into S[2]
-__global__ void __launch_bounds__(256) k_amg_update2(int n, double* __restrict__ S, const double* __restrict__ p,
-                                                     const double* __restrict__ q, double* __restrict__ x,
-                                                     double* __restrict__ r, const double* __restrict__ dinv,
-                                                     double* __restrict__ part, int* __restrict__ counter) {
+// The CG update fused with the first step of the V-cycle that follows it:
+// x += alpha p, r -= alpha q, r.D^-1 r reduced by the last CTA into S[2], and
+// with b = the new r: r0 = b, x0 = d = c2 D^-1 b (what k_l0_cheb_start does)
+__global__ void __launch_bounds__(256) k_amg_update_start(int n, double* __restrict__ S, const double* __restrict__ p,
+                                                          const double* __restrict__ q, double* __restrict__ x,
+                                                          double* __restrict__ r, const double* __restrict__ dinv,
+                                                          double* __restrict__ part, int* __restrict__ counter,
+                                                          double* __restrict__ r0, double* __restrict__ x0,
+                                                          double* __restrict__ d0, float4* __restrict__ d4,
+                                                          double c2) {
     __shared__ double sh[32];
     __shared__ int s_last;
     const double alpha = S[5];
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int64_t o3 = 3 * (int64_t)i;
         double rv[3];
         for (int c = 0; c < 3; ++c) {
-            x[3 * i + c] += alpha * p[3 * i + c];
-            rv[c] = r[3 * i + c] - alpha * q[3 * i + c];
-            r[3 * i + c] = rv[c];
+            x[o3 + c] += alpha * p[o3 + c];
+            rv[c] = r[o3 + c] - alpha * q[o3 + c];
+            r[o3 + c] = rv[c];
+            r0[o3 + c] = rv[c];
         }
         const double* D = dinv + 9 * (int64_t)i;
-        for (int c = 0; c < 3; ++c) acc += rv[c] * (D[3 * c] * rv[0] + D[3 * c + 1] * rv[1] + D[3 * c + 2] * rv[2]);
+        double t[3];
+        for (int c = 0; c < 3; ++c) {
+            const double dr = D[3 * c] * rv[0] + D[3 * c + 1] * rv[1] + D[3 * c + 2] * rv[2];
+            acc += rv[c] * dr;
+            t[c] = c2 * dr;
+            x0[o3 + c] = t[c];
+        }
+        if (d4) d4[i] = make_float4((float)t[0], (float)t[1], (float)t[2], 0.0f);
+        else
+            for (int c = 0; c < 3; ++c) d0[o3 + c] = t[c];
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     acc = warp_sum(acc);
     if (lane == 0) sh[w] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int k = 0; k < nw; ++k) t += sh[k];
-        part[blockIdx.x] = t;
+        double tt = 0.0;
+        for (int k = 0; k < nw; ++k) tt += sh[k];
+        part[blockIdx.x] = tt;
         __threadfence();
         s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
     }
     __syncthreads();
     if (!s_last || w != 0) return;
     __threadfence();
-    double t = 0.0;
-    for (int k = lane; k < (int)gridDim.x; k += 32) t += __ldcg(part + k);
-    t = warp_sum(t);
+    double tt = 0.0;
+    for (int k = lane; k < (int)gridDim.x; k += 32) tt += __ldcg(part + k);
+    tt = warp_sum(tt);
     if (lane == 0) {
-        S[2] = t;
+        S[2] = tt;
         *counter = 0;
     }
 }
@@ -1622,7 +1638,7 @@ void Amg::coarse(int m, cudaStream_t s) {
 // reduces r.z and beta for the outer CG.
 template <typename VT>
 void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
-                  const double* zold, cudaStream_t s) {
+                  const double* zold, cudaStream_t s, bool started) {
     AmgLevel& l = L[0];
     AmgLevel& c = L[1];
     const int64_t nd = (int64_t)l.n * 3;
@@ -1635,8 +1651,9 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     float4* dA4 = reinterpret_cast<float4*>(l.d4a.ptr);
     float4* dB4 = reinterpret_cast<float4*>(l.d4b.ptr);
     float4* x4 = reinterpret_cast<float4*>(l.x4.ptr);
-    FX_LAUNCH(k_l0_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.dinv0, b, l.r.ptr, dA, g32 ? dA4 : nullptr, l.x.ptr,
-              k.c2_start);
+    if (!started)
+        FX_LAUNCH(k_l0_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.dinv0, b, l.r.ptr, dA, g32 ? dA4 : nullptr,
+                  l.x.ptr, k.c2_start);
     auto op = [&]() {
         L0Op<VT> o = l0_op<VT>(l, vals);
         return o;
@@ -1703,9 +1720,20 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
 }
 
 void Amg::apply(const double* r, double* z, double* S, double* part, int* counter, const double* zold,
-                cudaStream_t s) {
-    if (vals0_f32_) vcycle0<float>(vals0_f32_, r, z, S, part, counter, zold, s);
-    else vcycle0<double>(L[0].vals0, r, z, S, part, counter, zold, s);
+                cudaStream_t s, bool started) {
+    if (vals0_f32_) vcycle0<float>(vals0_f32_, r, z, S, part, counter, zold, s, started);
+    else vcycle0<double>(L[0].vals0, r, z, S, part, counter, zold, s, started);
+}
+
+Amg::Start0 Amg::start0() const {
+    const AmgLevel& l = L[0];
+    Start0 o{};
+    o.r = l.r.ptr;
+    o.x = l.x.ptr;
+    o.d = l.d.ptr;
+    o.d4 = vals0_f32_ ? reinterpret_cast<float4*>(l.d4a.ptr) : nullptr;
+    o.c2 = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_).c2_start;
+    return o;
 }
 
 // ------------------------------------------------------------------ AMG-preconditioned CG (FP64)
@@ -1830,9 +1858,10 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         o.counter = counter_.ptr;
         o.S = sc_.ptr;
         FX_LAUNCH((k_l0_op<double, kL0Apply>), g0, 256, 0, s, o);  // q = A p, alpha
-        FX_LAUNCH(k_amg_update2, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
-                  counter_.ptr);                                    // x, r, r.D^-1 r
-        amg.apply(r_.ptr, zn, sc_.ptr, part_.ptr, counter_.ptr, amg.kcycle() ? zo : nullptr, s);  // z, r.z, beta
+        const Amg::Start0 s0 = amg.start0();
+        FX_LAUNCH(k_amg_update_start, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
+                  counter_.ptr, s0.r, s0.x, s0.d, s0.d4, s0.c2);  // x, r, r.D^-1 r; the V-cycle's first step
+        amg.apply(r_.ptr, zn, sc_.ptr, part_.ptr, counter_.ptr, amg.kcycle() ? zo : nullptr, s, true);  // z, r.z, beta
         FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, zn, sc_.ptr, p_.ptr);
     };
     // Four iterations per graph replay between host checks. (A device-side loop

@@ -90,8 +90,17 @@ class Amg {
     // z = cycle(r), FP64 vectors of 3 * n_nodes. With S != null the last
     // smoothing step also reduces r.z (and r.zold when zold != null, for the
     // flexible CG) into the outer CG scalars (S[0], S[4]).
+    // started: the level-0 start (r0 = b, x = d = c2 D^-1 b) was done by the caller, into start0()
     void apply(const double* r, double* z, double* S, double* part, int* counter, const double* zold,
-               cudaStream_t s);
+               cudaStream_t s, bool started = false);
+    // where the level-0 start writes: the smoother's residual, iterate and first direction
+    // (FP32 float4 per node when the smoother is FP32, else FP64), and its coefficient
+    struct Start0 {
+        double *r, *x, *d;
+        float4* d4;
+        double c2;
+    };
+    Start0 start0() const;
     std::vector<AmgLevel> L;
 
    private:
@@ -102,7 +111,7 @@ class Amg {
     void coarse(int m, cudaStream_t s);
     template <typename VT>
     void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
-                 const double* zold, cudaStream_t s);
+                 const double* zold, cudaStream_t s, bool started);
     bool kcycle_ = false;
     int cheb_kind_ = 0;
     double alpha_ = 1.0, cheb_ratio_ = 30.0;
