@@ -252,26 +252,36 @@ static size_t preprocess_range(std::string_view text, size_t begin, size_t end, 
 static const char* const kSolverPats[] = {"ITERATIVE CHOLESKY", "ITERATIVE SCALING", "PASTIX", "PARDISO", "SPOOLES"};
 static const char* const kSolverReps[] = {"ITERATIVE", "ITERATIVE", "DIRECT", "DIRECT", "DIRECT"};
 
-// Replaces every solver name in buf[0, len) in pattern order, in place (no
-// replacement is longer than its pattern); returns the new length.
+// Replaces the solver names in buf[0, len) in place in one left-to-right pass
+// over non-overlapping matches, as aho-corasick's replace_all does (standard
+// semantics; these five names never overlap or contain one another, so that is
+// the leftmost match at each point, and a replacement never forms a new match:
+// "ITERATIVE CHOLESKY SCALING" becomes "ITERATIVE SCALING"). No replacement is
+// longer than its name. Returns the new length.
 static size_t substitute_solvers(char* buf, size_t len) {
-    for (int k = 0; k < 5; ++k) {
-        const std::string_view pat(kSolverPats[k]), rep(kSolverReps[k]);
-        size_t r = std::string_view(buf, len).find(pat);
-        if (r == std::string_view::npos) continue;
-        size_t w = r;
-        while (r != std::string_view::npos) {
-            std::memmove(buf + w, rep.data(), rep.size());
-            w += rep.size();
-            size_t from = r + pat.size();
-            r = std::string_view(buf, len).find(pat, from);
-            const size_t stop = r == std::string_view::npos ? len : r;
-            std::memmove(buf + w, buf + from, stop - from);
-            w += stop - from;
+    bool any = false;
+    for (const char* q : kSolverPats)
+        if (std::string_view(buf, len).find(q) != std::string_view::npos) any = true;
+    if (!any) return len;
+    size_t r = 0, w = 0;
+    while (r < len) {
+        int hit = -1;
+        const char c = buf[r];
+        if (c == 'I' || c == 'P' || c == 'S')
+            for (int k = 0; k < 5 && hit < 0; ++k) {
+                const size_t pl = std::strlen(kSolverPats[k]);
+                if (len - r >= pl && std::memcmp(buf + r, kSolverPats[k], pl) == 0) hit = k;
+            }
+        if (hit < 0) {
+            buf[w++] = buf[r++];
+            continue;
         }
-        len = w;
+        const size_t rl = std::strlen(kSolverReps[hit]);
+        std::memmove(buf + w, kSolverReps[hit], rl);
+        w += rl;
+        r += std::strlen(kSolverPats[hit]);
     }
-    return len;
+    return w;
 }
 
 // Writes the str::lines views of text[a, b) (trailing '\r' dropped) to

@@ -28,6 +28,7 @@ BCs carry over between steps unless OP=NEW; unknown keywords are errors.
 from __future__ import annotations
 
 import bisect
+import re
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple
 
@@ -53,11 +54,18 @@ KEYWORDS = {
 }
 
 
+_SOLVER_NAMES = {"ITERATIVE CHOLESKY": "ITERATIVE", "ITERATIVE SCALING": "ITERATIVE",
+                 "PASTIX": "DIRECT", "PARDISO": "DIRECT", "SPOOLES": "DIRECT"}
+_SOLVER_RE = re.compile("|".join(re.escape(k) for k in _SOLVER_NAMES))
+
+
 def substitute_ccx_solvers(text: str) -> str:
-    for pat, rep in (("ITERATIVE CHOLESKY", "ITERATIVE"), ("ITERATIVE SCALING", "ITERATIVE"),
-                     ("PASTIX", "DIRECT"), ("PARDISO", "DIRECT"), ("SPOOLES", "DIRECT")):
-        text = text.replace(pat, rep)
-    return text
+    """parser.rs:930-942: one left-to-right pass replacing non-overlapping matches
+    (aho-corasick `replace_all`, standard match semantics; for these five names,
+    which never overlap or contain one another, that is the leftmost match), so a
+    replacement never forms a new match: "ITERATIVE CHOLESKY SCALING" becomes
+    "ITERATIVE SCALING"."""
+    return _SOLVER_RE.sub(lambda m: _SOLVER_NAMES[m.group(0)], text)
 
 
 def preprocess_inp(text: str) -> str:

@@ -231,6 +231,8 @@ def test_parser_quirks_match_oracle():
 @pytest.mark.parametrize("text,kind", [
     ("*ORIENTATION, NAME=X\n", "UnsupportedKeyword"),
     ("*STEP\n*STATIC, SOLVER=MAGIC\n", "UnknownSolver"),
+    # one substitution pass: ITERATIVE CHOLESKY -> ITERATIVE leaves "ITERATIVE SCALING", not replaced again
+    ("*STEP\n*STATIC, SOLVER=ITERATIVE CHOLESKY SCALING\n", "UnknownSolver"),
     ("*NODE\n1, 0, 0\n", "ParseError"),
     ("*MATERIAL\n", "ParseError"),
     ("*SOLID SECTION, MATERIAL=M\n", "ParseError"),

@@ -44,6 +44,10 @@ def test_preprocess_and_arguments():
     assert inp.positional_arguments("0.1, 1, 1E-05, 0.2") == ["0.1", "1", "1E-05", "0.2"]
     assert "DIRECT" in inp.preprocess_inp("*Static, Solver=Spooles") and \
         "ITERATIVE" in inp.preprocess_inp("*static, solver=iterative scaling")
+    # substitute_ccx_solvers (parser.rs:930-942) is one aho-corasick replace_all pass:
+    # a replacement never forms a new match
+    assert inp.substitute_ccx_solvers("ITERATIVE CHOLESKY SCALING") == "ITERATIVE SCALING"
+    assert inp.substitute_ccx_solvers("SPOOLESPOOLES PASTIX PARDISO") == "DIRECTPOOLES DIRECT DIRECT"
 
 
 def test_c3d20_shape_functions():
