@@ -480,7 +480,8 @@ __global__ void k_dense_from_bsr(int n, const int32_t* __restrict__ row_ptr, con
 // vanishing diagonal are decoupled first and get zero rows/columns in the inverse.
 constexpr int kPanel = 32;
 
-__global__ void __launch_bounds__(1024) k_dense_decouple(int nd, double* __restrict__ A, uint8_t* __restrict__ dead) {
+__global__ void __launch_bounds__(1024) k_dense_decouple(int nd, double* __restrict__ A, uint8_t* __restrict__ dead,
+                                                         double* __restrict__ diag) {
     __shared__ double s_red[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     double m = 0.0;
@@ -495,15 +496,26 @@ __global__ void __launch_bounds__(1024) k_dense_decouple(int nd, double* __restr
     for (int r = warp; r < nd; r += nw)
         for (int c = lane; c < nd; c += 32)
             if (dead[r] || dead[c]) A[(int64_t)r * nd + c] = (r == c) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < nd; k += blockDim.x) diag[k] = A[(int64_t)k * nd + k];  // before elimination
 }
 
-// P = inverse of the pivot block A[k0:k0+b, k0:k0+b], written in place (one CTA, 32 warps)
-__global__ void __launch_bounds__(1024) k_panel_inverse(int nd, int k0, int b, double* __restrict__ A) {
+// A pivot of the elimination below kSingularPivot of its row's original
+// diagonal means the coarse operator is singular: the rigid-body modes of an
+// insufficiently constrained model lie in the coarse space (an SPD coarse
+// matrix keeps each pivot at or above 1 / cond of the original diagonal).
+constexpr double kSingularPivot = 1e-12;
+
+// P = inverse of the pivot block A[k0:k0+b, k0:k0+b], written in place (one CTA, 32 warps);
+// *singular |= 1 when a pivot is not above kSingularPivot times its original diagonal
+__global__ void __launch_bounds__(1024) k_panel_inverse(int nd, int k0, int b, double* __restrict__ A,
+                                                        const double* __restrict__ diag, int* __restrict__ singular) {
     __shared__ double S[kPanel][kPanel + 1];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     S[w][lane] = (w < b && lane < b) ? A[(int64_t)(k0 + w) * nd + k0 + lane] : (w == lane ? 1.0 : 0.0);
     __syncthreads();
     for (int t = 0; t < b; ++t) {
+        if (threadIdx.x == 0 && !(S[t][t] > kSingularPivot * diag[k0 + t])) *singular = 1;
         const double ip = 1.0 / S[t][t];
         __syncthreads();
         if (w == t && lane != t) S[t][lane] *= ip;
@@ -1346,17 +1358,27 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
                       l.dense_inv.ptr);
             DBuf<uint8_t> dead;
             dead.alloc(nd, s);
-            FX_LAUNCH(k_dense_decouple, 1, 1024, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
+            DBuf<double> diag0;
+            DBuf<int> singular;
+            diag0.alloc(nd, s);
+            singular.alloc(1, s);
+            singular.zero(s);
+            FX_LAUNCH(k_dense_decouple, 1, 1024, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr, diag0.ptr);
             for (int k0 = 0; k0 < (int)nd; k0 += kPanel) {
                 const int b = std::min<int>(kPanel, (int)nd - k0);
-                FX_LAUNCH(k_panel_inverse, 1, 1024, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+                FX_LAUNCH(k_panel_inverse, 1, 1024, 0, s, (int)nd, k0, b, l.dense_inv.ptr, diag0.ptr, singular.ptr);
                 FX_LAUNCH(k_panel_rows, grid_for(nd, 128), 128, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
                 const unsigned tiles = (unsigned)((nd + 31) / 32);
                 FX_LAUNCH(k_panel_update, dim3(tiles, tiles), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
                 FX_LAUNCH(k_panel_cols, grid_for(nd * 32), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
             }
             FX_LAUNCH(k_dense_zero_dead, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
+            int sing = 0;
+            FX_CUDA_CHECK(cudaMemcpyAsync(&sing, singular.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
             stream_wait(s, "amg coarse inverse");
+            if (sing)
+                fail(FX_NUMERICAL, "Mathematical error: the multigrid coarse operator is singular (system not "
+                                   "positive definite). Check for rigid body modes!");
             break;
         }
         estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr);

@@ -336,6 +336,27 @@ def test_errors_are_reported(ctx):
         p.steps[0].solve(1, p, st, opts=fx.solve_opts(max_iter=2, poll_interval=2,
                                                       preconditioner=fx.PRECOND_BLOCK_JACOBI))
     assert e.value.kind == "ConvergenceError"
+    # insufficient constraints (rigid-body modes): the reference's Cholesky fails with NumericalError
+    # ("... Check for rigid body modes!"); the multigrid coarse solve finds the singular coarse operator
+    # (the default solver), block-Jacobi PCG breaks down on the free deck (p.Kp <= 0)
+    text = decks.c3d4_cantilever(3, 3, 6)
+    lines, keep, skip = text.split("\n"), [], False
+    for line in lines:  # the same deck without its *BOUNDARY blocks
+        if line.upper().startswith("*BOUNDARY"):
+            skip = True
+            continue
+        if skip and not line.startswith("*"):
+            continue
+        skip = False
+        keep.append(line)
+    free = "\n".join(keep)
+    one_node = free.replace("*Cload", "*Boundary\n1, 1, 3\n*Cload", 1)  # one node fixed: rotations remain
+    for deck, pcs in ((free, (fx.PRECOND_AMG, fx.PRECOND_BLOCK_JACOBI)), (one_node, (fx.PRECOND_AMG,))):
+        for pc in pcs:
+            p, st = _project(ctx, deck)
+            with pytest.raises(fx.FerrixError) as e:
+                p.steps[0].solve(1, p, st, opts=fx.solve_opts(preconditioner=pc))
+            assert e.value.kind == "NumericalError" and "rigid body modes" in str(e.value), (pc, str(e.value))
     # unknown node in an element: NodeNotFound at the first element loop
     orphan = decks.c3d4_cantilever(1, 1, 1).replace("*Element, Type=C3D4, Elset=Solid\n",
                                                     "*Element, Type=C3D4, Elset=Solid\n99, 1, 2, 3, 12345\n")
