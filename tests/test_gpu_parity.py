@@ -305,6 +305,18 @@ def test_amg_reference_decks(ctx, golden_dir, name):
         assert err <= tol, (name, k, err, stats)
 
 
+def test_step_without_loads(ctx):
+    """No *CLOAD: R = 0 passes the convergence test (absolute norm, static_step.rs:145-171)
+    before any linear solve, so u stays exactly 0, as in the oracle."""
+    text = decks.c3d4_cantilever(2, 2, 4)
+    head, tail = text.split("*Cload, op=New", 1)
+    text = head + "*End step" + tail.split("*End step", 1)[1]
+    ref, r = _oracle_run(text)
+    p, st = _project(ctx, text)
+    stats = p.steps[0].solve(1, p, st)
+    assert stats["linear_solves"] == 0 and np.array_equal(st.displacements, ref) and not ref.any()
+
+
 def test_determinism(ctx):
     text = decks.c3d20_box(2, 2, 6)
     outs = []
