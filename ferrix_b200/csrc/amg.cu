@@ -645,8 +645,8 @@ __global__ void k_sum_part(int nb, const double* __restrict__ part, double* __re
 }
 
 // x = d / sqrt(*nrm2), the norm read on the device
-__global__ void k_normalize(int64_t n, const double* __restrict__ nrm2, const double* __restrict__ d,
-                            double* __restrict__ x) {
+// x = d / |d| (x may be d itself)
+__global__ void k_normalize(int64_t n, const double* __restrict__ nrm2, const double* d, double* x) {
     const double v = *nrm2;
     const double inv = v > 0.0 ? 1.0 / sqrt(v) : 1.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
