@@ -1312,6 +1312,70 @@ static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const 
     l.lmax = 1.1 * (nd2 > 0.0 ? std::sqrt(nd2) : 1.0);
 }
 
+// The fine level of a Galerkin product as the kernels read it: the planar BSR3
+// at level 0, row-major 6x6 block CSR (with each block's row) above.
+static FineView fine_view(const AmgLevel& l) {
+    FineView F{};
+    F.bs = l.bs;
+    if (l.S0) {
+        F.blk_row = l.S0->blk_row.ptr;
+        F.vals = l.vals0;
+        F.row_ptr = l.S0->row_ptr.ptr;
+        F.goff = l.S0->goff.ptr;
+        F.cols4 = l.S0->cols.ptr;
+    } else {
+        F.blk_row = l.gal_rows.ptr;
+        F.blk_col = l.cols.ptr;
+        F.vals = l.vals.ptr;
+    }
+    return F;
+}
+
+// c.vals = Q^T A Q over lf's Galerkin map (fixed-order sums per coarse block)
+static void galerkin(const AmgLevel& lf, AmgLevel& c, cudaStream_t s) {
+    const FineView F = fine_view(lf);
+    const int64_t ncb = c.nblocks;
+    if (F.bs == 3)
+        FX_LAUNCH(k_galerkin<3>, grid_for(ncb * 32, 128), 128, 0, s, ncb, lf.gal_seg.ptr, lf.gal_blk.ptr, F, lf.Q.ptr,
+                  c.vals.ptr);
+    else
+        FX_LAUNCH(k_galerkin<6>, grid_for(ncb * 32, 128), 128, 0, s, ncb, lf.gal_seg.ptr, lf.gal_blk.ptr, F, lf.Q.ptr,
+                  c.vals.ptr);
+}
+
+// Dense inverse of the coarsest level's matrix (blocked Gauss-Jordan); fails
+// with FX_NUMERICAL when the matrix is singular (rigid-body modes).
+void Amg::coarsest_inverse(AmgLevel& l, cudaStream_t s) {
+    const int64_t nd = (int64_t)l.n * l.bs;
+    l.dense_inv.alloc((size_t)nd * nd, s);
+    l.dense_inv.zero(s);
+    FX_LAUNCH(k_dense_from_bsr, grid_for(l.n, 64), 64, 0, s, l.n, l.row_ptr.ptr, l.cols.ptr, l.vals.ptr,
+              l.dense_inv.ptr);
+    DBuf<uint8_t> dead;
+    dead.alloc(nd, s);
+    DBuf<double> diag0;
+    DBuf<int> singular;
+    diag0.alloc(nd, s);
+    singular.alloc(1, s);
+    singular.zero(s);
+    FX_LAUNCH(k_dense_decouple, 1, 1024, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr, diag0.ptr);
+    for (int k0 = 0; k0 < (int)nd; k0 += kPanel) {
+        const int b = std::min<int>(kPanel, (int)nd - k0);
+        FX_LAUNCH(k_panel_inverse, 1, 1024, 0, s, (int)nd, k0, b, l.dense_inv.ptr, diag0.ptr, singular.ptr);
+        FX_LAUNCH(k_panel_rows, grid_for(nd, 128), 128, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+        const unsigned tiles = (unsigned)((nd + 31) / 32);
+        FX_LAUNCH(k_panel_update, dim3(tiles, tiles), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+        FX_LAUNCH(k_panel_cols, grid_for(nd * 32), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
+    }
+    FX_LAUNCH(k_dense_zero_dead, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
+    int sing = 0;
+    FX_CUDA_CHECK(cudaMemcpyAsync(&sing, singular.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    stream_wait(s, "amg coarse inverse");
+    if (sing)
+        fail(FX_NUMERICAL, "Mathematical error: the multigrid coarse operator is singular (system not "
+                           "positive definite). Check for rigid body modes!");
+}
+
 void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0, const double* xyz, int n_nodes,
                 double cell0, cudaStream_t s, AmgStats* st) {
     EventTimer timer;
@@ -1352,33 +1416,7 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         }
         if (lev > 0 && (nd <= kCoarseMaxDof || lev + 1 >= kMaxLevels)) {
             l.coarsest = true;
-            l.dense_inv.alloc((size_t)nd * nd, s);
-            l.dense_inv.zero(s);
-            FX_LAUNCH(k_dense_from_bsr, grid_for(l.n, 64), 64, 0, s, l.n, l.row_ptr.ptr, l.cols.ptr, l.vals.ptr,
-                      l.dense_inv.ptr);
-            DBuf<uint8_t> dead;
-            dead.alloc(nd, s);
-            DBuf<double> diag0;
-            DBuf<int> singular;
-            diag0.alloc(nd, s);
-            singular.alloc(1, s);
-            singular.zero(s);
-            FX_LAUNCH(k_dense_decouple, 1, 1024, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr, diag0.ptr);
-            for (int k0 = 0; k0 < (int)nd; k0 += kPanel) {
-                const int b = std::min<int>(kPanel, (int)nd - k0);
-                FX_LAUNCH(k_panel_inverse, 1, 1024, 0, s, (int)nd, k0, b, l.dense_inv.ptr, diag0.ptr, singular.ptr);
-                FX_LAUNCH(k_panel_rows, grid_for(nd, 128), 128, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
-                const unsigned tiles = (unsigned)((nd + 31) / 32);
-                FX_LAUNCH(k_panel_update, dim3(tiles, tiles), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
-                FX_LAUNCH(k_panel_cols, grid_for(nd * 32), 256, 0, s, (int)nd, k0, b, l.dense_inv.ptr);
-            }
-            FX_LAUNCH(k_dense_zero_dead, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, dead.ptr);
-            int sing = 0;
-            FX_CUDA_CHECK(cudaMemcpyAsync(&sing, singular.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
-            stream_wait(s, "amg coarse inverse");
-            if (sing)
-                fail(FX_NUMERICAL, "Mathematical error: the multigrid coarse operator is singular (system not "
-                                   "positive definite). Check for rigid body modes!");
+            coarsest_inverse(l, s);
             break;
         }
         estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr);
@@ -1423,22 +1461,11 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         FX_LAUNCH(k_agg_qr, grid_for((int64_t)na * 32), 256, 0, s, na, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs,
                   coords.ptr, cent.ptr, Rprev.ptr, l.Q.ptr, Rnext.ptr);
         // ---- Galerkin coarse matrix
-        FineView F{};
-        F.bs = l.bs;
-        DBuf<int32_t> blk_row_c;
-        if (l.S0) {
-            F.blk_row = l.S0->blk_row.ptr;
-            F.vals = l.vals0;
-            F.row_ptr = l.S0->row_ptr.ptr;
-            F.goff = l.S0->goff.ptr;
-            F.cols4 = l.S0->cols.ptr;
-        } else {
-            blk_row_c.alloc(l.nblocks, s);
-            FX_LAUNCH(k_expand_rows, grid_for(l.n), 256, 0, s, l.n, l.row_ptr.ptr, blk_row_c.ptr);
-            F.blk_row = blk_row_c.ptr;
-            F.blk_col = l.cols.ptr;
-            F.vals = l.vals.ptr;
+        if (!l.S0) {
+            l.gal_rows.alloc(l.nblocks, s);
+            FX_LAUNCH(k_expand_rows, grid_for(l.n), 256, 0, s, l.n, l.row_ptr.ptr, l.gal_rows.ptr);
         }
+        const FineView F = fine_view(l);
         const int nbits = bits_for(na > 1 ? na : 2);
         DBuf<uint64_t> ck, ck_s;
         DBuf<int64_t> cb, cb_s;
@@ -1486,12 +1513,9 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
             return cub::DeviceScan::InclusiveSum(t, b, cnt.ptr, c.row_ptr.ptr + 1, na, s);
         }, tmp_, s);
         c.vals.alloc((size_t)ncb * 36, s);
-        if (F.bs == 3)
-            FX_LAUNCH(k_galerkin<3>, grid_for((int64_t)ncb * 32, 128), 128, 0, s, (int64_t)ncb, seg.ptr, cb_s.ptr, F,
-                      lf.Q.ptr, c.vals.ptr);
-        else
-            FX_LAUNCH(k_galerkin<6>, grid_for((int64_t)ncb * 32, 128), 128, 0, s, (int64_t)ncb, seg.ptr, cb_s.ptr, F,
-                      lf.Q.ptr, c.vals.ptr);
+        lf.gal_seg = std::move(seg);  // kept for refresh()
+        lf.gal_blk = std::move(cb_s);
+        galerkin(lf, c, s);
         stream_wait(s, "amg galerkin");
         // next level points and near-null-space
         coords = std::move(cent);
@@ -1504,6 +1528,31 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
         for (auto& v : l1.kc) v.alloc(nd1, s);
         l1.kcs.alloc(8, s);
         l1.kcs.zero(s);
+    }
+    if (st) {
+        st->levels = (int)L.size();
+        st->sizes.clear();
+        for (auto& l : L) st->sizes.push_back(l.n * l.bs);
+        st->setup_ms = timer.stop_ms(s);
+    }
+}
+
+void Amg::refresh(const double* vals0, const double* dinv0, cudaStream_t s, AmgStats* st) {
+    EventTimer timer;
+    timer.start(s);
+    L[0].vals0 = vals0;
+    L[0].dinv0 = dinv0;
+    for (size_t lev = 0; lev < L.size(); ++lev) {  // the numeric steps of setup(), in its order
+        AmgLevel& l = L[lev];
+        if (lev > 0)
+            FX_LAUNCH(k_block_inv6, grid_for(l.n, 128), 128, 0, s, l.n, l.row_ptr.ptr, l.cols.ptr, l.vals.ptr,
+                      l.dinv.ptr);
+        if (l.coarsest) {
+            coarsest_inverse(l, s);
+            break;
+        }
+        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr);
+        galerkin(l, L[lev + 1], s);
     }
     if (st) {
         st->levels = (int)L.size();
@@ -1825,7 +1874,7 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
 
 int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
                   double cell0, const double* b, double* x, const PcgOptions& opt, cudaStream_t s,
-                  int64_t* launches, long long* iters, double* relres, AmgStats* st) {
+                  int64_t* launches, long long* iters, double* relres, AmgStats* st, bool reuse) {
     const int n = S.n_rows;
     const int64_t nd = 3 * (int64_t)n;
     if (opt.amg_degree < 1 || opt.amg_degree > 8) fail(FX_INVALID_ARGUMENT, "multigrid smoother degree must be 1..8");
@@ -1837,7 +1886,13 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         v32 = vals32_.ptr;
     }
     amg.set_smoother(opt.amg_degree, v32);  // before setup: its eigenvalue estimate uses v32
-    amg.setup(S, vals64, dinv64, xyz, n, cell0, s, st);
+    if (reuse && amg.built_for == S.id && !amg.L.empty() && amg.L[0].n == n) {
+        amg.refresh(vals64, dinv64, s, st);
+    } else {
+        amg.built_for = 0;  // (a failed setup leaves nothing to reuse)
+        amg.setup(S, vals64, dinv64, xyz, n, cell0, s, st);
+        amg.built_for = S.id;
+    }
     amg.set_cycle(opt.amg_kcycle);
     amg.set_smoother_kind(opt.amg_cheb_kind);
     amg.set_overcorrect(opt.amg_overcorrect);

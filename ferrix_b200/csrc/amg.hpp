@@ -52,6 +52,11 @@ struct AmgLevel {
     DBuf<double> dense_inv;
     // K-cycle work vectors (first coarse level): z1, v1, r, z2, v2 and scalars
     DBuf<double> kc[5], kcs;
+    // Galerkin map to the next level (kept for refresh): the fine blocks sorted by
+    // coarse block, each coarse block's segment of them, and (levels > 0) the row
+    // of every fine block
+    DBuf<int64_t> gal_seg, gal_blk;
+    DBuf<int32_t> gal_rows;
     const double* dinv_ptr() const { return S0 ? dinv0 : dinv.ptr; }
 };
 
@@ -73,6 +78,11 @@ class Amg {
     // xyz: FP64 node coordinates (device, 3 per node); dinv0: fine 3x3 block inverses.
     void setup(const BsrStructure& S0, const double* vals0, const double* dinv0, const double* xyz, int n_nodes,
                double cell0, cudaStream_t s, AmgStats* st);
+    // New matrix values on the structure of the last setup: aggregates, prolongators
+    // and coarse patterns are kept; coarse values, block inverses, eigenvalue
+    // estimates and the coarsest inverse are recomputed.
+    void refresh(const double* vals0, const double* dinv0, cudaStream_t s, AmgStats* st);
+    uint64_t built_for = 0;  // BsrStructure::id of the last setup (0: none)
     // Smoother settings: Chebyshev degree (1..8) and, when vals_f32 is not null,
     // FP32 values of the fine matrix for the level-0 smoothing (FP64 vectors).
     void set_smoother(int degree, const float* vals_f32) {
@@ -109,6 +119,7 @@ class Amg {
     // the start that the restriction into level m does (dinv null: none)
     CoarseStart coarse_start(int m) const;
     void coarse(int m, cudaStream_t s);
+    void coarsest_inverse(AmgLevel& l, cudaStream_t s);
     template <typename VT>
     void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
                  const double* zold, cudaStream_t s, bool started);
@@ -130,9 +141,11 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
 
 class AmgPcg {
    public:
+    // reuse: keep the hierarchy's aggregates, prolongators and coarse patterns when
+    // the last setup was on the same structure S (only the values are refreshed)
     int solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz, double cell0,
               const double* b, double* x, const PcgOptions& opt, cudaStream_t s, int64_t* launches, long long* iters,
-              double* relres, AmgStats* st);
+              double* relres, AmgStats* st, bool reuse = false);
     Amg amg;
 
    private:

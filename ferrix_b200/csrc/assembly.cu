@@ -1,3 +1,4 @@
+#include <atomic>
 // BSR(3x3) assembly: symbolic pattern by a device sort-by-key of node-pair
 // keys built from the connectivity (once per mesh), numeric values by an
 // atomic-free, fixed-order gather of element-pair blocks (every BSR block
@@ -116,6 +117,8 @@ static void exclusive_scan_i32(const int32_t* in, int32_t* out, int n, DBuf<uint
 }
 
 void build_bsr_structure(const ElemView& g4, const ElemView& g20, int n_nodes, BsrStructure& S, cudaStream_t s) {
+    static std::atomic<uint64_t> next_id{1};
+    S.id = next_id.fetch_add(1);
     S.n_rows = n_nodes;
     const int64_t p4 = (int64_t)g4.n * 16, p20 = (int64_t)g20.n * 400;
     const int64_t P = p4 + p20;

@@ -627,9 +627,13 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
             StepRunner& r = *rs[i];
             if (r.amg) {
                 AmgStats ast;
+                // NLGEOM: the Newton iterations after the first of an increment keep the
+                // hierarchy built at the increment's first tangent (aggregates and
+                // rigid-body prolongators of that configuration) and refresh its values
+                const bool reuse = r.step->nlgeom && r.it > 0;
                 r.csr_status = ctx->amgpcg.solve(r.m->dev.S, r.m->dev.vals64.ptr, r.m->dev.minv64.ptr,
                                                  r.amg_xyz.ptr, r.amg_cell, r.m->dev.R.ptr, r.m->dev.du.ptr, po, s,
-                                                 &ctx->launches, &r.csr_iters, &r.csr_relres, &ast);
+                                                 &ctx->launches, &r.csr_iters, &r.csr_relres, &ast, reuse);
                 r.S.amg_levels = ast.levels;
                 r.S.amg_setup_ms += ast.setup_ms;
                 continue;

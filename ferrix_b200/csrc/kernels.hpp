@@ -49,6 +49,7 @@ void launch_nodal_stress(const ElemView& g4, const ElemView& g20, const double* 
 // lane k%4. Slot lists: the element-pair slots contributing to block b are
 // slot_sorted[seg[b] .. seg[b+1]) (bit 31 = transposed).
 struct BsrStructure {
+    uint64_t id = 0;  // distinct for every structure built in the process
     int n_rows = 0;
     int64_t n_blocks = 0, n_groups = 0, n_pairs = 0;
     DBuf<int32_t> row_ptr, goff, cols, diag_k, blk_row;
