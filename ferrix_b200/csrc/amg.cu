@@ -1286,13 +1286,20 @@ static void dot_dev(const double* a, const double* b, int64_t n, DBuf<double>& r
 // Largest eigenvalue of D^-1 A by 12 power iterations from a fixed hashed start
 // vector, normalised on the device; one host read at the end.
 // (vals32: FP32 copy of the fine matrix, used for the products at level 0 when given)
-static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const float* vals32) {
+// warm: start from the vector the previous estimate on this level ended with (a
+// refresh after a small change of the matrix) and iterate 4 times instead of 12.
+static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const float* vals32, bool warm) {
     const int64_t nd = (int64_t)l.n * l.bs;
     const int nb = 296;
-    FX_LAUNCH(k_fill_hash, grid_for(nd), 256, 0, s, nd, l.x.ptr);
+    const bool from_ev = warm && l.ev.n == (size_t)nd;
+    if (from_ev)
+        FX_CUDA_CHECK(cudaMemcpyAsync(l.x.ptr, l.ev.ptr, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    else
+        FX_LAUNCH(k_fill_hash, grid_for(nd), 256, 0, s, nd, l.x.ptr);
     dot_dev(l.x.ptr, l.x.ptr, nd, red, s);
     FX_LAUNCH(k_normalize, grid_for(nd), 256, 0, s, nd, red.ptr + nb, l.x.ptr, l.x.ptr);
-    for (int it = 0; it < 12; ++it) {
+    const int iters = from_ev ? 4 : 12;
+    for (int it = 0; it < iters; ++it) {
         if (l.S0 && vals32) {  // t = A x, |x| = 1
             L0Op<float> o = l0_op<float>(l, vals32);
             o.v = l.x.ptr;
@@ -1306,6 +1313,8 @@ static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const 
         dot_dev(l.d.ptr, l.d.ptr, nd, red, s);
         FX_LAUNCH(k_normalize, grid_for(nd), 256, 0, s, nd, red.ptr + nb, l.d.ptr, l.x.ptr);
     }
+    l.ev.alloc(nd, s);
+    FX_CUDA_CHECK(cudaMemcpyAsync(l.ev.ptr, l.x.ptr, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
     double nd2 = 0.0;
     FX_CUDA_CHECK(cudaMemcpyAsync(&nd2, red.ptr + nb, sizeof(double), cudaMemcpyDeviceToHost, s));
     stream_wait(s, "amg eigenvalue estimate");
@@ -1419,7 +1428,7 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
             coarsest_inverse(l, s);
             break;
         }
-        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr);
+        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr, false);
         // ---- aggregation by cells
         DBuf<uint64_t> keys, keys_s;
         DBuf<int32_t> ids, ids_s, head, rank1;
@@ -1551,7 +1560,7 @@ void Amg::refresh(const double* vals0, const double* dinv0, cudaStream_t s, AmgS
             coarsest_inverse(l, s);
             break;
         }
-        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr);
+        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr, true);
         galerkin(l, L[lev + 1], s);
     }
     if (st) {

@@ -57,6 +57,8 @@ struct AmgLevel {
     // of every fine block
     DBuf<int64_t> gal_seg, gal_blk;
     DBuf<int32_t> gal_rows;
+    // last power-iteration vector of the eigenvalue estimate (start of the next refresh's)
+    DBuf<double> ev;
     const double* dinv_ptr() const { return S0 ? dinv0 : dinv.ptr; }
 };
 
