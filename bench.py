@@ -559,12 +559,15 @@ def main():
             except fx.FerrixError as e:
                 arms[name] = {"error": str(e)}
 
-    # e2e through the public API from host text and host buffers (the oracle has not started yet)
+    # e2e through the public API from the deck's bytes in host memory (what a caller of
+    # fx_model_from_inp passes; a file read by Project.from_jobname arrives the same way)
+    # to displacements in host memory (the oracle has not started yet)
     h2d = d2h = 0
     e2e_elapsed = None
+    deck_bytes = text.encode()
     if rank == 0 or True:
         def e2e_step():
-            p = fx.Project.from_inp_text(text, ctx)
+            p = fx.Project.from_inp_text(deck_bytes, ctx)
             s = fx.SolutionState(p.num_dofs, p.num_nodes)
             s.initialize(p)
             p.steps[0].solve(1, p, s, opts=opts)

@@ -222,11 +222,11 @@ class Project:
     def from_jobname(cls, jobname: str, ctx: Optional[Context] = None) -> "Project":
         path = jobname if jobname.lower().endswith(".inp") else jobname + ".inp"
         try:
-            with open(path, "r") as fh:
-                text = fh.read()
+            with open(path, "rb") as fh:  # the bytes go to the parser as they are
+                raw = fh.read()
         except OSError as e:
             raise FerrixError(1, f"IO error at {path}: {e}")
-        return cls.from_inp_text(text, ctx)
+        return cls.from_inp_text(raw, ctx)
 
     @property
     def default_initial_temperature(self) -> float:
