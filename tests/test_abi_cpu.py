@@ -165,6 +165,38 @@ def test_preprocess_chunks_match_oracle():
     assert p.steps[0].info.solver == "ITERATIVE"
 
 
+def _reformat(text, seed):
+    """The same deck with the formatting the preprocessor must undo: CRLF line ends,
+    random letter case, spaces and tabs around fields, comment and blank lines
+    between data lines, and data lines split after a comma (continuation lines)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for line in text.split("\n"):
+        if rng.random() < 0.05:
+            out.append("** c" + ("," if rng.random() < 0.5 else ""))  # comment lines never continue
+        if rng.random() < 0.03:
+            out.append(" \t ")
+        if not line.startswith("**") and rng.random() < 0.5:
+            line = "".join(ch.lower() if rng.random() < 0.5 else ch for ch in line)
+        if "," in line and not line.startswith("*") and rng.random() < 0.3:
+            k = line.index(",")  # split after the first comma
+            head, tail = line[:k + 1], line[k + 1:]
+            out.append("  " + head + " \t")
+            line = tail
+        out.append(("\t" if rng.random() < 0.1 else "") + line + (" " if rng.random() < 0.2 else ""))
+    return "\r\n".join(out)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_parser_formatting_matches_oracle(seed):
+    """Multi-chunk decks (over 2 MB, so the preprocessor runs several threads) with CRLF,
+    mixed case, whitespace, interleaved comments / blank lines and continuation lines."""
+    text = _reformat(decks.c3d20_box(14, 14, 30), seed)
+    assert len(text) > 2 << 20
+    p, o = _compare(text)
+    assert p.num_nodes == len(o.nodes) > 0
+
+
 QUIRKS = """** comment
 *Heading
 title line
