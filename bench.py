@@ -33,13 +33,6 @@ import argparse
 import json
 import multiprocessing as mp
 import os
-
-# Every kernel is loaded when the CUDA context is created instead of at its first
-# launch: with lazy loading, the first launch of a kernel not yet loaded waited
-# for the kernels running on the request loop's other streams and stalled them
-# all (four concurrent requests of 7k-220k DOF took 0.5-0.6 s instead of 10-50 ms).
-# Set before anything initialises CUDA; a serving process should do the same.
-os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 import statistics
 import subprocess
 import sys

@@ -2006,4 +2006,7 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     return rc;
 }
 
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_amg() { return reinterpret_cast<const void*>(&k_xpby); }
+
 }  // namespace fx

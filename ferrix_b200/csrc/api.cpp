@@ -1,8 +1,13 @@
 // extern "C" boundary (include/ferrix_b200.h). Every entry point converts
 // fx::Error / CUDA failures into an fx_status and keeps the message for
 // fx_ctx_last_error.
+#include <cuda.h>
+
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <set>
+#include <vector>
 
 #include "engine.hpp"
 
@@ -38,6 +43,51 @@ static double profile_t(fx_model* m, int reps, double* bytes) {
 
 }  // namespace
 
+namespace fx {
+
+// Loads every kernel of the library's modules on `device` (CUDA 12.4 driver
+// entry points, looked up at run time; without them, or on any error, kernels
+// load at their first launch as before).
+void preload_kernels(int device) {
+    static std::mutex mu;
+    static std::set<int> done;
+    std::lock_guard<std::mutex> g(mu);
+    if (!done.insert(device).second) return;
+    using GetModule = CUresult (*)(CUmodule*, CUfunction);
+    using Count = CUresult (*)(unsigned int*, CUmodule);
+    using Enumerate = CUresult (*)(CUfunction*, unsigned int, CUmodule);
+    using Load = CUresult (*)(CUfunction);
+    void *p_get = nullptr, *p_count = nullptr, *p_enum = nullptr, *p_load = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    const bool ok = cudaGetDriverEntryPointByVersion("cuFuncGetModule", &p_get, 12040, cudaEnableDefault, &q) ==
+                        cudaSuccess && p_get &&
+                    cudaGetDriverEntryPointByVersion("cuModuleGetFunctionCount", &p_count, 12040, cudaEnableDefault,
+                                                     &q) == cudaSuccess && p_count &&
+                    cudaGetDriverEntryPointByVersion("cuModuleEnumerateFunctions", &p_enum, 12040, cudaEnableDefault,
+                                                     &q) == cudaSuccess && p_enum &&
+                    cudaGetDriverEntryPointByVersion("cuFuncLoad", &p_load, 12040, cudaEnableDefault, &q) ==
+                        cudaSuccess && p_load;
+    if (ok) {
+        for (const void* anchor : {kernels_anchor_amg(), kernels_anchor_assembly(), kernels_anchor_csr_solve(),
+                                   kernels_anchor_elements(), kernels_anchor_noalloc(), kernels_anchor_pcg(),
+                                   kernels_anchor_pcg_csr(), kernels_anchor_vectors()}) {
+            cudaFunction_t f = nullptr;
+            if (cudaGetFuncBySymbol(&f, anchor) != cudaSuccess || !f) continue;
+            CUmodule mod = nullptr;
+            unsigned int n = 0;
+            if (reinterpret_cast<GetModule>(p_get)(&mod, reinterpret_cast<CUfunction>(f)) != CUDA_SUCCESS ||
+                reinterpret_cast<Count>(p_count)(&n, mod) != CUDA_SUCCESS)
+                continue;
+            std::vector<CUfunction> fns(n);
+            if (n == 0 || reinterpret_cast<Enumerate>(p_enum)(fns.data(), n, mod) != CUDA_SUCCESS) continue;
+            for (CUfunction fn : fns) reinterpret_cast<Load>(p_load)(fn);
+        }
+    }
+    cudaGetLastError();
+}
+
+}  // namespace fx
+
 extern "C" {
 
 void fx_default_solve_opts(fx_solve_opts* o) {
@@ -71,6 +121,7 @@ int fx_ctx_create(int device, fx_ctx** out) {
         c->device = device;
         FX_CUDA_CHECK(cudaSetDevice(device));
         FX_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        preload_kernels(device);
         // keep freed stream-ordered allocations in this process's pool between solves
         // instead of returning them to the driver at every synchronisation
         cudaMemPool_t pool;

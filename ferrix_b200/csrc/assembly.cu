@@ -358,4 +358,7 @@ template void launch_bsr_to_csr<float>(const BsrStructure&, const float*, const 
 template void launch_bsr_to_csr<double>(const BsrStructure&, const double*, const int64_t*, int64_t*, double*,
                                         cudaStream_t);
 
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_assembly() { return reinterpret_cast<const void*>(&k_pair_keys); }
+
 }  // namespace fx

@@ -146,6 +146,9 @@ static int solve_csr_t(fx_ctx* ctx, int64_t n, const int64_t* ip, const int64_t*
     return sys.status;
 }
 
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_csr_solve() { return reinterpret_cast<const void*>(&k_csr_residual); }
+
 }  // namespace fx
 
 using namespace fx;

@@ -659,4 +659,7 @@ void launch_node_gather(int n_nodes, const int32_t* ptr, const int32_t* slots, c
     if (n_nodes) FX_LAUNCH(k_node_gather, (n_nodes + 255) / 256, 256, 0, s, n_nodes, ptr, slots, fe, out);
 }
 
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_elements() { return reinterpret_cast<const void*>(&k_stiff4<double>); }
+
 }  // namespace fx

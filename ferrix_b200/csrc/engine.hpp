@@ -99,6 +99,19 @@ inline int guarded(fx_ctx* ctx, F&& f) {
 namespace fx {
 
 void ensure_dense(fx_model* m);
+// One kernel of each source file's module, and the loading of every kernel of
+// those modules on the current device (once per device and process): with lazy
+// module loading, a kernel's first launch would otherwise wait for the kernels
+// running on other streams.
+const void* kernels_anchor_amg();
+const void* kernels_anchor_assembly();
+const void* kernels_anchor_csr_solve();
+const void* kernels_anchor_elements();
+const void* kernels_anchor_noalloc();
+const void* kernels_anchor_pcg();
+const void* kernels_anchor_pcg_csr();
+const void* kernels_anchor_vectors();
+void preload_kernels(int device);
 // Device bytes of one model while it is solved (an upper estimate), and the
 // spare pool memory held for it (with slack for fragmentation).
 double model_footprint(const DenseModel& D);

@@ -94,6 +94,9 @@ __global__ void __launch_bounds__(256) k_spmv_dot_noalloc(int64_t n, const int64
 }
 
 }  // namespace
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_noalloc() { return reinterpret_cast<const void*>(&k_spmv_dot_noalloc); }
+
 }  // namespace fx
 
 using namespace fx;

@@ -529,4 +529,7 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
 template class PcgBatch<float>;
 template class PcgBatch<double>;
 
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_pcg() { return reinterpret_cast<const void*>(&k_pcg_update<float>); }
+
 }  // namespace fx

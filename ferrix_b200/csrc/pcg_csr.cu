@@ -281,4 +281,7 @@ int CsrPcg::solve(CsrSystem& A, const double* b, double* x, const PcgOptions& op
     return rc;
 }
 
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_pcg_csr() { return reinterpret_cast<const void*>(&k_csr_spmv); }
+
 }  // namespace fx

@@ -94,4 +94,7 @@ void launch_masked_norms(int64_t n, const double* a, const double* b, const uint
     FX_LAUNCH(k_sum_partials, 1, 32, 0, s, kNormBlocks, partials, out);
 }
 
+// A kernel of this file's module (preload_kernels() loads all of the module's kernels).
+const void* kernels_anchor_vectors() { return reinterpret_cast<const void*>(&k_axpby); }
+
 }  // namespace fx
