@@ -197,6 +197,22 @@ def test_parser_formatting_matches_oracle(seed):
     assert p.num_nodes == len(o.nodes) > 0
 
 
+EDGE_DECKS = {
+    "empty": "",
+    "comments_only": "** a\n**b,\n   \n",
+    # line-by-line path (blocks under 1,024 lines): a later definition of a node / element wins
+    "repeated_ids": "*NODE\n1,0,0,0\n2,1,0,0\n1,5,5,5\n3,0,1,0\n4,0,0,1\n*ELEMENT,TYPE=C3D4,ELSET=E\n"
+                    "1,1,2,3,4\n1,2,1,3,4\n",
+    "element_without_type": "*NODE\n1,0,0,0\n*ELEMENT\n1,1,1,1,1\n",  # data dropped
+    "plus_sign_and_exponents": "*NODE\n+1,1E3,-2.5e-2,+3.\n2,inf,0,0\n",
+}
+
+
+@pytest.mark.parametrize("name", list(EDGE_DECKS))
+def test_parser_edge_decks_match_oracle(name):
+    _compare(EDGE_DECKS[name])
+
+
 QUIRKS = """** comment
 *Heading
 title line
@@ -273,6 +289,9 @@ def test_parser_quirks_match_oracle():
     ("*MATERIAL, NAME=M\n*SOLID SECTION, ELSET=A, MATERIAL=Q\n", "MaterialNotFound"),
     ("*ELEMENT, TYPE=C3D8\n1, 1, 2, 3, 4, 5, 6, 7, 8\n", "ParseError"),
     ("*ELEMENT, TYPE=C3D4\n1, 1, 2, 3\n", "ParseError"),
+    ("*NODE\n1, 0, 0, 0, 7\n", "ParseError"),
+    ("*NODE\n1, 0, x, 0\n", "ParseError"),
+    ("*NODE\n-1, 0, 0, 0\n", "ParseError"),
     ("*AMPLITUDE\n0, 1\n", "ParseError"),
 ])
 def test_parser_errors(text, kind):
