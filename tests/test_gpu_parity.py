@@ -305,6 +305,19 @@ def test_amg_reference_decks(ctx, golden_dir, name):
         assert err <= tol, (name, k, err, stats)
 
 
+def test_nlgeom_repeatable(ctx):
+    """An NLGEOM step solved twice on the same model gives the same bits: each increment's first
+    Newton iteration rebuilds the multigrid hierarchy, the later ones refresh it, in the same order."""
+    text = decks.c3d4_nlgeom_beam(12, 3, 3, tip_load=2.0e3, increments=4)
+    p, st = _project(ctx, text)
+    runs = []
+    for _ in range(2):
+        st.initialize(p)
+        stats = p.steps[0].solve(1, p, st)
+        runs.append((st.displacements.copy(), stats["pcg_iterations"], stats["newton_iterations"]))
+    assert np.array_equal(runs[0][0], runs[1][0]) and runs[0][1:] == runs[1][1:]
+
+
 def test_step_without_loads(ctx):
     """No *CLOAD: R = 0 passes the convergence test (absolute norm, static_step.rs:145-171)
     before any linear solve, so u stays exactly 0, as in the oracle."""
