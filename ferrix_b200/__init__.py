@@ -36,19 +36,32 @@ __all__ = ["Context", "Project", "SolutionState", "SolverTime", "FerrixError", "
 
 
 class FerrixError(Exception):
-    def __init__(self, status: int, message: str):
+    """A FerrixError variant (src/solver/error.rs:12-72): `kind` is the variant's name,
+    `line` the deck line of ParseError / UnsupportedKeyword, `id` the id of
+    NodeNotFound / ElementNotFound (None where the variant has none), `text` the
+    variant's string field (message, keyword, material / set / solver name)."""
+
+    def __init__(self, status: int, message: str, line: Optional[int] = None, id: Optional[int] = None,
+                 text: Optional[str] = None):
         self.status = status
         self.kind = _lib.STATUS_NAMES.get(status, str(status))
         self.message = message
+        self.line = line
+        self.id = id
+        self.text = message if text is None else text
         super().__init__(f"{self.kind}: {message}")
 
 
 def _check(rc: int, ctx=None, what: str = ""):
     if rc != 0:
-        msg = ""
-        if ctx is not None and ctx.handle:
-            msg = (_lib.load().fx_ctx_last_error(ctx.handle) or b"").decode(errors="replace")
-        raise FerrixError(rc, msg or what)
+        d = _lib.ErrorDetail()
+        h = ctx.handle if ctx is not None and ctx.handle else None
+        _lib.load().fx_last_error_detail(h, C.byref(d))
+        if d.status == rc:
+            msg = d.message.decode(errors="replace")
+            raise FerrixError(rc, msg or what, None if d.line < 0 else int(d.line), None if d.id < 0 else int(d.id),
+                              d.text.decode(errors="replace"))
+        raise FerrixError(rc, what)
 
 
 def _p(a: Optional[np.ndarray]):
@@ -71,6 +84,11 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(self.lib.fx_ctx_kernel_launches(self.handle))
+
+    @property
+    def preloaded_kernels(self) -> int:
+        """Kernels of the library found loaded on the device at creation (-1: loaded at first use)."""
+        return int(self.lib.fx_ctx_preloaded_kernels(self.handle))
 
     @property
     def stream(self) -> int:
@@ -96,7 +114,8 @@ def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 
                reliable_delta: float = 1e-2, use_graphs: bool = True, verbose: bool = False,
                reference_iterative: bool = False, preconditioner: int = PRECOND_AMG,
                amg_aggregate_nodes: int = 40, amg_smoother_degree: int = 2, amg_cycle: int = 0,
-               amg_smoother: int = 0, amg_overcorrect: float = 0.0, amg_cheb_ratio: float = 0.0) -> SolveOpts:
+               amg_smoother: int = 0, amg_overcorrect: float = 0.0, amg_cheb_ratio: float = 0.0,
+               amg_persistent_max_dof: int = 0) -> SolveOpts:
     o = SolveOpts()
     _lib.load().fx_default_solve_opts(C.byref(o))
     o.precision = precision
@@ -114,6 +133,7 @@ def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 
     o.amg_smoother = int(amg_smoother)
     o.amg_overcorrect = float(amg_overcorrect)
     o.amg_cheb_ratio = float(amg_cheb_ratio)
+    o.amg_persistent_max_dof = int(amg_persistent_max_dof)
     return o
 
 
@@ -217,6 +237,92 @@ class Project:
         h = C.c_void_p()
         _check(lib.fx_model_from_inp(ctx.handle if ctx else None, raw, len(raw), C.byref(h)), ctx)
         return cls(h, ctx)
+
+    @classmethod
+    def from_arrays(cls, node_ids, xyz, c3d4=None, c3d20=None, materials=(), amplitudes=(), steps=(),
+                    default_temperature: float = 0.0, initial_temperatures=None,
+                    ctx: Optional[Context] = None) -> "Project":
+        """fx_model_from_arrays: the model a parsed deck gives, from arrays.
+
+        node_ids (N,), xyz (N, 3); c3d4 / c3d20 = (element ids, node ids per element
+        (E, 4 | 20), material index per element or None); materials = dicts with
+        "name", "E", "nu", "alpha" ((T, value) pairs; alpha may be empty) and "tref";
+        amplitudes = dicts with "time", "value", "total_time", "shift_x", "shift_y";
+        steps = dicts with "nlgeom", "solver" (0 default, 1 direct, 2 iterative),
+        "increment" (initial, period, min, max), "max_increments" and "loads" / "bcs":
+        sequences of (node id, dof 0..2, value, amplitude index or -1, origin step);
+        initial_temperatures = {node id: T}."""
+        lib = _lib.load()
+        keep = []  # every array the descriptor points into stays alive until the call returns
+
+        def arr(a, dtype):
+            a = np.ascontiguousarray(np.asarray(a, dtype=dtype))
+            keep.append(a)
+            return a
+
+        def ptr(a):
+            return a.ctypes.data_as(C.c_void_p) if a.size else None
+
+        d = _lib.MeshDesc()
+        ids = arr(node_ids, np.int64)
+        xs = arr(xyz, np.float64).reshape(-1)
+        d.n_nodes = ids.size
+        d.node_ids, d.xyz = ptr(ids), ptr(xs)
+        for npe, grp in ((4, c3d4), (20, c3d20)):
+            if grp is None:
+                continue
+            eids = arr(grp[0], np.int64)
+            conn = arr(grp[1], np.int64).reshape(-1)
+            mat = None if len(grp) < 3 or grp[2] is None else arr(grp[2], np.int32)
+            setattr(d, f"n_c3d{npe}", eids.size)
+            setattr(d, f"c3d{npe}_ids", ptr(eids))
+            setattr(d, f"c3d{npe}_nodes", ptr(conn))
+            setattr(d, f"c3d{npe}_material", None if mat is None else ptr(mat))
+
+        def lut(pairs):
+            a = arr(pairs, np.float64).reshape(-1, 2) if len(pairs) else np.zeros((0, 2))
+            t, v = arr(a[:, 0], np.float64), arr(a[:, 1], np.float64)
+            return _lib.LutDesc(len(a), ptr(t), ptr(v))
+
+        mats = (_lib.MaterialDesc * max(1, len(materials)))()
+        for k, m in enumerate(materials):
+            name = (m.get("name") or "").encode()
+            keep.append(name)
+            mats[k] = _lib.MaterialDesc(name, lut(m.get("E", ())), lut(m.get("nu", ())),
+                                        lut(m.get("alpha", ())), float(m.get("tref", 0.0)))
+        d.n_materials, d.materials = len(materials), C.cast(mats, C.c_void_p)
+        amps = (_lib.AmplitudeDesc * max(1, len(amplitudes)))()
+        for k, a in enumerate(amplitudes):
+            t, v = arr(a["time"], np.float64), arr(a["value"], np.float64)
+            amps[k] = _lib.AmplitudeDesc(t.size, ptr(t), ptr(v), int(bool(a.get("total_time", False))),
+                                         float(a.get("shift_x", 0.0)), float(a.get("shift_y", 0.0)))
+        d.n_amplitudes, d.amplitudes = len(amplitudes), C.cast(amps, C.c_void_p)
+
+        def records(recs):
+            r = (_lib.RecordDesc * max(1, len(recs)))()
+            for k, (nid, dof, val, amp, org) in enumerate(recs):
+                r[k] = _lib.RecordDesc(int(nid), int(dof), int(amp), float(val), int(org))
+            keep.append(r)
+            return len(recs), C.cast(r, C.c_void_p)
+
+        sts = (_lib.StepDesc * max(1, len(steps)))()
+        for k, st in enumerate(steps):
+            nl, lp = records(st.get("loads", ()))
+            nb, bp = records(st.get("bcs", ()))
+            sts[k] = _lib.StepDesc(int(bool(st.get("nlgeom", False))), int(st.get("solver", 0)),
+                                   (C.c_double * 4)(*st.get("increment", (1.0, 1.0, 1e-5, 1.0))),
+                                   int(st.get("max_increments", 10000)), nl, lp, nb, bp)
+        d.n_steps, d.steps = len(steps), C.cast(sts, C.c_void_p)
+        d.default_temperature = float(default_temperature)
+        if initial_temperatures:
+            ti = arr(list(initial_temperatures.keys()), np.int64)
+            tv = arr(list(initial_temperatures.values()), np.float64)
+            d.n_initial_temperatures, d.initial_temperature_ids, d.initial_temperatures = ti.size, ptr(ti), ptr(tv)
+        h = C.c_void_p()
+        _check(lib.fx_model_from_arrays(ctx.handle if ctx else None, C.byref(d), C.byref(h)), ctx)
+        p = cls(h, ctx)
+        p._default_t = float(default_temperature)
+        return p
 
     @classmethod
     def from_jobname(cls, jobname: str, ctx: Optional[Context] = None) -> "Project":
@@ -395,6 +501,14 @@ class Server:
         self.handle = h
         self._pending = {}  # ticket -> project (kept alive while the server uses it)
 
+    def info(self) -> dict:
+        """fx_server_get_info: slots, kernels the slot contexts found loaded, admission budget,
+        device pool bytes held after the budget's reservation and its outcome (1 grew, 0 held
+        enough already, -1 could not grow in one piece)."""
+        i = _lib.ServerInfo()
+        _check(self.lib.fx_server_get_info(self.handle, C.byref(i)), None, "fx_server_get_info")
+        return {k: getattr(i, k) for k, _ in i._fields_}
+
     def submit(self, project: "Project") -> int:
         if project.ctx is not None:
             raise ValueError("submit a host-only project (Project.from_inp_text(text) without a context)")
@@ -416,7 +530,8 @@ class Server:
         out = {"status": res.status, "slot": res.slot, "queue_ms": res.queue_ms, "service_ms": res.service_ms,
                "latency_ms": res.latency_ms, "footprint_bytes": res.footprint_bytes,
                "admit_at_ms": res.admit_at_ms, "done_at_ms": res.done_at_ms,
-               "stats": res.stats.as_dict(), "error": res.error.decode(errors="replace")}
+               "stats": res.stats.as_dict(), "error": res.error.decode(errors="replace"),
+               "setup_ms": res.setup_ms, "solve_ms": res.solve_ms, "finish_ms": res.finish_ms}
         return (u if res.status == 0 else None), out
 
     def close(self):

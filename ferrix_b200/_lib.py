@@ -30,7 +30,8 @@ class SolveOpts(C.Structure):
                 ("reliable_delta", C.c_double), ("use_graphs", C.c_int), ("verbose", C.c_int),
                 ("reference_iterative", C.c_int), ("preconditioner", C.c_int),
                 ("amg_aggregate_nodes", C.c_int), ("amg_smoother_degree", C.c_int), ("amg_cycle", C.c_int),
-                ("amg_smoother", C.c_int), ("amg_overcorrect", C.c_double), ("amg_cheb_ratio", C.c_double)]
+                ("amg_smoother", C.c_int), ("amg_overcorrect", C.c_double), ("amg_cheb_ratio", C.c_double),
+                ("amg_persistent_max_dof", C.c_int)]
 
 
 class StepStats(C.Structure):
@@ -53,7 +54,55 @@ class RequestResult(C.Structure):
     _fields_ = [("status", C.c_int), ("slot", C.c_int), ("queue_ms", C.c_double), ("service_ms", C.c_double),
                 ("latency_ms", C.c_double), ("footprint_bytes", C.c_double), ("admit_at_ms", C.c_double),
                 ("done_at_ms", C.c_double), ("stats", StepStats),
-                ("error", C.c_char * 256)]
+                ("error", C.c_char * 256), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
+                ("finish_ms", C.c_double)]
+
+
+class ErrorDetail(C.Structure):
+    _fields_ = [("status", C.c_int), ("line", C.c_int64), ("id", C.c_int64), ("text", C.c_char * 512),
+                ("message", C.c_char * 768)]
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("slots", C.c_int), ("preloaded_kernels", C.c_int), ("budget_bytes", C.c_double),
+                ("pool_reserved_bytes", C.c_double), ("reservation", C.c_int)]
+
+
+class LutDesc(C.Structure):
+    _fields_ = [("n", C.c_int64), ("temperature", C.c_void_p), ("value", C.c_void_p)]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("youngs_modulus", LutDesc), ("poisson_ratio", LutDesc),
+                ("thermal_expansion", LutDesc), ("reference_temperature", C.c_double)]
+
+
+class AmplitudeDesc(C.Structure):
+    _fields_ = [("n", C.c_int64), ("time", C.c_void_p), ("value", C.c_void_p), ("total_time", C.c_int),
+                ("shift_x", C.c_double), ("shift_y", C.c_double)]
+
+
+class RecordDesc(C.Structure):
+    _fields_ = [("node_id", C.c_int64), ("dof", C.c_int32), ("amplitude", C.c_int32), ("value", C.c_double),
+                ("origin_step", C.c_int64)]
+
+
+class StepDesc(C.Structure):
+    _fields_ = [("nlgeom", C.c_int), ("solver", C.c_int), ("increment", C.c_double * 4),
+                ("max_increments", C.c_int64), ("n_loads", C.c_int64), ("loads", C.c_void_p),
+                ("n_bcs", C.c_int64), ("bcs", C.c_void_p)]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_nodes", C.c_int64), ("node_ids", C.c_void_p), ("xyz", C.c_void_p),
+                ("n_c3d4", C.c_int64), ("c3d4_ids", C.c_void_p), ("c3d4_nodes", C.c_void_p),
+                ("c3d4_material", C.c_void_p),
+                ("n_c3d20", C.c_int64), ("c3d20_ids", C.c_void_p), ("c3d20_nodes", C.c_void_p),
+                ("c3d20_material", C.c_void_p),
+                ("n_materials", C.c_int), ("materials", C.c_void_p), ("n_amplitudes", C.c_int),
+                ("amplitudes", C.c_void_p), ("n_steps", C.c_int), ("steps", C.c_void_p),
+                ("default_temperature", C.c_double), ("n_initial_temperatures", C.c_int64),
+                ("initial_temperature_ids", C.c_void_p), ("initial_temperatures", C.c_void_p)]
 
 
 # name -> (restype, argtypes); every symbol of include/ferrix_b200.h
@@ -64,9 +113,12 @@ SIGNATURES = {
     "fx_ctx_create": (C.c_int, [C.c_int, C.POINTER(P)]),
     "fx_ctx_destroy": (None, [P]),
     "fx_ctx_last_error": (C.c_char_p, [P]),
+    "fx_last_error_detail": (C.c_int, [P, C.POINTER(ErrorDetail)]),
+    "fx_ctx_preloaded_kernels": (C.c_int, [P]),
     "fx_ctx_kernel_launches": (C.c_int64, [P]),
     "fx_ctx_stream": (C.c_void_p, [P]),
     "fx_model_from_inp": (C.c_int, [P, C.c_char_p, C.c_size_t, C.POINTER(P)]),
+    "fx_model_from_arrays": (C.c_int, [P, C.POINTER(MeshDesc), C.POINTER(P)]),
     "fx_model_destroy": (None, [P]),
     "fx_model_sizes": (C.c_int, [P, I64P, I64P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fx_model_node_ids": (C.c_int, [P, P]),
@@ -95,6 +147,7 @@ SIGNATURES = {
     "fx_server_create": (C.c_int, [C.POINTER(ServerOpts), P]),
     "fx_server_submit": (C.c_int, [P, P, C.POINTER(C.c_int64)]),
     "fx_server_wait": (C.c_int, [P, C.c_int64, C.c_double, P, C.POINTER(RequestResult)]),
+    "fx_server_get_info": (C.c_int, [P, C.POINTER(ServerInfo)]),
     "fx_server_destroy": (None, [P]),
     "fx_spmv_dot_noalloc": (C.c_int, [C.c_int, C.c_int64, P, P, P, P, P, P, P]),
 }

@@ -1881,9 +1881,67 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
     return ms;
 }
 
-int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
-                  double cell0, const double* b, double* x, const PcgOptions& opt, cudaStream_t s,
-                  int64_t* launches, long long* iters, double* relres, AmgStats* st, bool reuse) {
+void Amg::describe(ClInst& o) const {
+    const AmgLevel& l0 = L[0];
+    o.n = l0.n;
+    o.levels = (int)L.size();
+    o.goff = l0.S0->goff.ptr;
+    o.cols = l0.S0->cols.ptr;
+    o.vals64 = l0.vals0;
+    o.vals32 = vals0_f32_;
+    o.dinv0 = l0.dinv0;
+    o.agg = l0.agg.ptr;
+    o.agg_ptr = l0.agg_ptr.ptr;
+    o.agg_nodes = l0.agg_nodes.ptr;
+    o.Q = l0.Q.ptr;
+    o.n_agg = l0.n_agg;
+    o.lr = l0.r.ptr;
+    o.lx = l0.x.ptr;
+    o.ld = l0.d.ptr;
+    o.lt = l0.t.ptr;
+    o.d4a = l0.d4a.ptr;
+    o.d4b = l0.d4b.ptr;
+    o.x4 = l0.x4.ptr;
+    const ChebCoef k0 = cheb_coef(l0.lmax, degree_, cheb_kind_, cheb_ratio_);
+    o.c2_start = k0.c2_start;
+    for (int i = 0; i < 8; ++i) {
+        o.c1[i] = k0.c1[i];
+        o.c2[i] = k0.c2[i];
+    }
+    for (size_t m = 1; m < L.size() && m < (size_t)kClMaxLevels; ++m) {
+        const AmgLevel& l = L[m];
+        ClLevel& c = o.lev[m];
+        c.n = l.n;
+        c.coarsest = l.coarsest ? 1 : 0;
+        c.n_agg = l.n_agg;
+        c.row_ptr = l.row_ptr.ptr;
+        c.cols = l.cols.ptr;
+        c.vals = l.vals.ptr;
+        c.dinv = l.dinv.ptr;
+        c.dense_inv = l.dense_inv.ptr;
+        c.agg = l.agg.ptr;
+        c.agg_ptr = l.agg_ptr.ptr;
+        c.agg_nodes = l.agg_nodes.ptr;
+        c.Q = l.Q.ptr;
+        c.x = l.x.ptr;
+        c.b = l.b.ptr;
+        c.r = l.r.ptr;
+        c.d = l.d.ptr;
+        c.t = l.t.ptr;
+        c.xs = l.xs.ptr;
+        if (!l.coarsest) {
+            const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
+            c.c2_start = k.c2_start;
+            for (int i = 0; i < 8; ++i) {
+                c.c1[i] = k.c1[i];
+                c.c2[i] = k.c2[i];
+            }
+        }
+    }
+}
+
+void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
+                     double cell0, const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse) {
     const int n = S.n_rows;
     const int64_t nd = 3 * (int64_t)n;
     if (opt.amg_degree < 1 || opt.amg_degree > 8) fail(FX_INVALID_ARGUMENT, "multigrid smoother degree must be 1..8");
@@ -1906,6 +1964,9 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     amg.set_smoother_kind(opt.amg_cheb_kind);
     amg.set_overcorrect(opt.amg_overcorrect);
     amg.set_cheb_ratio(opt.amg_cheb_ratio);
+    S_ = &S;
+    vals64_ = vals64;
+    dinv64_ = dinv64;
     r_.alloc(nd, s);
     z_.alloc(nd, s);
     p_.alloc(nd, s);
@@ -1917,6 +1978,42 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     sc_.zero(s);
     counter_.alloc(1, s);
     counter_.zero(s);
+}
+
+ClInst AmgPcg::describe(const double* b, double* x) const {
+    ClInst o{};
+    amg.describe(o);
+    o.b = b;
+    o.x = x;
+    o.r = r_.ptr;
+    o.z = z_.ptr;
+    o.p = p_.ptr;
+    o.q = q_.ptr;
+    return o;
+}
+
+double AmgPcg::true_relres(const double* b, const double* x, cudaStream_t s) {
+    const int n = S_->n_rows;
+    const int nb = 296;
+    level_spmv(amg.L[0], x, b, q_.ptr, s);
+    FX_LAUNCH(k_rdr_part, nb, 256, 0, s, n, q_.ptr, dinv64_, part_.ptr);
+    FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr, 1);
+    FX_LAUNCH(k_rdr_part, nb, 256, 0, s, n, b, dinv64_, part_.ptr);
+    FX_LAUNCH(k_fin, 1, 32, 0, s, nb, part_.ptr, sc_.ptr + 4, 1);
+    double h[8];
+    FX_CUDA_CHECK(cudaMemcpyAsync(h, sc_.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    stream_wait(s, "amg true residual");
+    return h[6] > 0.0 ? std::sqrt(std::max(0.0, h[2]) / h[6]) : 0.0;
+}
+
+int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
+                  double cell0, const double* b, double* x, const PcgOptions& opt, cudaStream_t s,
+                  int64_t* launches, long long* iters, double* relres, AmgStats* st, bool reuse) {
+    const int n = S.n_rows;
+    const int64_t nd = 3 * (int64_t)n;
+    prepare(S, vals64, dinv64, xyz, cell0, opt, s, st, reuse);
+    const int nb = 296;
+    const unsigned g0 = l0_grid(n);
     FX_CUDA_CHECK(cudaMemsetAsync(x, 0, nd * sizeof(double), s));
     FX_CUDA_CHECK(cudaMemcpyAsync(r_.ptr, b, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
     // ||b||_D, z = V(b) with r.z, p = z

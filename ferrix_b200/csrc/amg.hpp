@@ -26,6 +26,8 @@
 
 namespace fx {
 
+struct ClInst;
+
 struct AmgLevel {
     int n = 0;   // block rows (nodes at level 0, aggregates above)
     int bs = 3;  // block size
@@ -113,6 +115,10 @@ class Amg {
         double c2;
     };
     Start0 start0() const;
+    // the hierarchy, smoother coefficients and work vectors, for the persistent solve
+    void describe(ClInst& out) const;
+    int degree() const { return degree_; }
+    double overcorrect() const { return alpha_; }
     std::vector<AmgLevel> L;
 
    private:
@@ -134,6 +140,59 @@ class Amg {
     DBuf<double> red_;  // reduction scratch
 };
 
+// ---- persistent solve of small systems (amg_cluster.cu)
+// The whole multigrid-preconditioned CG of one system runs inside one thread-block
+// cluster: every CG step and V-cycle phase is a loop over the cluster's threads,
+// phases are separated by hardware cluster barriers, dot products are summed per
+// CTA and across the cluster through distributed shared memory in a fixed order.
+// One launch advances any number of systems (one cluster each); a system's
+// arithmetic does not depend on the others, so it is the same alone and in a batch.
+constexpr int kClMaxLevels = 8;
+
+struct ClLevel {  // coarse level m >= 1 (6x6 blocks) and its transfer to level m + 1
+    int n = 0, coarsest = 0, n_agg = 0;
+    const int32_t *row_ptr = nullptr, *cols = nullptr;
+    const double *vals = nullptr, *dinv = nullptr, *dense_inv = nullptr;
+    const int32_t *agg = nullptr, *agg_ptr = nullptr, *agg_nodes = nullptr;
+    const double* Q = nullptr;
+    double *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr, *xs = nullptr;
+    double c2_start = 0.0, c1[8] = {}, c2[8] = {};
+};
+
+struct ClInst {
+    int n = 0, levels = 0;
+    // level 0: planar BSR3 (FP64 values; FP32 copy for the smoother or null), 3x3 block inverses
+    const int32_t *goff = nullptr, *cols = nullptr;
+    const double* vals64 = nullptr;
+    const float* vals32 = nullptr;
+    const double* dinv0 = nullptr;
+    const int32_t *agg = nullptr, *agg_ptr = nullptr, *agg_nodes = nullptr;
+    const double* Q = nullptr;
+    int n_agg = 0;
+    double *lr = nullptr, *lx = nullptr, *ld = nullptr, *lt = nullptr;
+    float *d4a = nullptr, *d4b = nullptr, *x4 = nullptr;
+    double c2_start = 0.0, c1[8] = {}, c2[8] = {};
+    // the CG: right-hand side, iterate and work vectors (3n each)
+    const double* b = nullptr;
+    double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+    ClLevel lev[kClMaxLevels];
+};
+
+struct ClResult {
+    long long iterations;
+    int status;  // FX_OK, FX_NUMERICAL (breakdown), FX_CONVERGENCE (max_iter)
+    int pad;
+    double rzd, bd;  // r.D^-1 r at the end and b.D^-1 b
+};
+
+// Launches the persistent solve of `n` systems (descriptors and results in device
+// memory); fp32: level-0 smoothing with the FP32 values. Smoother degree 1..8,
+// coarse corrections scaled by alpha.
+void launch_amg_cluster(const ClInst* insts, ClResult* res, int n, bool fp32, double rtol, int max_iter, int degree,
+                        double alpha, cudaStream_t s);
+// Systems of at most this many DOF are solved by the persistent launch by default.
+constexpr int64_t kClDefaultMaxDof = 100000;
+
 // CG on the FP64 BSR3 system preconditioned by one V-cycle per iteration.
 // CUDA-event time (ms per launch) of the fused fine-level Chebyshev step (SpMV +
 // smoother update) on the given FP64 system, with FP32 values when fp32; bytes =
@@ -143,6 +202,13 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
 
 class AmgPcg {
    public:
+    // For the persistent solve: set up (or refresh) the hierarchy for the system and
+    // allocate the CG vectors, without iterating; then describe it for the kernel.
+    void prepare(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz, double cell0,
+                 const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse);
+    ClInst describe(const double* b, double* x) const;
+    // ||b - A x||_D / ||b||_D of the assembled FP64 system after a persistent solve
+    double true_relres(const double* b, const double* x, cudaStream_t s);
     // reuse: keep the hierarchy's aggregates, prolongators and coarse patterns when
     // the last setup was on the same structure S (only the values are refreshed)
     int solve(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz, double cell0,
@@ -151,6 +217,9 @@ class AmgPcg {
     Amg amg;
 
    private:
+    const BsrStructure* S_ = nullptr;
+    const double* vals64_ = nullptr;
+    const double* dinv64_ = nullptr;
     DBuf<double> r_, z_, z2_, p_, q_, part_, sc_;
     DBuf<float> vals32_;
     DBuf<int> counter_;

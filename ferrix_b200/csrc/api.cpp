@@ -3,10 +3,11 @@
 // fx_ctx_last_error.
 #include <cuda.h>
 
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <new>
-#include <set>
+#include <map>
 #include <vector>
 
 #include "engine.hpp"
@@ -45,14 +46,42 @@ static double profile_t(fx_model* m, int reps, double* bytes) {
 
 namespace fx {
 
+ErrorRecord& thread_error() {
+    static thread_local ErrorRecord rec;
+    return rec;
+}
+
+// The display prefixes of FerrixError (src/solver/error.rs:12-72) whose variant
+// carries only a message string: the payload is the text after the prefix.
+static std::string strip_variant_prefix(const std::string& m) {
+    for (const char* p : {"Mathematical error: ", "Solver failed to converge: ", "Invalid model state: ",
+                          "Generic error: ", "Generic IO error: "})
+        if (m.rfind(p, 0) == 0) return m.substr(std::strlen(p));
+    return m;
+}
+
+void ErrorRecord::set(const Error& e) {
+    status = e.status;
+    line = e.line;
+    id = e.id;
+    message = e.what();
+    text = e.text.empty() ? strip_variant_prefix(message) : e.text;
+}
+
+void ErrorRecord::set(int st, const std::string& msg) { set(Error(st, msg)); }
+
 // Loads every kernel of the library's modules on `device` (CUDA 12.4 driver
 // entry points, looked up at run time; without them, or on any error, kernels
-// load at their first launch as before).
-void preload_kernels(int device) {
+// load at their first launch as before). Returns the number of kernels the
+// first call on this device loaded (later calls return the same count), -1
+// when the driver entry points are missing.
+int preload_kernels(int device) {
     static std::mutex mu;
-    static std::set<int> done;
+    static std::map<int, int> done;
     std::lock_guard<std::mutex> g(mu);
-    if (!done.insert(device).second) return;
+    auto it = done.find(device);
+    if (it != done.end()) return it->second;
+    int loaded = -1;
     using GetModule = CUresult (*)(CUmodule*, CUfunction);
     using Count = CUresult (*)(unsigned int*, CUmodule);
     using Enumerate = CUresult (*)(CUfunction*, unsigned int, CUmodule);
@@ -68,7 +97,9 @@ void preload_kernels(int device) {
                     cudaGetDriverEntryPointByVersion("cuFuncLoad", &p_load, 12040, cudaEnableDefault, &q) ==
                         cudaSuccess && p_load;
     if (ok) {
-        for (const void* anchor : {kernels_anchor_amg(), kernels_anchor_assembly(), kernels_anchor_csr_solve(),
+        loaded = 0;
+        for (const void* anchor : {kernels_anchor_amg(), kernels_anchor_amg_cluster(), kernels_anchor_assembly(),
+                                   kernels_anchor_csr_solve(),
                                    kernels_anchor_elements(), kernels_anchor_noalloc(), kernels_anchor_pcg(),
                                    kernels_anchor_pcg_csr(), kernels_anchor_vectors()}) {
             cudaFunction_t f = nullptr;
@@ -80,10 +111,13 @@ void preload_kernels(int device) {
                 continue;
             std::vector<CUfunction> fns(n);
             if (n == 0 || reinterpret_cast<Enumerate>(p_enum)(fns.data(), n, mod) != CUDA_SUCCESS) continue;
-            for (CUfunction fn : fns) reinterpret_cast<Load>(p_load)(fn);
+            for (CUfunction fn : fns)
+                if (reinterpret_cast<Load>(p_load)(fn) == CUDA_SUCCESS) ++loaded;
         }
     }
     cudaGetLastError();
+    done[device] = loaded;
+    return loaded;
 }
 
 }  // namespace fx
@@ -107,6 +141,7 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->amg_smoother = 0;
     o->amg_overcorrect = 0.0;
     o->amg_cheb_ratio = 0.0;
+    o->amg_persistent_max_dof = 0;
 }
 
 int fx_ctx_create(int device, fx_ctx** out) {
@@ -121,7 +156,7 @@ int fx_ctx_create(int device, fx_ctx** out) {
         c->device = device;
         FX_CUDA_CHECK(cudaSetDevice(device));
         FX_CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-        preload_kernels(device);
+        c->preload_functions = preload_kernels(device);
         // keep freed stream-ordered allocations in this process's pool between solves
         // instead of returning them to the driver at every synchronisation
         cudaMemPool_t pool;
@@ -153,6 +188,19 @@ void fx_ctx_destroy(fx_ctx* ctx) {
 }
 
 const char* fx_ctx_last_error(const fx_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int fx_last_error_detail(const fx_ctx* ctx, fx_error_detail* out) {
+    if (!out) return FX_INVALID_ARGUMENT;
+    const ErrorRecord& r = ctx ? ctx->last_detail : thread_error();
+    out->status = r.status;
+    out->line = r.line;
+    out->id = r.id;
+    std::snprintf(out->text, sizeof(out->text), "%s", r.text.c_str());
+    std::snprintf(out->message, sizeof(out->message), "%s", r.message.c_str());
+    return FX_OK;
+}
+
+int fx_ctx_preloaded_kernels(const fx_ctx* ctx) { return ctx ? ctx->preload_functions : -1; }
 
 int64_t fx_ctx_kernel_launches(const fx_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
@@ -332,7 +380,7 @@ int fx_assemble_csr(fx_model* m, const double* u, int precision, int64_t* nnz, i
             ~R() { g_launch_counter = v; }
         } r{saved};
         ensure_dense(m);
-        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        if (m->dense.missing_node_id >= 0) fail_detail(FX_NODE_NOT_FOUND, m->dense.missing_node_error, -1, m->dense.missing_node_id, "");
         ensure_structure(m);
         ModelDev& d = m->dev;
         cudaStream_t s = ctx->stream;
@@ -380,7 +428,7 @@ static int force_common(fx_model* m, const double* u, const double* uconf, doubl
             ~R() { g_launch_counter = v; }
         } r{saved};
         ensure_dense(m);
-        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        if (m->dense.missing_node_id >= 0) fail_detail(FX_NODE_NOT_FOUND, m->dense.missing_node_error, -1, m->dense.missing_node_id, "");
         ensure_structure(m);
         cudaStream_t s = ctx->stream;
         const size_t n3 = 3 * (size_t)m->dense.n_nodes;
@@ -435,7 +483,7 @@ int fx_profile_spmv(fx_model* m, int precision, int reps, double* ms, double* by
             ~R() { g_launch_counter = v; }
         } r{saved};
         ensure_dense(m);
-        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        if (m->dense.missing_node_id >= 0) fail_detail(FX_NODE_NOT_FOUND, m->dense.missing_node_error, -1, m->dense.missing_node_id, "");
         ensure_structure(m);
         *ms = precision == FX_PREC_MIXED ? profile_t<float>(m, reps, bytes) : profile_t<double>(m, reps, bytes);
         return FX_OK;
@@ -453,7 +501,7 @@ int fx_profile_smoother(fx_model* m, int precision, int reps, double* ms, double
             ~R() { g_launch_counter = v; }
         } r{saved};
         ensure_dense(m);
-        if (m->dense.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, m->dense.missing_node_error);
+        if (m->dense.missing_node_id >= 0) fail_detail(FX_NODE_NOT_FOUND, m->dense.missing_node_error, -1, m->dense.missing_node_id, "");
         ensure_structure(m);
         ModelDev& d = m->dev;
         cudaStream_t s = m->ctx->stream;

@@ -124,6 +124,9 @@ void build_bsr_structure(const ElemView& g4, const ElemView& g20, int n_nodes, B
     const int64_t P = p4 + p20;
     if ((int64_t)g4.n * kPairs4 + (int64_t)g20.n * kPairs20 >= (int64_t(1) << 31))
         fail(FX_INVALID_ARGUMENT, "mesh too large for 31-bit element-pair slots");
+    // the sort items (ordered node pairs of every element) are counted, scanned and
+    // indexed in 32 bits: about twice the slots, so this bound is the tighter one
+    if (P >= (int64_t(1) << 31)) fail(FX_INVALID_ARGUMENT, "mesh too large for 32-bit node-pair sort items");
     S.n_pairs = P;
     const int nb = bits_for(n_nodes > 1 ? n_nodes : 2);
     DBuf<uint64_t> keys, keys_s;

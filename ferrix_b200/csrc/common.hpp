@@ -14,13 +14,34 @@
 
 namespace fx {
 
-// FerrixError (src/solver/error.rs:12-72) as a C++ exception carrying an fx_status.
+// FerrixError (src/solver/error.rs:12-72) as a C++ exception carrying an fx_status
+// and the variant's payload: the deck line of ParseError / UnsupportedKeyword,
+// the id of NodeNotFound / ElementNotFound, and the string field (message,
+// keyword, material / set / solver name, path). `text` empty = the display
+// message without its variant prefix.
 struct Error : std::runtime_error {
     int status;
+    int64_t line = -1, id = -1;
+    std::string text;
     Error(int s, const std::string& msg) : std::runtime_error(msg), status(s) {}
+    Error(int s, const std::string& msg, int64_t line_, int64_t id_, std::string text_)
+        : std::runtime_error(msg), status(s), line(line_), id(id_), text(std::move(text_)) {}
 };
 
 [[noreturn]] inline void fail(int status, const std::string& msg) { throw Error(status, msg); }
+[[noreturn]] inline void fail_detail(int status, const std::string& msg, int64_t line, int64_t id,
+                                     const std::string& text) {
+    throw Error(status, msg, line, id, text);
+}
+
+// The last failure an entry point reported, with its payload (fx_last_error_detail).
+struct ErrorRecord {
+    int status = FX_OK;
+    int64_t line = -1, id = -1;
+    std::string text, message;
+    void set(const Error& e);
+    void set(int status, const std::string& message);
+};
 
 #define FX_CUDA_CHECK(expr)                                                                          \
     do {                                                                                             \

@@ -23,6 +23,8 @@ __global__ void k_csr_residual(int64_t n, const int64_t* __restrict__ ip, const 
     if (lane == 0) r[row] = b[row] - acc;
 }
 
+constexpr int kStagnated = -1;
+
 template <typename T>
 static int solve_csr_t(fx_ctx* ctx, int64_t n, const int64_t* ip, const int64_t* ind, const double* data,
                        const double* b, double* x, const fx_solve_opts& o, fx_step_stats* st) {
@@ -114,7 +116,7 @@ static int solve_csr_t(fx_ctx* ctx, int64_t n, const int64_t* ip, const int64_t*
         FX_LAUNCH(k_csr_residual, (unsigned)((n3 * 32 + 255) / 256), 256, 0, ss, n3, pip, pind, pdat, xx, bb, r);
     };
     PcgOptions po;
-    po.rtol = o.rtol;
+    po.rtol = sizeof(T) == 4 ? o.rtol * kMixedBjResidualFactor : o.rtol;
     po.max_iter = o.max_iter;
     po.poll = o.poll_interval;
     po.reliable_delta = o.reliable_delta;
@@ -140,10 +142,53 @@ static int solve_csr_t(fx_ctx* ctx, int64_t n, const int64_t* ip, const int64_t*
         st->bsr_blocks = S.n_blocks;
     }
     if (sys.status == FX_NUMERICAL) fail(FX_NUMERICAL, "Mathematical error: PCG breakdown (matrix not positive definite)");
+    if (sys.stagnated) return kStagnated;  // FP32 refinement stopped improving: the caller finishes in FP64
     if (sys.status == FX_CONVERGENCE)
         fail(FX_CONVERGENCE, "Solver failed to converge: PCG did not converge after " + std::to_string(sys.iterations) +
                                  " iterations");
     return sys.status;
+}
+
+// Scalar-CSR Jacobi PCG on the caller's matrix as given: the reference
+// IterativeSolver (absolute sqrt(r.z) < tol, iterative.rs:26-136) when
+// `absolute`, else the plain FP64 PCG with the relative stopping test.
+static int solve_csr_scalar(fx_ctx* ctx, int64_t n, const int64_t* ip, const int64_t* ind, const double* data,
+                            const double* b, double* x, const fx_solve_opts& o, bool absolute, fx_step_stats* st) {
+    cudaStream_t s = ctx->stream;
+    if (n >= (int64_t(1) << 31)) fail(FX_INVALID_ARGUMENT, "matrix too large");
+    for (int64_t k = 0; k < ip[n]; ++k)
+        if (ind[k] < 0 || ind[k] >= n) fail(FX_INVALID_ARGUMENT, "column index out of range");
+    CsrSystem A;
+    A.from_host(n, ip, ind, data, s);
+    DBuf<double> d_b, d_x;
+    d_b.upload(b, (size_t)n, s);
+    d_x.alloc((size_t)n, s);
+    PcgOptions po;
+    po.rtol = o.rtol;
+    po.max_iter = o.max_iter;
+    po.poll = o.poll_interval;
+    po.graphs = o.use_graphs != 0;
+    long long iters = 0;
+    double relres = 0.0;
+    EventTimer t;
+    t.start(s);
+    const int rc = ctx->pcgcsr.solve(A, d_b.ptr, d_x.ptr, po, absolute, s, &ctx->launches, &iters, &relres);
+    const double ms = t.stop_ms(s);
+    d_x.download(x, (size_t)n, s);
+    FX_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (st) {
+        *st = fx_step_stats{};
+        st->linear_solves = 1;
+        st->pcg_iterations = iters;
+        st->last_linear_relres = relres;
+        st->t_pcg_ms = ms;
+        st->t_total_ms = ms;
+    }
+    if (rc == FX_NUMERICAL) fail(FX_NUMERICAL, "Mathematical error: PCG breakdown (matrix not positive definite)");
+    if (rc == FX_CONVERGENCE)
+        fail(FX_CONVERGENCE,
+             "Solver failed to converge: PCG did not converge after " + std::to_string(o.max_iter) + " iterations");
+    return rc;
 }
 
 // A kernel of this file's module (preload_kernels() loads all of the module's kernels).
@@ -168,13 +213,33 @@ extern "C" int fx_solve_csr(fx_ctx* ctx, int64_t n, const int64_t* indptr, const
             int64_t* v;
             ~R() { g_launch_counter = v; }
         } r{saved};
+        if (o.reference_iterative || o.precision == FX_PREC_FP64_CSR)
+            return solve_csr_scalar(ctx, n, indptr, indices, data, b, x, o, o.reference_iterative != 0, stats);
         if (o.precision == FX_PREC_FP64) return solve_csr_t<double>(ctx, n, indptr, indices, data, b, x, o, stats);
-        return solve_csr_t<float>(ctx, n, indptr, indices, data, b, x, o, stats);
+        const int rc = solve_csr_t<float>(ctx, n, indptr, indices, data, b, x, o, stats);
+        if (rc != kStagnated) return rc;
+        fx_step_stats first{};
+        if (stats) first = *stats;
+        fx_solve_opts o64 = o;  // the mixed solve's FP64 target
+        o64.rtol = o.rtol * kMixedBjResidualFactor;
+        const int rc64 = solve_csr_t<double>(ctx, n, indptr, indices, data, b, x, o64, stats);
+        if (stats) {
+            stats->pcg_iterations += first.pcg_iterations;
+            stats->reliable_updates += first.reliable_updates;
+            stats->t_pcg_ms += first.t_pcg_ms;
+            stats->t_total_ms += first.t_total_ms;
+            stats->fp64_fallbacks = 1;
+        }
+        return rc64;
     } catch (const Error& e) {
         ctx->last_error = e.what();
+        ctx->last_detail.set(e);
+        thread_error().set(e);
         return e.status;
     } catch (const std::exception& e) {
         ctx->last_error = e.what();
+        ctx->last_detail.set(FX_GENERIC, e.what());
+        thread_error().set(FX_GENERIC, e.what());
         return FX_GENERIC;
     }
 }

@@ -84,30 +84,42 @@ double model_slack(const DenseModel& D) { return 1.5 * model_footprint(D) + 256.
 // streams are in flight stalls those too (requests of 7k DOF took 0.3-0.5 s
 // instead of 10 ms in a four-slot request loop). One allocation before any work
 // is queued cost about 12 ms per GB.
-void reserve_pool(int device, cudaStream_t s, double bytes) {
-    if (!(bytes > 0.0)) return;
+int reserve_pool(int device, cudaStream_t s, double bytes) {
+    if (!(bytes > 0.0)) return 0;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) {
         cudaGetLastError();
-        return;
+        return -1;
     }
     uint64_t keep = UINT64_MAX, reserved = 0, used = 0;  // the pool keeps freed memory (fx_ctx_create sets the same)
     if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess ||
         cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
         cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
         cudaGetLastError();
-        return;
+        return -1;
     }
     const double spare = (double)reserved - (double)used;
-    if (spare >= bytes) return;
+    if (spare >= bytes) return 0;
     const size_t granule = (size_t)2 << 20;
     const size_t want = ((size_t)(bytes - spare) + granule - 1) / granule * granule;
     void* p = nullptr;
     if (cudaMallocAsync(&p, want, s) != cudaSuccess) {
         cudaGetLastError();  // not enough memory in one piece: the pool grows on demand instead
-        return;
+        return -1;
     }
     cudaFreeAsync(p, s);
+    return 1;
+}
+
+double pool_reserved_bytes(int device) {
+    cudaMemPool_t pool;
+    uint64_t reserved = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess) {
+        cudaGetLastError();
+        return -1.0;
+    }
+    return (double)reserved;
 }
 
 void upload_model(fx_model* m) {
@@ -187,7 +199,7 @@ void check_device_errors(fx_model* m, const char* where) {
 static void precheck(fx_model* m) {
     ensure_dense(m);
     const DenseModel& D = m->dense;
-    if (D.missing_node_id >= 0) fail(FX_NODE_NOT_FOUND, D.missing_node_error);
+    if (D.missing_node_id >= 0) fail_detail(FX_NODE_NOT_FOUND, D.missing_node_error, -1, D.missing_node_id, "");
     for (const ElemGroup* g : {&D.g4, &D.g20})
         for (int64_t k = 0; k < g->size(); ++k) {
             int mi = g->mat[k];
@@ -595,6 +607,8 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         const double oc = rs[0]->o.amg_overcorrect;
         po.amg_overcorrect = oc > 0.0 && oc < 2.0 ? oc : kAmgOvercorrect;
         po.amg_cheb_ratio = rs[0]->o.amg_cheb_ratio > 1.0 ? rs[0]->o.amg_cheb_ratio : kAmgChebRatio;
+        const int pm = rs[0]->o.amg_persistent_max_dof;
+        po.amg_persistent_max_dof = pm == 0 ? kClDefaultMaxDof : pm;
     }
     while (true) {
         bool any = false;
@@ -621,7 +635,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         if (solve.empty()) continue;
         EventTimer ph;
         ph.start(s);
-        std::vector<size_t> csr_ids, bsr_ids;
+        std::vector<size_t> csr_ids, bsr_ids, cluster_ids;
         for (size_t i : solve) (rs[i]->csr || rs[i]->amg ? csr_ids : bsr_ids).push_back(i);
         for (size_t i : csr_ids) {
             StepRunner& r = *rs[i];
@@ -631,9 +645,22 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
                 // hierarchy built at the increment's first tangent (aggregates and
                 // rigid-body prolongators of that configuration) and refresh its values
                 const bool reuse = r.step->nlgeom && r.it > 0;
-                r.csr_status = ctx->amgpcg.solve(r.m->dev.S, r.m->dev.vals64.ptr, r.m->dev.minv64.ptr,
-                                                 r.amg_xyz.ptr, r.amg_cell, r.m->dev.R.ptr, r.m->dev.du.ptr, po, s,
-                                                 &ctx->launches, &r.csr_iters, &r.csr_relres, &ast, reuse);
+                ModelDev& d = r.m->dev;
+                if (!d.amg) d.amg = std::make_unique<AmgPcg>();
+                const int64_t ndof = 3 * r.m->dense.n_nodes;
+                if (!po.amg_kcycle && po.amg_persistent_max_dof > 0 && ndof <= po.amg_persistent_max_dof) {
+                    // small system: hierarchy now, its whole CG in the round's persistent launch below
+                    guard(i, [&] {
+                        d.amg->prepare(d.S, d.vals64.ptr, d.minv64.ptr, r.amg_xyz.ptr, r.amg_cell, po, s, &ast,
+                                       reuse);
+                        r.S.amg_levels = ast.levels;
+                        r.S.amg_setup_ms += ast.setup_ms;
+                        cluster_ids.push_back(i);
+                    });
+                    continue;
+                }
+                r.csr_status = d.amg->solve(d.S, d.vals64.ptr, d.minv64.ptr, r.amg_xyz.ptr, r.amg_cell, d.R.ptr,
+                                            d.du.ptr, po, s, &ctx->launches, &r.csr_iters, &r.csr_relres, &ast, reuse);
                 r.S.amg_levels = ast.levels;
                 r.S.amg_setup_ms += ast.setup_ms;
                 continue;
@@ -646,6 +673,30 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
             r.csr_status = ctx->pcgcsr.solve(r.csr_sys, r.m->dev.R.ptr, r.m->dev.du.ptr, pc, r.csr_reference, s,
                                              &ctx->launches, &r.csr_iters, &r.csr_relres);
         }
+        if (!cluster_ids.empty()) {
+            // every small multigrid system of the round in one persistent launch (a cluster each)
+            std::vector<ClInst> desc;
+            for (size_t i : cluster_ids) desc.push_back(rs[i]->m->dev.amg->describe(rs[i]->m->dev.R.ptr,
+                                                                                    rs[i]->m->dev.du.ptr));
+            DBuf<ClInst> d_desc;
+            DBuf<ClResult> d_res;
+            d_desc.upload(desc, s);
+            d_res.alloc(desc.size(), s);
+            const AmgPcg& a0 = *rs[cluster_ids[0]]->m->dev.amg;
+            launch_amg_cluster(d_desc.ptr, d_res.ptr, (int)desc.size(), po.amg_fp32, po.rtol, po.max_iter,
+                               a0.amg.degree(), a0.amg.overcorrect(), s);
+            std::vector<ClResult> res(desc.size());
+            d_res.download(res.data(), res.size(), s);
+            stream_wait(s, "persistent multigrid CG");
+            for (size_t k = 0; k < cluster_ids.size(); ++k) {
+                StepRunner& r = *rs[cluster_ids[k]];
+                r.csr_status = res[k].status;
+                r.csr_iters = res[k].iterations;
+                guard(cluster_ids[k], [&] {
+                    r.csr_relres = r.m->dev.amg->true_relres(r.m->dev.R.ptr, r.m->dev.du.ptr, s);
+                });
+            }
+        }
         {
             std::vector<PcgSystem<double>*> v64;
             std::vector<PcgSystem<float>*> v32;
@@ -655,7 +706,9 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
             }
             if (!v64.empty()) ctx->pcg64.solve(v64, po, s, &ctx->launches);
             if (!v32.empty()) {
-                ctx->pcg32.solve(v32, po, s, &ctx->launches);
+                PcgOptions p32 = po;  // mixed: the tightened residual target, also for its FP64 finish
+                p32.rtol = po.rtol * kMixedBjResidualFactor;
+                ctx->pcg32.solve(v32, p32, s, &ctx->launches);
                 std::vector<PcgSystem<double>*> fb;
                 for (size_t i : bsr_ids)
                     if (!rs[i]->fp64 && rs[i]->sys32.stagnated)
@@ -663,7 +716,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
                             rs[i]->prepare_fp64_fallback();
                             fb.push_back(&rs[i]->sys64);
                         });
-                if (!fb.empty()) ctx->pcg64.solve(fb, po, s, &ctx->launches);
+                if (!fb.empty()) ctx->pcg64.solve(fb, p32, s, &ctx->launches);
             }
         }
         solve.swap(bsr_ids);

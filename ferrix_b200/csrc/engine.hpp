@@ -17,11 +17,12 @@ struct fx_ctx {
     cudaStream_t stream = nullptr;
     fx::DeviceTables tables;
     std::string last_error;
+    fx::ErrorRecord last_detail;
+    int preload_functions = -1;  // kernels loaded by fx_ctx_create on this device (-1: entry points missing)
     int64_t launches = 0;
     fx::PcgBatch<float> pcg32;
     fx::PcgBatch<double> pcg64;
     fx::CsrPcg pcgcsr;
-    fx::AmgPcg amgpcg;
 };
 
 namespace fx {
@@ -61,6 +62,9 @@ struct ModelDev {
     DBuf<double> norm_part, norm_out;
     DBuf<int32_t> load_dof;
     DBuf<double> load_val;
+    // the model's multigrid hierarchy and CG workspace (kept between Newton iterations,
+    // whose values are refreshed on it, and across steps until the structure changes)
+    std::unique_ptr<AmgPcg> amg;
     ElemView g4() const { return ElemView{(int)conn4.n / 4, conn4.ptr, mat4.ptr}; }
     ElemView g20() const { return ElemView{(int)conn20.n / 20, conn20.ptr, mat20.ptr}; }
 };
@@ -78,21 +82,33 @@ struct fx_model {
     fx::ModelDev dev;
 };
 
+namespace fx {
+// The calling thread's last failure (entry points called without a context,
+// e.g. fx_model_from_inp with ctx NULL, report here only).
+ErrorRecord& thread_error();
+}  // namespace fx
+
 // Runs an entry point's body: fx::Error and standard exceptions become status
-// codes, with the message stored as the context's last error.
+// codes, with the message stored as the context's last error and the message
+// and payload as the context's and the thread's last error detail.
 template <typename F>
 inline int guarded(fx_ctx* ctx, F&& f) {
+    auto record = [&](const fx::Error& e) {
+        fx::thread_error().set(e);
+        if (ctx) {
+            ctx->last_error = e.what();
+            ctx->last_detail.set(e);
+        }
+        return e.status;
+    };
     try {
         return f();
     } catch (const fx::Error& e) {
-        if (ctx) ctx->last_error = e.what();
-        return e.status;
+        return record(e);
     } catch (const std::bad_alloc&) {
-        if (ctx) ctx->last_error = "host allocation failed";
-        return FX_GENERIC;
+        return record(fx::Error(FX_GENERIC, "Generic error: host allocation failed"));
     } catch (const std::exception& e) {
-        if (ctx) ctx->last_error = e.what();
-        return FX_GENERIC;
+        return record(fx::Error(FX_GENERIC, e.what()));
     }
 }
 
@@ -104,6 +120,7 @@ void ensure_dense(fx_model* m);
 // module loading, a kernel's first launch would otherwise wait for the kernels
 // running on other streams.
 const void* kernels_anchor_amg();
+const void* kernels_anchor_amg_cluster();
 const void* kernels_anchor_assembly();
 const void* kernels_anchor_csr_solve();
 const void* kernels_anchor_elements();
@@ -111,7 +128,7 @@ const void* kernels_anchor_noalloc();
 const void* kernels_anchor_pcg();
 const void* kernels_anchor_pcg_csr();
 const void* kernels_anchor_vectors();
-void preload_kernels(int device);
+int preload_kernels(int device);
 // Device bytes of one model while it is solved (an upper estimate), and the
 // spare pool memory held for it (with slack for fragmentation).
 double model_footprint(const DenseModel& D);
@@ -119,8 +136,11 @@ double model_slack(const DenseModel& D);
 // Grows the device's stream-ordered memory pool (which keeps what it holds) so
 // that it has `bytes` more than it has in use, by one allocation queued on `s`
 // and freed again, before the caller queues any work. Best effort: a failed
-// allocation leaves the pool as it was.
-void reserve_pool(int device, cudaStream_t s, double bytes);
+// allocation leaves the pool as it was. Returns 1 when the pool grew, 0 when it
+// already held enough, -1 when it could not grow (it then grows on demand).
+int reserve_pool(int device, cudaStream_t s, double bytes);
+// Bytes the device's memory pool holds (reserved), -1 when it cannot be read.
+double pool_reserved_bytes(int device);
 void upload_model(fx_model* m);
 void ensure_structure(fx_model* m);
 void state_initialize(fx_model* m);

@@ -500,7 +500,8 @@ struct Parser {
     std::string ic_type;
 
     [[noreturn]] void perr(const std::string& msg) {
-        fail(FX_PARSE, "Parsing error at line " + std::to_string(line_nr) + ": " + msg);
+        fail_detail(FX_PARSE, "Parsing error at line " + std::to_string(line_nr) + ": " + msg, (int64_t)line_nr, -1,
+                    msg);
     }
     const std::string* peek() { return pos < views.size() ? &line_at(pos) : nullptr; }
 
@@ -600,7 +601,8 @@ struct Parser {
         std::string key = name;
         std::replace(key.begin(), key.end(), ' ', '_');
         if (!keywords().count(key))
-            fail(FX_UNSUPPORTED_KEYWORD, "Unsupported keyword at line " + std::to_string(line_nr) + ": " + name);
+            fail_detail(FX_UNSUPPORTED_KEYWORD, "Unsupported keyword at line " + std::to_string(line_nr) + ": " + name,
+                        (int64_t)line_nr, -1, name);
         kw = key;
         KwArgs ka = keyword_arguments(line);
         if (key == "ELEMENT") {
@@ -646,9 +648,9 @@ struct Parser {
                     midx = (int)i;
                     break;
                 }
-            if (midx < 0) fail(FX_MATERIAL_NOT_FOUND, "Material " + *mn + " not found");
+            if (midx < 0) fail_detail(FX_MATERIAL_NOT_FOUND, "Material " + *mn + " not found", -1, -1, *mn);
             auto it = p.element_sets.find(*es);
-            if (it == p.element_sets.end()) fail(FX_ELSET_NOT_FOUND, "Elset " + *es + " not found");
+            if (it == p.element_sets.end()) fail_detail(FX_ELSET_NOT_FOUND, "Elset " + *es + " not found", -1, -1, *es);
             for (int64_t eid : it->second) p.elem_material_lines.emplace_back(eid, midx);
         } else if (key == "STEP") {
             if (step_counter == 0) {
@@ -672,7 +674,7 @@ struct Parser {
                 if (sv) {
                     if (*sv == "DIRECT") st = SolverType::Direct;
                     else if (*sv == "ITERATIVE") st = SolverType::Iterative;
-                    else fail(FX_UNKNOWN_SOLVER, "Unknown solver type: " + *sv);
+                    else fail_detail(FX_UNKNOWN_SOLVER, "Unknown solver type: " + *sv, -1, -1, *sv);
                 }
                 ++pos;  // consume *STATIC
                 IncrementData incd;
@@ -807,15 +809,20 @@ struct Parser {
             nums.reserve(fields.size());
             for (auto s : fields) {
                 int64_t v;
-                if (!parse_usize_sv(s, &v)) fail(FX_PARSE, "Parsing error at line 0: Integer conversion failed");
+                if (!parse_usize_sv(s, &v))
+                    fail_detail(FX_PARSE, "Parsing error at line 0: Integer conversion failed", 0, -1,
+                                "Integer conversion failed");
                 nums.push_back(v);
             }
             int npe;
             if (elem_type == "C3D4") npe = 4;
             else if (elem_type == "C3D20") npe = 20;
-            else fail(FX_PARSE, "Parsing error at line 0: Unknown element definition: " + elem_type);
+            else
+                fail_detail(FX_PARSE, "Parsing error at line 0: Unknown element definition: " + elem_type, 0, -1,
+                            "Unknown element definition: " + elem_type);
             if ((int)nums.size() - 1 != npe)
-                fail(FX_PARSE, "Parsing error at line 0: Wrong node count for " + elem_type);
+                fail_detail(FX_PARSE, "Parsing error at line 0: Wrong node count for " + elem_type, 0, -1,
+                            "Wrong node count for " + elem_type);
             int64_t eid = nums[0];
             if (has_elset && !elset_name.empty()) p.element_sets[elset_name].push_back(eid);
             p.elem_line_ids.push_back(eid);

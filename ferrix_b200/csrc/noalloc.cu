@@ -26,6 +26,7 @@
 // scratch and give wrong results: order them on one stream or with events.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "common.hpp"
@@ -105,6 +106,12 @@ extern "C" int fx_spmv_dot_noalloc(int device, int64_t n, const int64_t* indptr,
                                    const double* data, const double* x, double* y, double* dot, void* stream) {
     if (n <= 0 || !indptr || !indices || !data || !x || !y || !dot) return FX_INVALID_ARGUMENT;
     if (n > kNaMaxRows) return FX_INVALID_ARGUMENT;  // beyond the scratch array: at most 524,288 rows
+    // y is written while other rows still read x: the two must not overlap
+    const uintptr_t xb = reinterpret_cast<uintptr_t>(x), yb = reinterpret_cast<uintptr_t>(y);
+    const uintptr_t nbytes = (uintptr_t)n * sizeof(double);
+    if (xb < yb + nbytes && yb < xb + nbytes) return FX_INVALID_ARGUMENT;
+    // an error left pending by the caller's own earlier CUDA calls is reported, not consumed
+    if (cudaPeekAtLastError() != cudaSuccess) return FX_CUDA;
     if (device < 0 || device >= kNaMaxDevices) return FX_INVALID_ARGUMENT;
     int current = -1;
     if (cudaGetDevice(&current) != cudaSuccess) return FX_CUDA;
@@ -130,7 +137,7 @@ extern "C" int fx_spmv_dot_noalloc(int device, int64_t n, const int64_t* indptr,
     if (rc == FX_OK) {
         const unsigned grid = (unsigned)((n + kNaRowsPerCta - 1) / kNaRowsPerCta);
         k_spmv_dot_noalloc<<<grid, 32 * kNaRowsPerCta, 0, s>>>(n, indptr, indices, data, x, y, dot, sc);
-        if (cudaGetLastError() != cudaSuccess) rc = FX_CUDA;
+        if (cudaGetLastError() != cudaSuccess) rc = FX_CUDA;  // no error was pending: this launch's own
     }
     if (current != device) cudaSetDevice(current);
     return rc;

@@ -1,4 +1,5 @@
 // Batched BSR3 PCG kernels and host loop (see pcg.hpp).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -9,7 +10,7 @@
 namespace fx {
 
 constexpr int kChunkRows = 256;   // rows per CTA work item
-constexpr int kSpmvThreads = 512; // 64 rows in flight, 8 lanes per row
+constexpr int kSpmvThreads = 256; // 32 rows per pass, 8 lanes per row
 constexpr int kUpdThreads = 256;  // one row per thread
 
 __device__ __forceinline__ void ld4(const float* p, int64_t i4, float o[4]) {
@@ -87,86 +88,94 @@ __device__ __forceinline__ bool cta_running(const int* status) {
     return s_st == kRun;
 }
 
-// (A) q = K p_new, p_new = z + beta p_old (fused), partial p_new . q
-// residency and column groups in flight per lane: FP32 rows are short in bytes and
-// favour 2 CTAs of 64 registers; FP64 rows favour 1 CTA with 2 groups in flight
+// (A) q = K p_new, p_new = z + beta p_old (fused), partial p_new . q.
+// Persistent CTAs walk the chunk list (chunk c, c + gridDim.x, ...); in a chunk,
+// 8 lanes share a block row (32 rows per pass) and each lane keeps two column
+// groups in flight; with FP32 values each 4-block group is summed in FP32 and
+// added to the FP64 row sums. 256-thread CTAs, two per SM (at most 128 registers).
 template <typename T>
-constexpr int pcg_min_blocks() {
-    return sizeof(T) == 8 ? 1 : 2;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kSpmvThreads, pcg_min_blocks<T>()) k_pcg_spmv(const ChunkDev* __restrict__ chunks,
-                                                           const InstDev<T>* __restrict__ insts, int parity) {
+__global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __restrict__ chunks, int nchunks,
+                                                             const InstDev<T>* __restrict__ insts, int parity) {
     __shared__ double sh[4 * 32];
-    const ChunkDev ck = chunks[blockIdx.x];
-    const InstDev<T> I = insts[ck.inst];
-    if (!cta_running(I.status)) return;
-    const T beta = (T)I.scal[kBeta];
-    const T* __restrict__ pold = parity ? I.p1 : I.p0;
-    T* __restrict__ pnew = parity ? I.p0 : I.p1;
-    const T* __restrict__ z = I.z;
     const int sub = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    double dot = 0.0;
-    const int nrows = ck.row1 - ck.row0;
-    // The trip count is uniform across the CTA so that every lane reaches the
-    // full-warp shuffles below; lanes past the chunk end carry zeros.
-    for (int base = 0; base < nrows; base += kSpmvThreads / 8) {
-        const bool valid = base + grp < nrows;
-        const int row = ck.row0 + (valid ? base + grp : 0);
-        const int g0 = valid ? I.goff[row] : 0;
-        const int ng = valid ? I.goff[row + 1] - g0 : 0;
-        T a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll(sizeof(T) == 8 ? 2 : 1)
-        for (int g = sub; g < ng; g += 8) {
-            int4 cc = __ldcs(reinterpret_cast<const int4*>(I.cols) + g0 + g);
-            T v[9][4];
+    for (int ci = blockIdx.x; ci < nchunks; ci += gridDim.x) {
+        const ChunkDev ck = chunks[ci];
+        const InstDev<T> I = insts[ck.inst];
+        if (!cta_running(I.status)) continue;  // CTA-uniform
+        const T beta = (T)I.scal[kBeta];
+        const T* __restrict__ pold = parity ? I.p1 : I.p0;
+        T* __restrict__ pnew = parity ? I.p0 : I.p1;
+        const T* __restrict__ z = I.z;
+        double dot = 0.0;
+        const int nrows = ck.row1 - ck.row0;
+        // The trip count is uniform across the CTA so that every lane reaches the
+        // full-warp shuffles below; lanes past the chunk end carry zeros.
+        for (int base = 0; base < nrows; base += kSpmvThreads / 8) {
+            const bool valid = base + grp < nrows;
+            const int row = ck.row0 + (valid ? base + grp : 0);
+            const int g0 = valid ? I.goff[row] : 0;
+            const int ng = valid ? I.goff[row + 1] - g0 : 0;
+            // the row's own direction, loaded ahead of the gathers (lanes 0..2: one component each)
+            const int c = sub < 3 ? sub : 0;
+            T zc = 0, pc = 0;
+            if (valid && sub < 3) {
+                zc = __ldg(z + 3 * (int64_t)row + c);
+                pc = __ldg(pold + 3 * (int64_t)row + c);
+            }
+            double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll 2
+            for (int g = sub; g < ng; g += 8) {
+                const int4 cc = __ldg(reinterpret_cast<const int4*>(I.cols) + g0 + g);
+                const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
+                T xv[4][3];
 #pragma unroll
-            for (int e = 0; e < 9; ++e) ld4(I.vals, (int64_t)g0 * 9 + (int64_t)e * ng + g, v[e]);
-            const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
+                for (int q = 0; q < 4; ++q)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int c3 = 3 * cj[j];
-                T q0 = z[c3] + beta * pold[c3];
-                T q1 = z[c3 + 1] + beta * pold[c3 + 1];
-                T q2 = z[c3 + 2] + beta * pold[c3 + 2];
-                a0 += v[0][j] * q0 + v[1][j] * q1 + v[2][j] * q2;
-                a1 += v[3][j] * q0 + v[4][j] * q1 + v[5][j] * q2;
-                a2 += v[6][j] * q0 + v[7][j] * q1 + v[8][j] * q2;
+                    for (int k = 0; k < 3; ++k) {
+                        const int64_t at = 3 * (int64_t)cj[q] + k;
+                        xv[q][k] = __ldg(z + at) + beta * __ldg(pold + at);
+                    }
+                const int64_t pl = (int64_t)ng;
+                const int64_t vb = (int64_t)g0 * 9 + g;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    T m0[4], m1[4], m2[4];
+                    ld4(I.vals, vb + (3 * r) * pl, m0);
+                    ld4(I.vals, vb + (3 * r + 1) * pl, m1);
+                    ld4(I.vals, vb + (3 * r + 2) * pl, m2);
+                    T t = 0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) t += m0[q] * xv[q][0] + m1[q] * xv[q][1] + m2[q] * xv[q][2];
+                    acc[r] += (double)t;
+                }
+            }
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+                for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+            if (valid && sub < 3) {
+                const int64_t at = 3 * (int64_t)row + c;
+                const T qc = (T)(c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]));
+                const T pn = zc + beta * pc;
+                I.q[at] = qc;
+                pnew[at] = pn;
+                dot += (double)pn * (double)qc;
             }
         }
-#pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
-            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        double v[1] = {dot}, tot[1];
+        block_sum<1>(v, sh);
+        __syncthreads();
+        if (last_cta_reduce<1>(v, I.part, ck.pad, I.chunk0, I.nchunks, I.counter, sh, tot) && threadIdx.x == 0) {
+            double pq = tot[0];
+            I.scal[kPq] = pq;
+            if (!(pq > 0.0) || !isfinite(pq)) {
+                *I.status = kBreak;
+                I.scal[kAlpha] = 0.0;
+            } else {
+                I.scal[kAlpha] = I.scal[kRz] / pq;
+            }
         }
-        if (valid && sub == 0) {
-            const int r3 = 3 * row;
-            T p0 = z[r3] + beta * pold[r3];
-            T p1 = z[r3 + 1] + beta * pold[r3 + 1];
-            T p2 = z[r3 + 2] + beta * pold[r3 + 2];
-            I.q[r3] = a0;
-            I.q[r3 + 1] = a1;
-            I.q[r3 + 2] = a2;
-            pnew[r3] = p0;
-            pnew[r3 + 1] = p1;
-            pnew[r3 + 2] = p2;
-            dot += (double)p0 * (double)a0 + (double)p1 * (double)a1 + (double)p2 * (double)a2;
-        }
-    }
-    double v[1] = {dot}, tot[1];
-    block_sum<1>(v, sh);
-    __syncthreads();
-    if (last_cta_reduce<1>(v, I.part, ck.pad, I.chunk0, I.nchunks, I.counter, sh, tot) && threadIdx.x == 0) {
-        double pq = tot[0];
-        I.scal[kPq] = pq;
-        if (!(pq > 0.0) || !isfinite(pq)) {
-            *I.status = kBreak;
-            I.scal[kAlpha] = 0.0;
-        } else {
-            I.scal[kAlpha] = I.scal[kRz] / pq;
-        }
+        __syncthreads();  // shared partials and s_last are reused by the next chunk
     }
 }
 
@@ -269,6 +278,22 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_replace(const ChunkDev* __r
 
 // ------------------------------------------------------------------ host loop
 
+// Resident CTAs of the SpMV kernel on the current device (its persistent grid).
+template <typename T>
+int64_t PcgBatch<T>::spmv_resident() {
+    if (resident_ > 0) return resident_;
+    int dev = 0, sms = 148, per_sm = 2;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_spmv<T>, kSpmvThreads, 0) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    resident_ = (int64_t)sms * per_sm;
+    return resident_;
+}
+
 template <typename T>
 void PcgBatch<T>::prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::vector<ChunkDev>& all_chunks,
                           std::vector<int>& chunk0, std::vector<int>& nch) {
@@ -284,11 +309,21 @@ void PcgBatch<T>::prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::
     d_counter_.zero(s);
     chunk0.assign(n, 0);
     nch.assign(n, 0);
+    // Chunks of at most kChunkRows rows, sized so that the SpMV's resident CTAs get
+    // equal shares: total rows over a whole number of chunks per resident CTA.
+    int64_t total = 0;
+    for (int i = 0; i < n; ++i) total += sys[i]->S->n_rows;
+    const int64_t res = spmv_resident();
+    const int64_t per_cta = std::max<int64_t>(1, (total + res * kChunkRows - 1) / (res * kChunkRows));
+    const int64_t target = std::max<int64_t>(1, (total + res * per_cta - 1) / (res * per_cta));
     for (int i = 0; i < n; ++i) {
         const int rows = sys[i]->S->n_rows;
         chunk0[i] = (int)all_chunks.size();
-        for (int r0 = 0; r0 < rows; r0 += kChunkRows)
-            all_chunks.push_back(ChunkDev{i, r0, std::min(rows, r0 + kChunkRows), (int)all_chunks.size()});
+        const int64_t k = std::max<int64_t>(1, (rows + target - 1) / target);
+        for (int64_t j = 0; j < k; ++j) {
+            const int r0 = (int)(rows * j / k), r1 = (int)(rows * (j + 1) / k);
+            all_chunks.push_back(ChunkDev{i, r0, r1, (int)all_chunks.size()});
+        }
         nch[i] = (int)all_chunks.size() - chunk0[i];
     }
     d_part_.alloc(all_chunks.size() * 4 + 4, s);
@@ -347,11 +382,13 @@ double PcgBatch<T>::profile_spmv(PcgSystem<T>& sys, int reps, cudaStream_t s) {
     prepare(v, s, chunks, c0, nc);
     FX_LAUNCH(k_pcg_replace<T>, (unsigned)chunks.size(), kUpdThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, 1, 0.0);
     for (int k = 0; k < 3; ++k)  // warm-up
-        FX_LAUNCH(k_pcg_spmv<T>, (unsigned)chunks.size(), kSpmvThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, k & 1);
+        FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(chunks.size()), kSpmvThreads, 0, s, d_chunks_.ptr, (int)chunks.size(),
+                  d_inst_.ptr, k & 1);
     EventTimer t;
     t.start(s);
     for (int k = 0; k < reps; ++k)
-        FX_LAUNCH(k_pcg_spmv<T>, (unsigned)chunks.size(), kSpmvThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, k & 1);
+        FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(chunks.size()), kSpmvThreads, 0, s, d_chunks_.ptr, (int)chunks.size(),
+                  d_inst_.ptr, k & 1);
     return t.stop_ms(s) / reps;
 }
 
@@ -417,7 +454,8 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
                 g_launch_counter = nullptr;
                 FX_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 for (int k = 0; k < poll; ++k) {
-                    FX_LAUNCH(k_pcg_spmv<T>, (unsigned)act.size(), kSpmvThreads, 0, s, d_act.ptr, d_inst_.ptr, k & 1);
+                    FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(act.size()), kSpmvThreads, 0, s, d_act.ptr, (int)act.size(),
+                              d_inst_.ptr, k & 1);
                     FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr,
                               k & 1);
                 }
@@ -434,7 +472,8 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
             int64_t* saved = g_launch_counter;
             g_launch_counter = nullptr;
             for (int k = 0; k < poll; ++k) {
-                FX_LAUNCH(k_pcg_spmv<T>, (unsigned)act.size(), kSpmvThreads, 0, s, d_act.ptr, d_inst_.ptr, k & 1);
+                FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(act.size()), kSpmvThreads, 0, s, d_act.ptr, (int)act.size(),
+                          d_inst_.ptr, k & 1);
                 FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr, k & 1);
             }
             g_launch_counter = saved;

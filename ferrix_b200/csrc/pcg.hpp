@@ -1,7 +1,7 @@
 // Batched preconditioned conjugate gradient over BSR(3x3) systems.
 //
 // Stands in for the reference's DirectSolver (src/solver/solvers/direct.rs:19-55,
-// an FP64 sparse Cholesky) and IterativeSolver (src/solver/solvers/iterative.rs:82-177,
+// an FP64 sparse Cholesky) and IterativeSolver (src/solver/solvers/iterative.rs:26-136,
 // a Jacobi-PCG): both solve K du = R; this solver returns du to a stated
 // tolerance on the FP64 true residual.
 //
@@ -23,6 +23,7 @@
 // replayed between host checks.
 #pragma once
 
+#include <algorithm>
 #include <functional>
 #include <vector>
 
@@ -85,6 +86,15 @@ struct PcgSystem {
 constexpr double kAmgOvercorrect = 1.7;
 constexpr double kAmgChebRatio = 12.0;
 
+// Mixed block-Jacobi PCG: FP64 true-residual target as a fraction of the
+// caller's rtol. Its FP32 Krylov recurrence leaves a residual whose smooth
+// (low-eigenvalue) components are larger than those FP64 CG leaves at the same
+// residual norm, so its displacement error at rtol = 1e-8 reached 2e-9 on the
+// 417k-DOF C3D20 box and exceeded 1e-8 on thin random boxes, where FP64 PCG
+// stays below; a residual 100x smaller keeps the mixed displacement error within
+// the rtol that the caller asked for.
+constexpr double kMixedBjResidualFactor = 1e-2;
+
 struct PcgOptions {
     double rtol = 1e-10;
     int max_iter = 20000;
@@ -101,6 +111,7 @@ struct PcgOptions {
     int amg_cheb_kind = 0;    // 0: Chebyshev of the first kind on [lmax/ratio, lmax], 1: fourth kind
     double amg_overcorrect = kAmgOvercorrect;  // scale of every coarse correction
     double amg_cheb_ratio = kAmgChebRatio;  // lmax / lmin of the first-kind Chebyshev interval
+    int64_t amg_persistent_max_dof = 0;     // systems up to this size: one persistent cluster launch (< 0: never)
 };
 
 template <typename T>
@@ -114,6 +125,9 @@ class PcgBatch {
    private:
     void prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::vector<ChunkDev>& chunks,
                  std::vector<int>& chunk0, std::vector<int>& nch);
+    int64_t spmv_resident();
+    unsigned spmv_grid(size_t nchunks) { return (unsigned)std::min<int64_t>((int64_t)nchunks, spmv_resident()); }
+    int64_t resident_ = 0;
     struct Work {
         DBuf<T> r, z, p0, p1, q;
         DBuf<double> r64;

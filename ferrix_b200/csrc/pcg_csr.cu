@@ -1,5 +1,5 @@
 // Scalar-CSR FP64 Jacobi PCG on the GPU: the algorithm of the reference's
-// IterativeSolver (src/solver/solvers/iterative.rs:82-177) with its
+// IterativeSolver (src/solver/solvers/iterative.rs:26-136) with its
 // DiagonalPreconditioner (src/solver/preconditioner.rs:36-58): x0 = 0,
 // z = D^-1 r (1/d when |d| > 1e-9, else 1), row-wise CSR SpMV.
 //
@@ -12,6 +12,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
+
+#include <vector>
 
 #include "pcg_csr.hpp"
 
@@ -206,6 +208,20 @@ void CsrSystem::from_bsr(const BsrStructure& S, const double* vals64, cudaStream
         FX_LAUNCH(k_bsr_to_csr32, (unsigned)((S.n_blocks + 255) / 256), 256, 0, s, S.n_blocks, S.blk_row.ptr,
                   S.row_ptr.ptr, S.goff.ptr, S.cols.ptr, vals64, ip.ptr, ind.ptr, val.ptr);
     FX_LAUNCH(k_csr_dinv, (unsigned)((n + 255) / 256), 256, 0, s, n, ip.ptr, ind.ptr, val.ptr, dinv.ptr);
+}
+
+void CsrSystem::from_host(int64_t rows, const int64_t* h_ip, const int64_t* h_ind, const double* h_val,
+                          cudaStream_t s) {
+    n = rows;
+    nnz = h_ip[rows];
+    std::vector<int32_t> ind32((size_t)nnz);
+    for (int64_t k = 0; k < nnz; ++k) ind32[(size_t)k] = (int32_t)h_ind[k];
+    ip.upload(h_ip, (size_t)n + 1, s);
+    ind.upload(ind32, s);
+    val.upload(h_val, (size_t)nnz, s);
+    dinv.alloc((size_t)n, s);
+    FX_LAUNCH(k_csr_dinv, (unsigned)((n + 255) / 256), 256, 0, s, n, ip.ptr, ind.ptr, val.ptr, dinv.ptr);
+    stream_wait(s, "csr upload");  // the host column copy must outlive the transfer
 }
 
 int CsrPcg::solve(CsrSystem& A, const double* b, double* x, const PcgOptions& opt, bool absolute, cudaStream_t s,

@@ -12,6 +12,8 @@ struct CsrSystem {
     DBuf<double> val, dinv;
     // scalar CSR of an FP64 BSR3 matrix (3 rows per block row) + Jacobi inverse diagonal
     void from_bsr(const BsrStructure& S, const double* vals64, cudaStream_t s);
+    // a caller's host CSR (int64 row offsets and columns, columns checked by the caller)
+    void from_host(int64_t rows, const int64_t* ip, const int64_t* ind, const double* val, cudaStream_t s);
 };
 
 class CsrPcg {

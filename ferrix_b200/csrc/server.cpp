@@ -40,6 +40,7 @@ struct Request {
     fx_model* model = nullptr;
     double bytes = 0.0;
     Clock::time_point t_submit, t_admit, t_done;
+    double setup_ms = 0.0, solve_ms = 0.0, finish_ms = 0.0;
     bool done = false;
     int slot = -1;
     int status = FX_OK;
@@ -62,6 +63,9 @@ struct fx_server {
     double in_use = 0.0;
     int running = 0;
     int started = 0;  // workers whose context creation has finished (or failed)
+    int preloaded = -2;  // kernels the slot contexts found loaded on the device (min over slots; -2: none yet)
+    int reservation = 0;  // reserve_pool result for the budget
+    double pool_bytes = 0.0;  // device pool reservation after the budget was reserved
     int64_t next_ticket = 1;
     bool stop = false;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -86,6 +90,10 @@ void worker(fx_server* srv, int slot) {
     {
         std::lock_guard<std::mutex> g(srv->mu);
         ++srv->started;
+        if (rc == FX_OK) {
+            const int pre = fx_ctx_preloaded_kernels(ctx);
+            srv->preloaded = srv->preloaded == -2 ? pre : std::min(srv->preloaded, pre);
+        }
         if (rc != FX_OK) {
             srv->last_error = "slot context creation failed";
             --srv->n_slots;
@@ -118,14 +126,20 @@ void worker(fx_server* srv, int slot) {
         int st = FX_OK;
         std::string err;
         m->ctx = ctx;
+        const Clock::time_point a = Clock::now();
         st = fx_state_initialize(m);
+        const Clock::time_point b = Clock::now();
         if (st == FX_OK) st = fx_step_solve(m, 0, &srv->opts, &r->stats);
+        const Clock::time_point c = Clock::now();
         if (st == FX_OK) {
             r->u.resize(3 * (size_t)m->dense.n_nodes);
             st = fx_state_get_displacements(m, r->u.data());
         }
         if (st != FX_OK) err = fx_ctx_last_error(ctx);
         release_device(m);
+        r->setup_ms = ms_since(a, b);
+        r->solve_ms = ms_since(b, c);
+        r->finish_ms = ms_since(c, Clock::now());
         {
             std::lock_guard<std::mutex> g(srv->mu);
             r->status = st;
@@ -174,18 +188,31 @@ int fx_server_create(const fx_server_opts* opts, fx_server** out) {
     // never grow the pool while other requests' kernels run
     cudaStream_t rs = nullptr;
     if (cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking) == cudaSuccess) {
-        reserve_pool(o.device, rs, std::min(s->budget, 0.9 * (double)free_b));
+        s->reservation = reserve_pool(o.device, rs, std::min(s->budget, 0.9 * (double)free_b));
         cudaStreamSynchronize(rs);
         cudaStreamDestroy(rs);
     } else {
         cudaGetLastError();
+        s->reservation = -1;
     }
+    s->pool_bytes = pool_reserved_bytes(o.device);
     for (int i = 0; i < o.slots; ++i) s->workers.emplace_back(worker, s, i);
     {  // every slot has its context (stream, workspaces) before the first request
         std::unique_lock<std::mutex> lk(s->mu);
         s->cv_done.wait_for(lk, std::chrono::seconds(60), [&] { return s->started == o.slots; });
     }
     *out = s;
+    return FX_OK;
+}
+
+int fx_server_get_info(fx_server* s, fx_server_info* out) {
+    if (!s || !out) return FX_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(s->mu);
+    out->slots = s->n_slots;
+    out->preloaded_kernels = s->preloaded == -2 ? -1 : s->preloaded;
+    out->budget_bytes = s->budget;
+    out->pool_reserved_bytes = s->pool_bytes;
+    out->reservation = s->reservation;
     return FX_OK;
 }
 
@@ -242,6 +269,9 @@ int fx_server_wait(fx_server* s, int64_t ticket, double timeout_s, double* u, fx
         res->done_at_ms = ms_since(s->t0, r->t_done);
         res->slot = r->slot;
         res->stats = r->stats;
+        res->setup_ms = r->setup_ms;
+        res->solve_ms = r->solve_ms;
+        res->finish_ms = r->finish_ms;
         std::strncpy(res->error, r->error.c_str(), sizeof(res->error) - 1);
         res->error[sizeof(res->error) - 1] = 0;
     }

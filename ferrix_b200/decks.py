@@ -189,29 +189,84 @@ def write_deck(spec: DeckSpec) -> str:
     return s.getvalue()
 
 
-def c3d4_cantilever(nx: int = 10, ny: int = 10, nz: int = 40) -> str:
+def deck_arrays(spec: DeckSpec) -> dict:
+    """The model write_deck(spec) describes, as Project.from_arrays arguments (the
+    binary mesh path, fx_model_from_arrays): what the reference parser makes of that
+    text, without the text. Node and element ids are 1-based positions; the single
+    material is *Elastic rows (E, nu, T; T = 0 when absent) and the optional
+    *Expansion (alpha at T = 0, ZERO = reference temperature); the step's solver
+    is DIRECT (Spooles); its BCs are the clamped face's nodes x DOFs 1-3 in node
+    order, its loads the loaded face's nodes per force component."""
+    m = spec.mesh
+    n = m.xyz.shape[0]
+    ids = np.arange(1, n + 1, dtype=np.int64)
+    eids = np.arange(1, m.conn.shape[0] + 1, dtype=np.int64)
+    group = (eids, m.conn.astype(np.int64) + 1, np.zeros(len(eids), dtype=np.int32))
+    mat = {"name": "MAT", "E": [(0.0 if t is None else t, e) for e, _, t in spec.materials],
+           "nu": [(0.0 if t is None else t, nu) for _, nu, t in spec.materials], "alpha": [], "tref": 0.0}
+    if spec.expansion is not None:
+        mat["alpha"] = [(0.0, spec.expansion[0])]
+        mat["tref"] = spec.expansion[1]
+    amps = []
+    if spec.amplitude is not None:
+        amps.append({"time": [t for t, _ in spec.amplitude], "value": [v for _, v in spec.amplitude]})
+    clamp = face_nodes(m, spec.clamp_axis, spec.clamp_side)
+    loaded = face_nodes(m, spec.clamp_axis, 1 - spec.clamp_side)
+    bcs = [(int(i) + 1, d, 0.0, -1, 1) for i in clamp for d in range(3)]
+    amp = 0 if spec.amplitude is not None else -1
+    loads = [(int(i) + 1, d, float(spec.load_total[d]) / len(loaded), amp, 1)
+             for d in range(3) if spec.load_total[d] != 0.0 for i in loaded]
+    inc = (1.0, 1.0, 1e-5, 1.0)
+    if spec.static_line:
+        inc = tuple(float(v) for v in spec.static_line.split(","))
+    step = {"nlgeom": spec.nlgeom, "solver": 1 if spec.solver.upper() in ("SPOOLES", "PARDISO", "PASTIX") else 0,
+            "increment": inc, "max_increments": 10000, "loads": loads, "bcs": bcs}
+    temps = None
+    if spec.init_temp is not None:
+        temps = {int(i) + 1: float(t) for i, t in enumerate(spec.init_temp)}
+    return {"node_ids": ids, "xyz": m.xyz, "c3d4": group if m.npe == 4 else None,
+            "c3d20": group if m.npe == 20 else None, "materials": [mat], "amplitudes": amps, "steps": [step],
+            "initial_temperatures": temps}
+
+
+def c3d4_cantilever_spec(nx: int = 10, ny: int = 10, nz: int = 40) -> DeckSpec:
     m = tet_box(nx, ny, nz, 10.0, 10.0, 40.0)
-    return write_deck(DeckSpec(m, [(210000.0, 0.3, None)], clamp_axis=2, load_total=(0.0, -1000.0, 0.0)))
+    return DeckSpec(m, [(210000.0, 0.3, None)], clamp_axis=2, load_total=(0.0, -1000.0, 0.0))
+
+
+def c3d4_cantilever(nx: int = 10, ny: int = 10, nz: int = 40) -> str:
+    return write_deck(c3d4_cantilever_spec(nx, ny, nz))
+
+
+def c3d20_box_spec(nx: int = 20, ny: int = 20, nz: int = 80, seed: int = 2024,
+                   lengths=(20.0, 20.0, 80.0)) -> DeckSpec:
+    m = hex20_box(nx, ny, nz, *lengths, jitter=0.10, seed=seed)
+    return DeckSpec(m, [(70000.0, 0.33, None)], clamp_axis=2, load_total=(-5000.0, 0.0, 0.0))
 
 
 def c3d20_box(nx: int = 20, ny: int = 20, nz: int = 80, seed: int = 2024, lengths=(20.0, 20.0, 80.0)) -> str:
-    m = hex20_box(nx, ny, nz, *lengths, jitter=0.10, seed=seed)
-    return write_deck(DeckSpec(m, [(70000.0, 0.33, None)], clamp_axis=2, load_total=(-5000.0, 0.0, 0.0)))
+    return write_deck(c3d20_box_spec(nx, ny, nz, seed, lengths))
+
+
+def c3d4_nlgeom_beam_spec(nx: int = 100, ny: int = 20, nz: int = 20, tip_load: float = 6.0e4,
+                          increments: int = 10) -> DeckSpec:
+    m = tet_box(nx, ny, nz, 50.0, 10.0, 10.0)
+    temp = 20.0 + 200.0 * m.xyz[:, 0] / 50.0
+    dt = 1.0 / increments
+    return DeckSpec(m, [(210000.0, 0.3, 20.0), (198000.0, 0.3, 220.0)], expansion=(1.2e-5, 20.0),
+                    clamp_axis=0, load_total=(0.0, 0.0, -tip_load), nlgeom=True,
+                    static_line=f"{dt!r}, 1.0, 1e-05, {dt!r}", amplitude=[(0.0, 0.0), (1.0, 1.0)],
+                    init_temp=temp)
 
 
 def c3d4_nlgeom_beam(nx: int = 100, ny: int = 20, nz: int = 20, tip_load: float = 6.0e4,
                      increments: int = 10) -> str:
-    m = tet_box(nx, ny, nz, 50.0, 10.0, 10.0)
-    temp = 20.0 + 200.0 * m.xyz[:, 0] / 50.0
-    dt = 1.0 / increments
-    return write_deck(DeckSpec(m, [(210000.0, 0.3, 20.0), (198000.0, 0.3, 220.0)], expansion=(1.2e-5, 20.0),
-                               clamp_axis=0, load_total=(0.0, 0.0, -tip_load), nlgeom=True,
-                               static_line=f"{dt!r}, 1.0, 1e-05, {dt!r}", amplitude=[(0.0, 0.0), (1.0, 1.0)],
-                               init_temp=temp))
+    return write_deck(c3d4_nlgeom_beam_spec(nx, ny, nz, tip_load, increments))
 
 
-def random_box(rng: np.random.Generator, dof_target: float, npe: int = 4) -> Tuple[str, int]:
-    """One member of the batched / serving population; returns (deck, dof)."""
+def random_box(rng: np.random.Generator, dof_target: float, npe: int = 4, arrays: bool = False):
+    """One member of the batched / serving population; returns (deck, dof), with
+    arrays=True (Project.from_arrays arguments of the same model, dof) instead."""
     L = rng.uniform(5.0, 50.0, size=3)
     nodes_target = dof_target / 3.0
     # cells c_i ~ L_i * s with node count ~ prod(c_i + 1) (C3D4) or ~4 prod(c_i) (C3D20)
@@ -229,17 +284,18 @@ def random_box(rng: np.random.Generator, dof_target: float, npe: int = 4) -> Tup
         m = tet_box(int(cells[0]), int(cells[1]), int(cells[2]), *L)
     else:
         m = hex20_box(int(cells[0]), int(cells[1]), int(cells[2]), *L, jitter=0.1, seed=int(rng.integers(1 << 30)))
-    deck = write_deck(DeckSpec(m, [(e_mod, nu, None)], clamp_axis=axis,
-                               load_total=tuple(float(v) for v in direction * mag)))
-    return deck, 3 * m.xyz.shape[0]
+    spec = DeckSpec(m, [(e_mod, nu, None)], clamp_axis=axis, load_total=tuple(float(v) for v in direction * mag))
+    return (deck_arrays(spec) if arrays else write_deck(spec)), 3 * m.xyz.shape[0]
 
 
 def batch_population(n: int = 256, seed: int = 7, dof_lo: float = 2e3, dof_hi: float = 6e4,
-                     c3d20_fraction: float = 0.0) -> List[Tuple[str, int]]:
+                     c3d20_fraction: float = 0.0, arrays: bool = False) -> List[Tuple[object, int]]:
+    """n seeded population members (deck text, or from_arrays arguments with arrays=True:
+    the same models, draw for draw)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
         target = float(np.exp(rng.uniform(math.log(dof_lo), math.log(dof_hi))))
         npe = 20 if rng.uniform() < c3d20_fraction else 4
-        out.append(random_box(rng, target, npe))
+        out.append(random_box(rng, target, npe, arrays))
     return out

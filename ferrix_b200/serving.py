@@ -7,7 +7,9 @@ clamped, a random-direction load of 100-5000 N on the opposite face. Each
 request draws a pool deck; its model is parsed on the host before the timed
 stream starts (a request carries an already parsed deck), so latency counts
 from submission: queueing for a slot and HBM budget, upload, symbolic pattern,
-assembly, solve to 1e-8 and the download of the displacements.
+assembly, solve to 1e-8 and the download of the displacements. The result
+splits each request's latency into queueing, set-up / upload, the solve (host
+wall time and device time) and download / release, as p50 / p99.
 """
 from __future__ import annotations
 
@@ -68,14 +70,17 @@ def run_stream(pool: List[str], rate: float, n_requests: int, opts, device: int 
             tickets.append(srv.submit(models[k]))
         outs = [srv.wait(t, timeout=3600.0) for t in tickets]
         t_end = time.perf_counter()
+        info = srv.info()
     finally:
         srv.close()
     kept = {}
     recs = []
     for k, (u, r) in enumerate(outs):
         recs.append({"pool": int(order[k]), "status": r["status"], "latency_ms": r["latency_ms"],
-                     "queue_ms": r["queue_ms"], "service_ms": r["service_ms"], "dofs": models[k].num_dofs,
-                     "pcg_iterations": r["stats"]["pcg_iterations"], "error": r["error"]})
+                     "queue_ms": r["queue_ms"], "service_ms": r["service_ms"], "device_ms": r["stats"]["t_total_ms"],
+                     "setup_ms": r["setup_ms"], "solve_ms": r["solve_ms"], "finish_ms": r["finish_ms"],
+                     "dofs": models[k].num_dofs, "pcg_iterations": r["stats"]["pcg_iterations"],
+                     "error": r["error"]})
         if keep is not None and int(order[k]) in keep and int(order[k]) not in kept and u is not None:
             kept[int(order[k])] = u
     for m in models:
@@ -83,7 +88,14 @@ def run_stream(pool: List[str], rate: float, n_requests: int, opts, device: int 
     lat = np.array([r["latency_ms"] for r in recs if r["status"] == 0])
     ok = int(sum(1 for r in recs if r["status"] == 0))
     span = max(t_end - t0, 1e-9)
+    # where the latency goes: p50 / p99 of each part over the completed requests
+    parts = {}
+    for key in ("queue_ms", "service_ms", "setup_ms", "solve_ms", "device_ms", "finish_ms"):
+        v = np.array([r[key] for r in recs if r["status"] == 0])
+        if len(v):
+            parts[key] = [round(float(np.percentile(v, 50)), 2), round(float(np.percentile(v, 99)), 2)]
     return {"rate_per_s": rate, "requests": n_requests, "completed": ok, "slots": slots,
+            "p50_p99_parts_ms": parts, "server": info,
             "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "mean_ms": float(lat.mean()) if len(lat) else None,

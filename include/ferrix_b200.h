@@ -11,6 +11,8 @@
  * crate root):
  *   fx_model_from_inp            Project::from_jobname / Parser::parse
  *                                (src/solver/project.rs:93-127, src/solver/parser.rs:111-147)
+ *   fx_model_from_arrays         the Project that Parser::parse builds, from arrays
+ *                                (src/solver/parser.rs:111-482, src/solver/mesh_lib/mesh.rs:35-50)
  *   fx_state_initialize          SolutionState::new + initialize (src/solver/state.rs:32-79)
  *                                and SolverTime::new (src/solver/time.rs:27-33)
  *   fx_step_solve                Step::solve -> StaticStep::solve
@@ -20,7 +22,8 @@
  *   fx_internal_force            Assembler::assemble_internal_force (src/solver/assembler.rs:157-241)
  *   fx_thermal_force             Assembler::assemble_thermal_force (src/solver/assembler.rs:247-299)
  *   fx_solve_csr                 Solver::solve (src/solver/solvers/mod.rs:18-43), the seam behind
- *                                DirectSolver (direct.rs:19-55) and IterativeSolver (iterative.rs:82-177)
+ *                                DirectSolver (direct.rs:19-55) and IterativeSolver (iterative.rs:26-136)
+ *   fx_last_error_detail         the payload of the FerrixError variant (src/solver/error.rs:12-72)
  *   fx_batch_solve               no reference counterpart (one deck per process there): many
  *                                independent decks' first *STATIC step in one batched launch sequence
  *   fx_server_*                  no reference counterpart: continuous-batching request loop
@@ -80,7 +83,7 @@ typedef struct {
     int use_graphs;         /* capture the PCG iteration block in a CUDA graph */
     int verbose;            /* print the reference's per-iteration |R| lines to stdout */
     int reference_iterative; /* SOLVER=ITERATIVE steps: reference semantics (Jacobi PCG, absolute
-                                sqrt(r.z) < 1e-8, at most 1000 iterations; iterative.rs:82-177) */
+                                sqrt(r.z) < 1e-8, at most 1000 iterations; iterative.rs:26-136) */
     int preconditioner;     /* fx_preconditioner */
     int amg_aggregate_nodes; /* FX_PRECOND_AMG: mean nodes per fine aggregate (cell size); 0 = 40 */
     int amg_smoother_degree; /* FX_PRECOND_AMG: Chebyshev steps per pre/post smoothing, 1..8; 0 = 2 */
@@ -91,6 +94,10 @@ typedef struct {
     double amg_overcorrect;  /* FX_PRECOND_AMG: coarse corrections are scaled by this factor, in (0, 2);
                                 0 = 1.7 */
     double amg_cheb_ratio;   /* FX_PRECOND_AMG: lmax / lmin of the first-kind Chebyshev interval; 0 = 12 */
+    int amg_persistent_max_dof; /* FX_PRECOND_AMG, V-cycle: systems of at most this many DOF run their
+                                   whole CG in one persistent launch, one thread-block cluster per system
+                                   (all such systems of a batch in the same launch); 0 = 100,000,
+                                   < 0 = never (one launch per CG step and V-cycle phase) */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */
@@ -125,16 +132,127 @@ void fx_default_solve_opts(fx_solve_opts* opts);
 int fx_ctx_create(int device, fx_ctx** out);
 void fx_ctx_destroy(fx_ctx* ctx);
 const char* fx_ctx_last_error(const fx_ctx* ctx);
+
+/* The last failure with the payload of its FerrixError variant (src/solver/error.rs:12-72):
+ *   FX_PARSE                line = deck line (0 for element-line errors, as the reference
+ *                           reports them), text = the message
+ *   FX_UNSUPPORTED_KEYWORD  line = deck line, text = the keyword
+ *   FX_NODE_NOT_FOUND       id = the node id;   FX_ELEMENT_NOT_FOUND: id = the element id
+ *   FX_UNKNOWN_SOLVER, FX_MATERIAL_NOT_FOUND, FX_ELSET_NOT_FOUND, FX_NSET_NOT_FOUND
+ *                           text = the name
+ *   FX_NUMERICAL, FX_CONVERGENCE, FX_INVALID_MODEL, FX_GENERIC, FX_GENERIC_IO, FX_IO
+ *                           text = the variant's message (the path for FX_IO)
+ * line / id are -1 where the variant has none; message = the full display text
+ * (as fx_ctx_last_error). With ctx NULL: the calling thread's last failure, which
+ * also covers calls made without a context (fx_model_from_inp with ctx NULL).
+ * status is FX_OK when nothing has failed yet. Texts are truncated to fit. */
+typedef struct {
+    int status;
+    int64_t line;
+    int64_t id;
+    char text[512];
+    char message[768];
+} fx_error_detail;
+int fx_last_error_detail(const fx_ctx* ctx, fx_error_detail* out);
 /* Number of kernel launches issued by this context so far (all entry points). */
 int64_t fx_ctx_kernel_launches(const fx_ctx* ctx);
 /* The context's cudaStream_t (as void*), for callers that time or order work on it. */
 void* fx_ctx_stream(const fx_ctx* ctx);
+/* Kernels of the library that fx_ctx_create found loaded on the context's device
+ * (all of them are loaded once per device and process, so that no kernel's first
+ * launch waits for other streams' work); -1 when the driver offers no way to
+ * load them ahead (they then load at first launch). */
+int fx_ctx_preloaded_kernels(const fx_ctx* ctx);
 
 /* ---- model (Project) -------------------------------------------------- */
 /* Preprocess + parse `.inp` text with the reference parser's semantics.
  * ctx may be NULL: the model can then be inspected but not solved. */
 int fx_model_from_inp(fx_ctx* ctx, const char* text, size_t len, fx_model** out);
 void fx_model_destroy(fx_model* model);
+
+/* ---- model from arrays (binary mesh path) ---------------------------------
+ * The model that Project::from_jobname / Parser::parse builds
+ * (src/solver/parser.rs:111-482, src/solver/mesh_lib/mesh.rs:35-50,
+ * src/solver/material.rs:14-69, src/solver/step/boundary_conds.rs:9-102,
+ * src/solver/step/amplitude.rs:9-57), handed over as arrays instead of .inp
+ * text, for callers that already hold the mesh in memory (a service receiving
+ * binary meshes, a mesh generator): no text is formatted or parsed. Every field
+ * means what it means after a deck is parsed, so the model equals the one
+ * fx_model_from_inp builds from a deck that defines the same data (same node
+ * index order, element groups, material tables and step records; the same
+ * displacements, bit for bit). All arrays are the caller's and are copied. */
+typedef struct {
+    int64_t n;                  /* (temperature, value) pairs, 0 = property not defined */
+    const double* temperature;  /* n; pairs are inserted in this order and kept sorted by temperature
+                                   (stable), as the reference's TemperatureDependentLUT::push */
+    const double* value;        /* n */
+} fx_lut_desc;
+
+typedef struct {
+    const char* name;                 /* NUL-terminated; may be NULL */
+    fx_lut_desc youngs_modulus;       /* *ELASTIC column 1 over column 3 */
+    fx_lut_desc poisson_ratio;        /* *ELASTIC column 2 over column 3 */
+    fx_lut_desc thermal_expansion;    /* *EXPANSION; n = 0 when the material has none */
+    double reference_temperature;     /* *EXPANSION, ZERO= */
+} fx_material_desc;
+
+typedef struct {
+    int64_t n;             /* (time, value) pairs of a tabular *AMPLITUDE, >= 1 */
+    const double* time;    /* n, ascending */
+    const double* value;   /* n */
+    int total_time;        /* TIME=TOTAL TIME: evaluated at the total time, else at the step time */
+    double shift_x, shift_y;
+} fx_amplitude_desc;
+
+typedef struct {
+    int64_t node_id;
+    int32_t dof;          /* 0..2 (DOFs 4-6 of a deck are dropped by the parser) */
+    int32_t amplitude;    /* index into fx_mesh_desc.amplitudes; -1 = the step ramp */
+    double value;
+    int64_t origin_step;  /* the step the record was defined in (1-based); 0 = before the first *STEP */
+} fx_record_desc;
+
+typedef struct {
+    int nlgeom;
+    int solver;              /* 0 default, 1 direct, 2 iterative (*STATIC, SOLVER=) */
+    double increment[4];     /* initial, period, min, max increment (the *STATIC data line) */
+    int64_t max_increments;  /* *STEP, INC= (10000 when absent) */
+    int64_t n_loads;         /* the step's *CLOAD records in effect (carried over ones first), in order */
+    const fx_record_desc* loads;
+    int64_t n_bcs;           /* the step's *BOUNDARY records in effect, in order */
+    const fx_record_desc* bcs;
+} fx_step_desc;
+
+typedef struct {
+    int64_t n_nodes;
+    const int64_t* node_ids;      /* n_nodes ids, any order; a repeated id: the later entry wins */
+    const double* xyz;            /* 3 * n_nodes */
+    int64_t n_c3d4;
+    const int64_t* c3d4_ids;      /* element ids, unique over both types */
+    const int64_t* c3d4_nodes;    /* 4 node ids per element */
+    const int32_t* c3d4_material; /* material index per element, -1 = no *SOLID SECTION (NULL: all -1) */
+    int64_t n_c3d20;
+    const int64_t* c3d20_ids;
+    const int64_t* c3d20_nodes;   /* 20 node ids per element, Abaqus order */
+    const int32_t* c3d20_material;
+    int n_materials;
+    const fx_material_desc* materials;
+    int n_amplitudes;
+    const fx_amplitude_desc* amplitudes;
+    int n_steps;
+    const fx_step_desc* steps;
+    double default_temperature;   /* Project.default_initial_temperature */
+    int64_t n_initial_temperatures; /* *INITIAL CONDITIONS, TYPE=TEMPERATURE */
+    const int64_t* initial_temperature_ids;
+    const double* initial_temperatures;
+} fx_mesh_desc;
+
+/* Builds a model from `desc` (ctx as in fx_model_from_inp; NULL = host only, for
+ * fx_server_submit). Element nodes that are not in the mesh are reported as
+ * FX_NODE_NOT_FOUND by the first solve, as for a deck. FX_INVALID_ARGUMENT for
+ * inconsistent descriptions (missing arrays, dof outside 0..2, an index outside
+ * its table, a table without pairs where one is required). */
+int fx_model_from_arrays(fx_ctx* ctx, const fx_mesh_desc* desc, fx_model** out);
 /* Counts: nodes, elements (all types), steps, materials. */
 int fx_model_sizes(const fx_model* model, int64_t* n_nodes, int64_t* n_elements, int* n_steps, int* n_materials);
 /* Mesh::index_to_node_id: ids[i] = node id of matrix index i (ascending ids). */
@@ -182,8 +300,21 @@ int fx_assemble_csr(fx_model* model, const double* u_or_null, int precision, int
 int fx_internal_force(fx_model* model, const double* u, const double* uconf_or_null, double* f);
 int fx_thermal_force(fx_model* model, double* f);
 /* Solver::solve seam: solve K x = b for a host CSR matrix (square, symmetric
- * positive definite, n rows) with the GPU PCG; tol / max_iter as the caller's
- * Solver::solve arguments are mapped by `opts`. */
+ * positive definite, n rows, int64 row offsets and columns) on the GPU.
+ * Solver::solve(k, f, precond, tol, max_iter) maps onto `opts`:
+ *   IterativeSolver (iterative.rs:26-136): reference_iterative = 1, rtol = tol,
+ *     max_iter = max_iter -> Jacobi PCG on the matrix as given, stopping when the
+ *     ABSOLUTE sqrt(r.z) < tol (z = D^-1 r), FX_CONVERGENCE after max_iter
+ *     iterations, as the reference (the static step passes tol 1e-8, 1000);
+ *   DirectSolver (direct.rs:19-55, which ignores tol and max_iter): leave
+ *     reference_iterative 0 and keep the library's rtol (1e-8) and max_iter;
+ *     the matrix is regrouped into 3x3 blocks and solved by block-Jacobi PCG
+ *     (FX_PREC_MIXED: FP32 with FP64 residual replacement and a 100x tighter
+ *     FP64 target, finished in FP64 if FP32 stalls; FX_PREC_FP64), stopping on
+ *     the RELATIVE ||b - K x||_M / ||b||_M <= rtol, M = 3x3 block-Jacobi;
+ *     FX_PREC_FP64_CSR: scalar-CSR Jacobi PCG with the relative test.
+ * The matrix carries no node coordinates, so the multigrid preconditioner of
+ * fx_step_solve is not available here. */
 int fx_solve_csr(fx_ctx* ctx, int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
                  const double* b, double* x, const fx_solve_opts* opts, fx_step_stats* stats);
 
@@ -259,6 +390,9 @@ typedef struct {
     double done_at_ms;      /* completion time, ms since fx_server_create */
     fx_step_stats stats;    /* of the solved step */
     char error[256];        /* message when status != FX_OK */
+    double setup_ms;        /* service_ms split: state initialisation and model upload, */
+    double solve_ms;        /* the step solve (host wall time; stats.t_total_ms is its device time), */
+    double finish_ms;       /* displacement download and release of the model's device memory */
 } fx_request_result;
 
 void fx_default_server_opts(fx_server_opts* opts);
@@ -272,6 +406,20 @@ int fx_server_submit(fx_server* server, fx_model* model, int64_t* ticket);
  * the ticket and returns the request's status. */
 int fx_server_wait(fx_server* server, int64_t ticket, double timeout_s, double* u, fx_request_result* result);
 /* Finishes the running requests, cancels the queued ones, joins the workers. */
+/* What the server set up: slots with a context, kernels found loaded on the device
+ * by the slot contexts (fx_ctx_preloaded_kernels, least over slots), the admission
+ * budget, the bytes the device's memory pool held after the budget was reserved,
+ * and the reservation's outcome (1 the pool grew, 0 it held enough already, -1
+ * it could not grow in one piece and grows on demand, which stalls the streams
+ * running at that moment). */
+typedef struct {
+    int slots;
+    int preloaded_kernels;
+    double budget_bytes;
+    double pool_reserved_bytes;
+    int reservation;
+} fx_server_info;
+int fx_server_get_info(fx_server* server, fx_server_info* out);
 void fx_server_destroy(fx_server* server);
 
 /* ---- allocation-free SpMV with fused dot -------------------------------
@@ -285,7 +433,9 @@ void fx_server_destroy(fx_server* server);
  * into the library, held by every GPU that loads it until exit. Limit: at most
  * 524,288 rows (FX_INVALID_ARGUMENT beyond). The first call on a device looks
  * up the scratch address — make it before any stream capture. Calls share the
- * scratch: calls that overlap on the GPU race and must be ordered. */
+ * scratch: calls that overlap on the GPU race and must be ordered. y must not
+ * overlap x (FX_INVALID_ARGUMENT). A CUDA error already pending in the calling
+ * thread when the call starts is returned as FX_CUDA and left pending. */
 int fx_spmv_dot_noalloc(int device, int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
                         const double* x, double* y, double* dot, void* stream);
 

@@ -60,7 +60,7 @@ class Timings:
 
 
 def jacobi_pcg(K: sp.csr_matrix, b: np.ndarray, tol: float = 1e-8, max_iter: int = 1000) -> np.ndarray:
-    """IterativeSolver::solve (iterative.rs:82-177) with DiagonalPreconditioner."""
+    """IterativeSolver::solve (iterative.rs:26-136) with DiagonalPreconditioner."""
     d = K.diagonal()
     inv = np.ones_like(d)
     big = np.abs(d) > 1e-9

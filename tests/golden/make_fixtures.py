@@ -1,8 +1,9 @@
-"""Regenerate the golden fixtures under tests/golden/ from the FerriX checkout.
+"""Regenerate the golden fixtures under tests/golden/.
 
-    python tests/golden/make_fixtures.py [path-to-ferrix-checkout]
+    python tests/golden/make_fixtures.py decks <path-to-ferrix-checkout>
+    python tests/golden/make_fixtures.py box
 
-Writes
+`decks` (needs a FerriX checkout, passed explicitly) writes
   decks/<name>.inp.gz   gzip copies of the reference's four test decks
                         (tests/data/*.inp of the FerriX repository), so the
                         GPU parity tests can run where the checkout is absent;
@@ -11,13 +12,22 @@ Writes
                         tests/calculix_parity.rs:29,91,187,279);
   calculix.json         the CalculiX displacement goldens and tolerances that
                         the reference's tests/calculix_parity.rs asserts.
+
+`box` (no checkout needed) writes
+  oracle_c3d20_box.npz  the oracle's FP64 direct solution of the 417,123-DOF
+                        C3D20 box that the benchmark solves (ferrix_b200.decks
+                        .c3d20_box() with its default seed), plus the deck's
+                        SHA-256 so a test can tell when the generator changed.
+                        One oracle run: about 70 s on 16 cores, ~10 GB of RAM.
 """
 from __future__ import annotations
 
 import gzip
+import hashlib
 import json
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -38,8 +48,10 @@ CALCULIX = {
     "C3D20": {"node": 17, "tol": 1e-6, "steps": [[5.752112e-02, -2.497816e-04, -8.074951e-03]]},
 }
 
+BOX_FIXTURE = "oracle_c3d20_box.npz"
 
-def main(ref: str) -> None:
+
+def make_decks(ref: str) -> None:
     os.makedirs(os.path.join(HERE, "decks"), exist_ok=True)
     for name in DECKS:
         src = os.path.join(ref, "tests", "data", name + ".inp")
@@ -62,5 +74,28 @@ def main(ref: str) -> None:
         json.dump(CALCULIX, fh, indent=1)
 
 
+def box_deck() -> str:
+    from ferrix_b200 import decks
+    return decks.c3d20_box()
+
+
+def deck_digest(text: str) -> str:
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+def make_box() -> None:
+    text = box_deck()
+    t0 = time.perf_counter()
+    p = inp.parse_inp_text(text)
+    u = static_step.Runner(p).run().displacements
+    np.savez_compressed(os.path.join(HERE, BOX_FIXTURE), u=u, deck_sha256=np.array(deck_digest(text)))
+    print(BOX_FIXTURE, "dof", len(u), f"{time.perf_counter() - t0:.1f} s")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) == 3 and sys.argv[1] == "decks":
+        make_decks(sys.argv[2])
+    elif len(sys.argv) == 2 and sys.argv[1] == "box":
+        make_box()
+    else:
+        sys.exit(__doc__)

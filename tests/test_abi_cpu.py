@@ -1,6 +1,7 @@
 """C-ABI checks that need no GPU: the library loads, exports every symbol the
 header declares, and its `.inp` parser builds the same model as the oracle's
 restatement of src/solver/parser.rs (no compute call is made)."""
+import ctypes as C
 import gzip
 import os
 
@@ -301,3 +302,33 @@ def test_parser_errors(text, kind):
     with pytest.raises(fx.FerrixError) as eg:
         fx.Project.from_inp_text(text)
     assert eg.value.kind == kind
+    # the variant's payload crosses the C ABI (fx_last_error_detail): the deck line of
+    # ParseError / UnsupportedKeyword, the keyword, material / set / solver name or message
+    e, o = eg.value, eo.value
+    assert e.text == o.message, (e.text, o.message)
+    if kind in ("ParseError", "UnsupportedKeyword"):
+        assert e.line == o.line, (e.line, o.line)
+    else:
+        assert e.line is None
+    assert e.id is None
+
+
+def test_error_detail_without_context_is_per_thread():
+    """fx_last_error_detail(NULL) reports the calling thread's last failure."""
+    import threading
+    lib = _lib.load()
+    seen = {}
+
+    def parse(tag, text):
+        with pytest.raises(fx.FerrixError):
+            fx.Project.from_inp_text(text)
+        d = _lib.ErrorDetail()
+        assert lib.fx_last_error_detail(None, C.byref(d)) == 0
+        seen[tag] = (d.status, d.line, d.text.decode())
+
+    t = threading.Thread(target=parse, args=("other", "*NODE\n1, 0, 0, 0\n*FOO\n"))
+    t.start()
+    t.join()
+    parse("main", "*STEP\n*STATIC, SOLVER=MAGIC\n")
+    assert seen["other"] == (4, 3, "FOO")
+    assert seen["main"] == (5, -1, "MAGIC")

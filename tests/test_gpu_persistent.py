@@ -1,0 +1,87 @@
+"""The persistent multigrid-CG launch (one thread-block cluster per system) against
+the multi-launch path and the oracle's FP64 direct solution.
+
+Small systems (up to amg_persistent_max_dof DOF, 100,000 by default) run their
+whole CG in one launch; amg_persistent_max_dof = -1 forces one launch per step.
+Both paths implement the same algorithm, so their iteration counts agree to a
+few iterations and both meet the accuracy bounds of the other parity tests
+(1e-8 relative displacement error for the mixed solver, 1e-10 for FP64)."""
+import numpy as np
+import pytest
+
+import ferrix_b200 as fx
+from ferrix_b200 import decks
+from oracle import inp, static_step
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = fx.Context(0)
+    yield c
+    c.close()
+
+
+def _oracle_run(text):
+    o = inp.parse_inp_text(text)
+    o.default_initial_temperature = 20.0
+    return static_step.Runner(o).run().displacements
+
+
+def _solve(ctx, text, **kw):
+    p = fx.Project.from_inp_text(text, ctx)
+    p.default_initial_temperature = 20.0
+    st = fx.SolutionState(p.num_dofs, p.num_nodes)
+    st.initialize(p)
+    stats = p.steps[0].solve(1, p, st, opts=fx.solve_opts(**kw))
+    return st.displacements, stats
+
+
+CASES = {
+    "c3d4_cantilever": lambda: decks.c3d4_cantilever(),          # 14,883 DOF, 2 levels
+    "c3d20_3_levels": lambda: decks.c3d20_box(8, 8, 32),
+    "c3d20_small": lambda: decks.c3d20_box(2, 2, 3),
+    "random_c3d4": lambda: decks.random_box(np.random.default_rng(9), 20000.0, 4)[0],
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("prec,tol", [(fx.PREC_MIXED, 1e-8), (fx.PREC_FP64, 1e-10)])
+def test_persistent_matches_multi_launch_and_oracle(ctx, case, prec, tol):
+    text = CASES[case]()
+    ref = _oracle_run(text)
+    u1, s1 = _solve(ctx, text, precision=prec)                                # persistent (small system)
+    u2, s2 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1)     # one launch per step
+    e1 = float(np.linalg.norm(u1 - ref) / np.linalg.norm(ref))
+    e2 = float(np.linalg.norm(u2 - ref) / np.linalg.norm(ref))
+    assert e1 <= tol and e2 <= tol, (e1, e2)
+    assert abs(s1["pcg_iterations"] - s2["pcg_iterations"]) <= 4, (s1["pcg_iterations"], s2["pcg_iterations"])
+    assert s1["last_linear_relres"] <= 1e-8
+
+
+def test_persistent_solve_is_repeatable(ctx):
+    text = CASES["c3d20_3_levels"]()
+    a, _ = _solve(ctx, text)
+    b, _ = _solve(ctx, text)
+    assert np.array_equal(a, b)
+
+
+def test_persistent_iteration_cap_and_breakdown(ctx):
+    text = decks.c3d4_cantilever(3, 3, 6)
+    with pytest.raises(fx.FerrixError) as e:
+        _solve(ctx, text, max_iter=2)
+    assert e.value.kind == "ConvergenceError"
+    # a model without boundary conditions: singular, found by the multigrid setup or the CG
+    lines, keep, skip = text.split("\n"), [], False
+    for line in lines:
+        if line.upper().startswith("*BOUNDARY"):
+            skip = True
+            continue
+        if skip and not line.startswith("*"):
+            continue
+        skip = False
+        keep.append(line)
+    with pytest.raises(fx.FerrixError) as e:
+        _solve(ctx, "\n".join(keep))
+    assert e.value.kind == "NumericalError"

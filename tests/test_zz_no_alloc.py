@@ -60,6 +60,11 @@ def test_spmv_dot_noalloc_matches_existing_entry_points():
                                        C.c_void_p(d_dat.data_ptr()), C.c_void_p(d_u.data_ptr()),
                                        C.c_void_p(d_y.data_ptr()), C.c_void_p(d_dot.data_ptr()),
                                        C.c_void_p(stream.cuda_stream)) == 18
+        # y written in place of x would be read by other rows: refused on the host, nothing launched
+        assert lib.fx_spmv_dot_noalloc(0, n, C.c_void_p(d_ip.data_ptr()), C.c_void_p(d_ind.data_ptr()),
+                                       C.c_void_p(d_dat.data_ptr()), C.c_void_p(d_u.data_ptr()),
+                                       C.c_void_p(d_u.data_ptr() + 8), C.c_void_p(d_dot.data_ptr()),
+                                       C.c_void_p(stream.cuda_stream)) == 18
         p.close()
     finally:
         ctx.close()
