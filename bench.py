@@ -124,6 +124,66 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+BATCH_DECKS = 64
+
+
+def _batch_figure(ctx, stream):
+    """64 C3D4 box decks of the batched workload's population (DOF log-uniform [2k, 60k],
+    E log-uniform, random load), built from arrays (fx_model_from_arrays, no text) and
+    solved by one fx_batch_solve with the default options: each deck's first step
+    (pattern, assembly, multigrid setup, CG to 1e-8, Newton re-check); the small
+    systems' CG iterations all run in one persistent launch. Device time, mean of two
+    timed batches after one untimed."""
+    import numpy as np
+    import torch
+    import ferrix_b200 as fx
+    from ferrix_b200 import decks
+    pop = decks.batch_population(BATCH_DECKS, seed=7, dof_lo=2e3, dof_hi=6e4, c3d20_fraction=0.0, arrays=True)
+    opts = fx.solve_opts()
+    times, first = [], None
+    for rep in range(3):
+        ps = [fx.Project.from_arrays(**dict(kw, default_temperature=20.0), ctx=ctx) for kw, _ in pop]
+        for p in ps:
+            fx.SolutionState(p.num_dofs, p.num_nodes).initialize(p)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        status, stats = fx.batch_solve(ctx, ps, opts)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rep > 0:
+            times.append(e0.elapsed_time(e1))
+        if first is None:
+            first = []
+            for p in ps[:2]:
+                st = fx.SolutionState(p.num_dofs, p.num_nodes)
+                st.project = p
+                first.append(st.displacements)
+        for p in ps:
+            p.close()
+    ms = float(np.mean(times))
+    return {"decks": BATCH_DECKS, "total_dofs": int(sum(d for _, d in pop)), "device_ms": ms,
+            "solves_per_s": BATCH_DECKS / (ms * 1e-3), "failed": int(np.sum(status != 0)),
+            "pcg_iterations_max": int(max(s["pcg_iterations"] for s in stats)),
+            "solver": "default (mixed multigrid CG; systems up to 100k DOF in one persistent cluster launch)",
+            "input": "fx_model_from_arrays"}, first
+
+
+def _batch_oracle_errors(first):
+    """Relative errors of the first two batch decks against the oracle's FP64 direct solve."""
+    import numpy as np
+    from ferrix_b200 import decks
+    from oracle import inp, static_step
+    errs = []
+    for (text, _), u in zip(decks.batch_population(2, seed=7, dof_lo=2e3, dof_hi=6e4, c3d20_fraction=0.0), first):
+        o = inp.parse_inp_text(text)
+        o.default_initial_temperature = 20.0
+        ref = static_step.Runner(o).run().displacements
+        errs.append(float(np.linalg.norm(u - ref) / np.linalg.norm(ref)))
+    return errs
+
+
 def run_reference(args, rank: int, world: int) -> None:
     """--impl reference: the reference's CPU path (oracle port) on this host's cores, rank 0 only."""
     if rank != 0:
@@ -599,15 +659,20 @@ def main():
                + 2 * project.num_nodes * 8)
         d2h = project.num_dofs * 8
 
+    batch_line = batch_first = None
+    if rank == 0 and not args.no_arms:
+        batch_line, batch_first = _batch_figure(ctx, stream)
+
     serving_line = None
     if rank == 0 and not args.no_arms:
         from ferrix_b200 import serving
-        pool = serving.make_pool()
+        pool = serving.make_pool(arrays=True)  # the same 16 models as the deck pool, built from arrays
         res = serving.run_stream(pool, 25.0, 32, fx.solve_opts(precision=fx.PREC_MIXED, preconditioner=fx.PRECOND_AMG),
                                  device=local, slots=4, seed=25)
         serving_line = _serve_summary(res)
         serving_line["solver"] = "mixed multigrid CG"
         serving_line["pool"] = "16 seeded boxes, 60% C3D4 / 40% C3D20, DOF log-uniform [5k, 500k]"
+        serving_line["input"] = "fx_model_from_arrays"
 
     cpu = None
     rel_err = None
@@ -630,6 +695,8 @@ def main():
             pass
     for a in arms.values():
         a.pop("u", None)
+    if batch_line is not None and oracle_p is not None:
+        batch_line["rel_err_vs_oracle_first2"] = _batch_oracle_errors(batch_first)
 
     if rank == 0:
         import json as _j
@@ -692,6 +759,7 @@ def main():
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "ms_per_step": e2e_elapsed * 1e3 if e2e_elapsed else None},
             "cpu_baseline": cpu,
+            "batch": batch_line,
             "serving": serving_line,
         }
         print(json.dumps(line), flush=True)

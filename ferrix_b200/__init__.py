@@ -298,12 +298,21 @@ class Project:
                                          float(a.get("shift_x", 0.0)), float(a.get("shift_y", 0.0)))
         d.n_amplitudes, d.amplitudes = len(amplitudes), C.cast(amps, C.c_void_p)
 
+        rec_dtype = np.dtype({"names": ["node_id", "dof", "amplitude", "value", "origin_step"],
+                              "formats": [np.int64, np.int32, np.int32, np.float64, np.int64],
+                              "offsets": [0, 8, 12, 16, 24], "itemsize": C.sizeof(_lib.RecordDesc)})
+
         def records(recs):
-            r = (_lib.RecordDesc * max(1, len(recs)))()
-            for k, (nid, dof, val, amp, org) in enumerate(recs):
-                r[k] = _lib.RecordDesc(int(nid), int(dof), int(amp), float(val), int(org))
+            if isinstance(recs, np.ndarray) and recs.dtype == rec_dtype:
+                r = np.ascontiguousarray(recs)
+            else:
+                r = np.zeros(len(recs), dtype=rec_dtype)
+                if len(recs):
+                    cols = list(zip(*recs))
+                    r["node_id"], r["dof"], r["value"] = cols[0], cols[1], cols[2]
+                    r["amplitude"], r["origin_step"] = cols[3], cols[4]
             keep.append(r)
-            return len(recs), C.cast(r, C.c_void_p)
+            return r.size, (r.ctypes.data_as(C.c_void_p) if r.size else None)
 
         sts = (_lib.StepDesc * max(1, len(steps)))()
         for k, st in enumerate(steps):

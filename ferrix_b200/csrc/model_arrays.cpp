@@ -46,6 +46,10 @@ void add_elements(Project& p, int64_t n, const int64_t* ids, const int64_t* node
                   int n_materials, const char* type) {
     const std::string t(type);
     require(n >= 0 && (n == 0 || (ids && nodes)), t + " elements without arrays");
+    p.elem_line_off.reserve(p.elem_line_off.size() + (size_t)n);
+    p.elem_line_ids.reserve(p.elem_line_ids.size() + (size_t)n);
+    p.elem_line_npe.reserve(p.elem_line_npe.size() + (size_t)n);
+    p.elem_line_conn.reserve(p.elem_line_conn.size() + (size_t)n * npe);
     for (int64_t e = 0; e < n; ++e) {
         p.elem_line_off.push_back((int64_t)p.elem_line_conn.size());
         p.elem_line_ids.push_back(ids[e]);

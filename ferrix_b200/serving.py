@@ -23,14 +23,19 @@ from . import Project, Server, decks, _lib
 
 
 def make_pool(n: int = 16, seed: int = 2027, dof_lo: float = 5e3, dof_hi: float = 5e5,
-              c3d20_fraction: float = 0.4) -> List[str]:
-    return [text for text, _ in decks.batch_population(n, seed=seed, dof_lo=dof_lo, dof_hi=dof_hi,
-                                                        c3d20_fraction=c3d20_fraction)]
+              c3d20_fraction: float = 0.4, arrays: bool = False) -> List[object]:
+    """The seeded deck pool: deck texts, or with arrays=True the same models as
+    Project.from_arrays arguments (the binary mesh path, no text)."""
+    return [d for d, _ in decks.batch_population(n, seed=seed, dof_lo=dof_lo, dof_hi=dof_hi,
+                                                  c3d20_fraction=c3d20_fraction, arrays=arrays)]
 
 
-def _host_model(text: str) -> Project:
-    p = Project.from_inp_text(text)
-    p.default_initial_temperature = 20.0
+def _host_model(entry) -> Project:
+    if isinstance(entry, dict):
+        p = Project.from_arrays(**dict(entry, default_temperature=20.0))
+    else:
+        p = Project.from_inp_text(entry)
+        p.default_initial_temperature = 20.0
     n4 = C.c_int64()
     n20 = C.c_int64()
     # builds the dense arrays now (counts only), so that submission is cheap
@@ -54,8 +59,13 @@ def run_stream(pool: List[str], rate: float, n_requests: int, opts, device: int 
     try:
         # the smallest deck of each element type once per slot: loads the kernels of both
         # element types and builds every slot's workspaces before the timed stream
-        kinds = [[t for t in pool if ("C3D20" in t) == is20] for is20 in (False, True)]
-        smalls = [min(k, key=len) for k in kinds if k]
+        def is20(e):
+            return e["c3d20"] is not None if isinstance(e, dict) else "C3D20" in e
+
+        def size(e):
+            return len(e["node_ids"]) if isinstance(e, dict) else len(e)
+        kinds = [[t for t in pool if is20(t) == want] for want in (False, True)]
+        smalls = [min(k, key=size) for k in kinds if k]
         warm = [_host_model(t) for t in smalls for _ in range(slots)]
         for t in [srv.submit(w) for w in warm]:
             srv.wait(t, timeout=600.0)
