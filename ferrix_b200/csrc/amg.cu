@@ -1759,11 +1759,15 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
         o.r = l.r.ptr;
         FX_LAUNCH((k_l0_op<VT, kL0RUpd, g32>), grid, 256, 0, s, o);  // r = b - A x
     }
-    FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
-              l.Q.ptr, l.r.ptr, c.b.ptr, coarse_start(1));
-    coarse(1, s);
-    if (g32) FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4, alpha_);
-    else FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, alpha_);
+    if (fused_coarse_ && !kcycle_ && desc_.ptr) {  // restriction, coarse levels, prolongation: one launch
+        launch_coarse_grid(desc_.ptr, gbar_.ptr, gflag_, g32, degree_, alpha_, s);
+    } else {
+        FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
+                  l.Q.ptr, l.r.ptr, c.b.ptr, coarse_start(1));
+        coarse(1, s);
+        if (g32) FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4, alpha_);
+        else FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, alpha_);
+    }
     for (int st = 0; st < degree_; ++st) {
         L0Op<VT> o = op();
         o.b = b;
@@ -1978,6 +1982,19 @@ void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* 
     sc_.zero(s);
     counter_.alloc(1, s);
     counter_.zero(s);
+    // the fused coarse cycle reads the hierarchy from a device descriptor, re-uploaded
+    // after every setup / refresh (new eigenvalue estimates, new Chebyshev coefficients);
+    // a barrier timeout sets S[7]
+    amg.set_fused_coarse(opt.amg_fused_coarse && !opt.amg_kcycle, sc_.ptr + 7);
+    if (opt.amg_fused_coarse && !opt.amg_kcycle) amg.upload_descriptor(s);
+}
+
+void Amg::upload_descriptor(cudaStream_t s) {
+    ClInst h{};
+    describe(h);
+    desc_.upload(&h, 1, s);
+    gbar_.alloc(1, s);
+    gbar_.zero(s);
 }
 
 ClInst AmgPcg::describe(const double* b, double* x) const {
@@ -2074,6 +2091,7 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     while (true) {
         FX_CUDA_CHECK(cudaMemcpyAsync(h, sc_.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
         stream_wait(s, "amg pcg poll");
+        if (h[7] != 0.0) fail(FX_TIMEOUT, "multigrid: a grid barrier of the coarse cycle timed out");
         if (h[6] != 0.0) {
             rc = FX_NUMERICAL;
             break;

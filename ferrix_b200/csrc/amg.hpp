@@ -26,6 +26,12 @@
 
 namespace fx {
 
+// State of the software grid barrier of the cooperative coarse-cycle launch (zeroed
+// before a solve; a wait that ran out leaves it inconsistent until then).
+struct GridBarState {
+    unsigned int count, gen;
+};
+
 struct ClInst;
 
 struct AmgLevel {
@@ -117,6 +123,14 @@ class Amg {
     Start0 start0() const;
     // the hierarchy, smoother coefficients and work vectors, for the persistent solve
     void describe(ClInst& out) const;
+    // The coarse part of each V-cycle as one cooperative launch (on: after every setup /
+    // refresh the hierarchy's descriptor is uploaded; flag = where a barrier timeout is
+    // reported) or as one launch per coarse-level step (off).
+    void set_fused_coarse(bool on, double* flag) {
+        fused_coarse_ = on;
+        gflag_ = flag;
+    }
+    void upload_descriptor(cudaStream_t s);
     int degree() const { return degree_; }
     double overcorrect() const { return alpha_; }
     std::vector<AmgLevel> L;
@@ -136,6 +150,10 @@ class Amg {
     double alpha_ = 1.0, cheb_ratio_ = 30.0;
     int degree_ = 2;
     const float* vals0_f32_ = nullptr;
+    bool fused_coarse_ = false;
+    double* gflag_ = nullptr;
+    DBuf<ClInst> desc_;
+    DBuf<GridBarState> gbar_;
     DBuf<uint8_t> tmp_;
     DBuf<double> red_;  // reduction scratch
 };
@@ -190,6 +208,11 @@ struct ClResult {
 // coarse corrections scaled by alpha.
 void launch_amg_cluster(const ClInst* insts, ClResult* res, int n, bool fp32, double rtol, int max_iter, int degree,
                         double alpha, cudaStream_t s);
+// The coarse part of one V-cycle (restriction from the level-0 residual, coarse
+// levels, prolongation into the level-0 iterate) of the system `inst` describes,
+// as one cooperative launch over all SMs; *flag = 1 when a barrier wait ran out.
+void launch_coarse_grid(const ClInst* inst, GridBarState* st, double* flag, bool fp32, int degree, double alpha,
+                        cudaStream_t s);
 // Systems of at most this many DOF are solved by the persistent launch by default.
 constexpr int64_t kClDefaultMaxDof = 100000;
 

@@ -19,6 +19,7 @@
 // counts.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "amg.hpp"
@@ -405,6 +406,115 @@ __device__ __noinline__ double start0_op(Vg g, const ClInst& I, double alpha, bo
 
 // One V-cycle for the right-hand side I.r (level-0 start already done by start0_op):
 // z = cycle(r); returns this thread's part of r.z (the last post-smoothing step).
+// Barriers between the phases of a cycle: the cluster's hardware barrier, or
+// (for one system spread over the whole GPU) a software grid barrier whose wait
+// is bounded; sync() returns false when that wait ran out.
+struct ClusterBar {
+    cg::cluster_group& cl;
+    __device__ __forceinline__ bool sync() {
+        cl.sync();
+        return true;
+    }
+};
+
+constexpr unsigned kGridSpinLimit = 1u << 22;  // polls of the barrier generation (~0.2-1 s) before giving up
+
+struct GridBar {
+    GridBarState* st;
+    double* flag;  // set to 1 when a wait ran out
+    unsigned nblocks;
+    __device__ bool sync() {
+        __shared__ int ok;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            ok = 1;
+            volatile unsigned* gen = &st->gen;
+            const unsigned g0 = *gen;  // read before arriving: the last arrival moves it on
+            __threadfence();
+            if (atomicAdd(&st->count, 1u) == nblocks - 1) {
+                atomicExch(&st->count, 0u);
+                __threadfence();
+                atomicAdd(&st->gen, 1u);
+            } else {
+                unsigned polls = 0;
+                while (*gen == g0) {
+                    if (++polls > kGridSpinLimit) {
+                        ok = 0;
+                        *flag = 1.0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        return ok != 0;
+    }
+};
+
+// The coarse part of one V-cycle, from the level-0 residual I.lr: restriction into
+// level 1 (with its first smoothing step unless it is the coarsest), the coarse
+// levels down to the dense coarsest solve and back up, and the prolongation of the
+// correction into the level-0 iterate (I.lx, and I.x4 with FP32 smoother vectors).
+// Returns false when a barrier wait ran out (the caller stops).
+template <bool G32, typename Bar>
+__device__ bool coarse_cycle(const ClInst& I, Vg g, int degree, double alpha, Bar& bar) {
+    // restriction into level 1 (with its first smoothing step unless it is the coarsest)
+    {
+        const ClLevel& c = I.lev[1];
+        restrict_op(g, I.n_agg, I.agg_ptr, I.agg_nodes, 3, I.Q, I.lr, c.b, c.coarsest ? nullptr : c.dinv, c.r, c.d,
+                    c.xs, c.c2_start);
+        if (!bar.sync()) return false;
+    }
+    // coarse levels: down to the coarsest, dense solve, back up
+    int m = 1;
+    const int last = min(I.levels, kClMaxLevels) - 1;  // the coarsest level (setup always ends with one)
+    for (; m < last && !I.lev[m].coarsest; ++m) {
+        const ClLevel& l = I.lev[m];
+        double* cA = l.d;
+        double* cB = l.t;
+        for (int st = 1; st < degree; ++st) {
+            ln_op<kOpChebK>(l, g, cA, nullptr, l.r, cB, l.xs, l.c1[st], l.c2[st]);
+            if (!bar.sync()) return false;
+            double* t = cA;
+            cA = cB;
+            cB = t;
+        }
+        ln_op<kOpRUpd>(l, g, cA, nullptr, l.r, nullptr, nullptr, 0.0, 0.0);
+        if (!bar.sync()) return false;
+        const ClLevel& c = I.lev[m + 1];
+        restrict_op(g, l.n_agg, l.agg_ptr, l.agg_nodes, 6, l.Q, l.r, c.b, c.coarsest ? nullptr : c.dinv, c.r, c.d,
+                    c.xs, c.c2_start);
+        if (!bar.sync()) return false;
+    }
+    {
+        const ClLevel& l = I.lev[m];
+        dense_op(g, 6 * l.n, l.dense_inv, l.b, l.x);
+        if (!bar.sync()) return false;
+    }
+    for (--m; m >= 1; --m) {
+        const ClLevel& l = I.lev[m];
+        const ClLevel& c = I.lev[m + 1];
+        prolong_op(g, 6 * l.n, 6, l.agg, l.Q, c.x, l.xs, alpha);
+        if (!bar.sync()) return false;
+        double* cA = l.d;
+        double* cB = l.t;
+        ln_op<kOpCheb0>(l, g, l.xs, l.b, l.r, cA, l.x, 0.0, l.c2_start);
+        if (!bar.sync()) return false;
+        for (int st = 1; st < degree; ++st) {
+            ln_op<kOpChebK>(l, g, cA, nullptr, l.r, cB, l.x, l.c1[st], l.c2[st]);
+            if (!bar.sync()) return false;
+            double* t = cA;
+            cA = cB;
+            cB = t;
+        }
+    }
+    if (G32) prolong0_op(g, I, I.lev[1].x, alpha);
+    else prolong_op(g, 3 * I.n, 3, I.agg, I.Q, I.lev[1].x, I.lx, alpha);
+    return bar.sync();
+}
+
 template <typename VT, bool G32>
 __device__ double vcycle(const ClInst& I, Vg g, const VT* vals, int degree, double alpha, cg::cluster_group& cl) {
     double dummy = 0.0;
@@ -427,63 +537,9 @@ __device__ double vcycle(const ClInst& I, Vg g, const VT* vals, int degree, doub
     l0_op<VT, kOpRUpd, G32>(I, g, vals, dA, reinterpret_cast<const float4*>(dA4), nullptr, nullptr, I.lr, nullptr,
                             nullptr, nullptr, 0.0, 0.0, false, dummy);  // r = b - A x
     cl.sync();
-    // restriction into level 1 (with its first smoothing step unless it is the coarsest)
-    {
-        const ClLevel& c = I.lev[1];
-        restrict_op(g, I.n_agg, I.agg_ptr, I.agg_nodes, 3, I.Q, I.lr, c.b, c.coarsest ? nullptr : c.dinv, c.r, c.d,
-                    c.xs, c.c2_start);
-        cl.sync();
-    }
-    // coarse levels: down to the coarsest, dense solve, back up
-    int m = 1;
-    const int last = min(I.levels, kClMaxLevels) - 1;  // the coarsest level (setup always ends with one)
-    for (; m < last && !I.lev[m].coarsest; ++m) {
-        const ClLevel& l = I.lev[m];
-        double* cA = l.d;
-        double* cB = l.t;
-        for (int st = 1; st < degree; ++st) {
-            ln_op<kOpChebK>(l, g, cA, nullptr, l.r, cB, l.xs, l.c1[st], l.c2[st]);
-            cl.sync();
-            double* t = cA;
-            cA = cB;
-            cB = t;
-        }
-        ln_op<kOpRUpd>(l, g, cA, nullptr, l.r, nullptr, nullptr, 0.0, 0.0);
-        cl.sync();
-        const ClLevel& c = I.lev[m + 1];
-        restrict_op(g, l.n_agg, l.agg_ptr, l.agg_nodes, 6, l.Q, l.r, c.b, c.coarsest ? nullptr : c.dinv, c.r, c.d,
-                    c.xs, c.c2_start);
-        cl.sync();
-    }
-    {
-        const ClLevel& l = I.lev[m];
-        dense_op(g, 6 * l.n, l.dense_inv, l.b, l.x);
-        cl.sync();
-    }
-    for (--m; m >= 1; --m) {
-        const ClLevel& l = I.lev[m];
-        const ClLevel& c = I.lev[m + 1];
-        prolong_op(g, 6 * l.n, 6, l.agg, l.Q, c.x, l.xs, alpha);
-        cl.sync();
-        double* cA = l.d;
-        double* cB = l.t;
-        ln_op<kOpCheb0>(l, g, l.xs, l.b, l.r, cA, l.x, 0.0, l.c2_start);
-        cl.sync();
-        for (int st = 1; st < degree; ++st) {
-            ln_op<kOpChebK>(l, g, cA, nullptr, l.r, cB, l.x, l.c1[st], l.c2[st]);
-            cl.sync();
-            double* t = cA;
-            cA = cB;
-            cB = t;
-        }
-    }
-    // prolongation into level 0 and post-smoothing into z (the last step reduces r.z)
-    if (G32) {
-        prolong0_op(g, I, I.lev[1].x, alpha);
-    } else {
-        prolong_op(g, 3 * I.n, 3, I.agg, I.Q, I.lev[1].x, I.lx, alpha);
-    }
-    cl.sync();
+    ClusterBar bar{cl};
+    coarse_cycle<G32>(I, g, degree, alpha, bar);
+    // post-smoothing into z (the last step reduces r.z)
     double dsum = 0.0;
     l0_op<VT, kOpCheb0, G32>(I, g, vals, I.lx, reinterpret_cast<const float4*>(I.x4), I.r, nullptr, I.lr, dA, dA4,
                              I.z, 0.0, I.c2_start, degree == 1, dsum);
@@ -579,6 +635,16 @@ __global__ void __launch_bounds__(kClThreads, 2)
     }
 }
 
+// The coarse part of the V-cycle of one large system as one cooperative launch
+// (all CTAs resident), in place of a launch per coarse-level step.
+template <bool G32>
+__global__ void __launch_bounds__(kClThreads, 2) k_coarse_grid(const ClInst* __restrict__ inst, GridBarState* st,
+                                                               double* flag, int degree, double alpha) {
+    const Vg g{(int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(gridDim.x * blockDim.x)};
+    GridBar bar{st, flag, gridDim.x};
+    coarse_cycle<G32>(*inst, g, degree, alpha, bar);
+}
+
 template <typename VT, bool G32>
 void launch_t(const ClInst* insts, ClResult* res, int n, double rtol2, int max_iter, int degree, double alpha,
               cudaStream_t s) {
@@ -608,6 +674,45 @@ void launch_amg_cluster(const ClInst* insts, ClResult* res, int n, bool fp32, do
     const double rtol2 = rtol * rtol;
     if (fp32) launch_t<float, true>(insts, res, n, rtol2, max_iter, degree, alpha, s);
     else launch_t<double, false>(insts, res, n, rtol2, max_iter, degree, alpha, s);
+}
+
+unsigned coarse_grid_size() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 0;
+    if (!cached[dev]) {
+        int sms = 0, per = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_coarse_grid<true>, kClThreads, 0) != cudaSuccess) {
+            cudaGetLastError();
+            per = 0;
+        }
+        int per64 = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_coarse_grid<false>, kClThreads, 0) != cudaSuccess) {
+            cudaGetLastError();
+            per64 = 0;
+        }
+        cached[dev] = std::max(1, sms * std::min(per, per64));
+    }
+    return (unsigned)cached[dev];
+}
+
+void launch_coarse_grid(const ClInst* inst, GridBarState* st, double* flag, bool fp32, int degree, double alpha,
+                        cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(coarse_grid_size(), 1, 1);
+    cfg.blockDim = dim3(kClThreads, 1, 1);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (fp32) FX_CUDA_CHECK(cudaLaunchKernelEx(&cfg, k_coarse_grid<true>, inst, st, flag, degree, alpha));
+    else FX_CUDA_CHECK(cudaLaunchKernelEx(&cfg, k_coarse_grid<false>, inst, st, flag, degree, alpha));
+    if (g_launch_counter) ++*g_launch_counter;
+    if (debug_sync()) stream_wait(s, "k_coarse_grid", 20.0);
 }
 
 const void* kernels_anchor_amg_cluster() { return reinterpret_cast<const void*>(&k_amg_cluster<double, false>); }

@@ -607,6 +607,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         const double oc = rs[0]->o.amg_overcorrect;
         po.amg_overcorrect = oc > 0.0 && oc < 2.0 ? oc : kAmgOvercorrect;
         po.amg_cheb_ratio = rs[0]->o.amg_cheb_ratio > 1.0 ? rs[0]->o.amg_cheb_ratio : kAmgChebRatio;
+        po.amg_fused_coarse = rs[0]->o.amg_coarse_launches == 0;
         const int pm = rs[0]->o.amg_persistent_max_dof;
         po.amg_persistent_max_dof = pm == 0 ? kClDefaultMaxDof : pm;
     }

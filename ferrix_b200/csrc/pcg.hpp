@@ -112,6 +112,7 @@ struct PcgOptions {
     double amg_overcorrect = kAmgOvercorrect;  // scale of every coarse correction
     double amg_cheb_ratio = kAmgChebRatio;  // lmax / lmin of the first-kind Chebyshev interval
     int64_t amg_persistent_max_dof = 0;     // systems up to this size: one persistent cluster launch (< 0: never)
+    bool amg_fused_coarse = true;           // coarse part of each V-cycle as one cooperative launch
 };
 
 template <typename T>

@@ -98,6 +98,9 @@ typedef struct {
                                    whole CG in one persistent launch, one thread-block cluster per system
                                    (all such systems of a batch in the same launch); 0 = 100,000,
                                    < 0 = never (one launch per CG step and V-cycle phase) */
+    int amg_coarse_launches;    /* FX_PRECOND_AMG, V-cycle, larger systems: 0 = the coarse part of each
+                                   V-cycle (restriction, coarse levels, dense coarsest solve, prolongation)
+                                   is one cooperative launch over all SMs, 1 = one launch per step */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */

@@ -85,3 +85,18 @@ def test_persistent_iteration_cap_and_breakdown(ctx):
     with pytest.raises(fx.FerrixError) as e:
         _solve(ctx, "\n".join(keep))
     assert e.value.kind == "NumericalError"
+
+
+@pytest.mark.parametrize("prec", [fx.PREC_MIXED, fx.PREC_FP64])
+def test_fused_coarse_cycle_matches_per_step_launches(ctx, prec):
+    """The multi-launch path's coarse V-cycle part as one cooperative launch (default)
+    and as one launch per coarse-level step compute every row the same way: the
+    displacements agree bit for bit, and both match the oracle."""
+    text = CASES["c3d20_3_levels"]()
+    u1, s1 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1)
+    u2, s2 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1, amg_coarse_launches=1)
+    assert s1["amg_levels"] >= 3
+    assert np.array_equal(u1, u2) and s1["pcg_iterations"] == s2["pcg_iterations"]
+    ref = _oracle_run(text)
+    tol = 1e-8 if prec == fx.PREC_MIXED else 1e-10
+    assert np.linalg.norm(u1 - ref) <= tol * np.linalg.norm(ref)
