@@ -71,8 +71,10 @@ def _oracle_job(out_path: str, q, go=None) -> None:
     st = r.run()
     dt = time.perf_counter() - t0
     np.save(out_path, st.displacements)
+    threads = os.environ.get("OPENBLAS_NUM_THREADS")
     q.put({"seconds": dt, "phases": {k: round(v, 3) for k, v in vars(r.t).items()},
-           "cores": os.cpu_count(), "blas_threads": os.environ.get("OPENBLAS_NUM_THREADS", "all")})
+           "cores": int(threads) if threads else os.cpu_count(), "host_cores": os.cpu_count(),
+           "blas_threads": threads or "all"})
 
 
 class ClockSampler:
@@ -188,6 +190,9 @@ def run_reference(args, rank: int, world: int) -> None:
     """--impl reference: the reference's CPU path (oracle port) on this host's cores, rank 0 only."""
     if rank != 0:
         return
+    if args.threads > 0:  # before NumPy loads its BLAS (the oracle's only parallel part)
+        for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
+            os.environ[k] = str(args.threads)
     q = mp.get_context("spawn").Queue()
     t0 = time.perf_counter()
     _oracle_job(os.path.join("/tmp", f"u_oracle_ref_{os.getpid()}.npy"), q)
@@ -202,6 +207,7 @@ def run_reference(args, rank: int, world: int) -> None:
         "solver": {"name": "FP64 multifrontal Cholesky (oracle port of the reference DirectSolver path)",
                    "precision": "fp64"},
         "cpu_baseline": {"value": 1.0 / sec, "unit": "solves/s", "cores": res["cores"], "kind": "port",
+                         "host_cores": res["host_cores"],
                          "sample": "one full-size solve (the step is ~minutes on the CPU, so 1 step regardless of K)",
                          "phases_s": res["phases"]},
         "e2e": {"value": 1.0 / sec, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -498,6 +504,8 @@ def main():
     ap.add_argument("--mode", default="solve", choices=["solve", "spmv", "serve", "batch", "nlgeom", "once"],
                     help="spmv: only assemble and time REPS standalone SpMV launches (profiling case)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--threads", type=int, default=0,
+                    help="reference arm: BLAS threads of the CPU path (0 = all host cores; FerriX's default pool is 4)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

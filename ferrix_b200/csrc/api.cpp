@@ -164,6 +164,12 @@ int fx_ctx_create(int device, fx_ctx** out) {
         FX_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
         uint64_t keep = UINT64_MAX;
         FX_CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        // an allocation never takes memory whose free is still queued behind another
+        // stream's work: with that reuse, a request of one request-loop slot waited for the
+        // queued solve of another (set-up stalls of up to 0.7 s in the four-slot loop); the
+        // pool holds the memory reserved ahead, so allocations do not need it
+        int no = 0;
+        FX_CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
         c->tables.init(c->stream);
         return FX_OK;
     });

@@ -531,6 +531,7 @@ struct StepRunner {
         sys64.x = d.du.ptr;
         sys64.residual64 = sys32.residual64;
         sys64.warm_start = true;
+        sys64.bnorm2 = sys32.bnorm2_seen;  // the tolerance stays relative to the step's right-hand side
         fallback = true;
         S.fp64_fallbacks++;
     }

@@ -29,6 +29,22 @@ __device__ __forceinline__ void ld4(const double* p, int64_t i4, double o[4]) {
     o[3] = b.y;
 }
 
+// The three components of node j of a vector stored four per node (the fourth is
+// padding), in one 16-byte load (FP32) or two (FP64).
+__device__ __forceinline__ void ld_node(const float* v, int64_t j, float o[3]) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(v) + j);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+}
+__device__ __forceinline__ void ld_node(const double* v, int64_t j, double o[3]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(v) + 2 * j);
+    const double b = __ldg(v + 4 * j + 2);
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b;
+}
+
 // Fixed-order block reduction of NV doubles; result valid in thread 0.
 template <int NV>
 __device__ __forceinline__ void block_sum(double v[NV], double* sh /* [NV][32] */) {
@@ -119,8 +135,8 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
             const int c = sub < 3 ? sub : 0;
             T zc = 0, pc = 0;
             if (valid && sub < 3) {
-                zc = __ldg(z + 3 * (int64_t)row + c);
-                pc = __ldg(pold + 3 * (int64_t)row + c);
+                zc = __ldg(z + 4 * (int64_t)row + c);
+                pc = __ldg(pold + 4 * (int64_t)row + c);
             }
             double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll 2
@@ -129,12 +145,13 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
                 const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
                 T xv[4][3];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
+                for (int q = 0; q < 4; ++q) {
+                    T zq[3], pq[3];
+                    ld_node(z, cj[q], zq);
+                    ld_node(pold, cj[q], pq);
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const int64_t at = 3 * (int64_t)cj[q] + k;
-                        xv[q][k] = __ldg(z + at) + beta * __ldg(pold + at);
-                    }
+                    for (int k = 0; k < 3; ++k) xv[q][k] = zq[k] + beta * pq[k];
+                }
                 const int64_t pl = (int64_t)ng;
                 const int64_t vb = (int64_t)g0 * 9 + g;
 #pragma unroll
@@ -158,7 +175,7 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
                 const T qc = (T)(c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]));
                 const T pn = zc + beta * pc;
                 I.q[at] = qc;
-                pnew[at] = pn;
+                pnew[4 * (int64_t)row + c] = pn;
                 dot += (double)pn * (double)qc;
             }
         }
@@ -195,7 +212,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_update(const ChunkDev* __re
         T r[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            T pc = p[r3 + c];
+            T pc = p[4 * (int64_t)row + c];
             I.x[r3 + c] += alpha * (double)pc;
             r[c] = I.r[r3 + c] - (T)alpha * I.q[r3 + c];
             I.r[r3 + c] = r[c];
@@ -204,7 +221,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_update(const ChunkDev* __re
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             T zc = m[3 * c] * r[0] + m[3 * c + 1] * r[1] + m[3 * c + 2] * r[2];
-            I.z[r3 + c] = zc;
+            I.z[4 * (int64_t)row + c] = zc;
             rz += (double)r[c] * (double)zc;
             rr += (double)r[c] * (double)r[c];
         }
@@ -249,7 +266,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_pcg_replace(const ChunkDev* __r
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             T zc = m[3 * c] * r[0] + m[3 * c + 1] * r[1] + m[3 * c + 2] * r[2];
-            I.z[r3 + c] = zc;
+            I.z[4 * (int64_t)row + c] = zc;
             rz += (double)r[c] * (double)zc;
             double z64 = (double)m[3 * c] * r64[0] + (double)m[3 * c + 1] * r64[1] + (double)m[3 * c + 2] * r64[2];
             rz64 += r64[c] * z64;
@@ -309,15 +326,15 @@ void PcgBatch<T>::prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::
     d_counter_.zero(s);
     chunk0.assign(n, 0);
     nch.assign(n, 0);
-    // Chunks of at most kChunkRows rows, sized so that the SpMV's resident CTAs get
-    // equal shares: total rows over a whole number of chunks per resident CTA.
-    int64_t total = 0;
-    for (int i = 0; i < n; ++i) total += sys[i]->S->n_rows;
+    // Chunks of 64..kChunkRows rows. A system's chunks depend on its own row count only
+    // (its partial sums, and so its results, are the same alone and in a batch); a large
+    // system gets a whole number of equal chunks per resident SpMV CTA.
     const int64_t res = spmv_resident();
-    const int64_t per_cta = std::max<int64_t>(1, (total + res * kChunkRows - 1) / (res * kChunkRows));
-    const int64_t target = std::max<int64_t>(1, (total + res * per_cta - 1) / (res * per_cta));
     for (int i = 0; i < n; ++i) {
         const int rows = sys[i]->S->n_rows;
+        const int64_t per_cta = std::max<int64_t>(1, (rows + res * kChunkRows - 1) / (res * kChunkRows));
+        const int64_t target = std::min<int64_t>(kChunkRows, std::max<int64_t>(
+                                   64, (rows + res * per_cta - 1) / (res * per_cta)));
         chunk0[i] = (int)all_chunks.size();
         const int64_t k = std::max<int64_t>(1, (rows + target - 1) / target);
         for (int64_t j = 0; j < k; ++j) {
@@ -332,9 +349,11 @@ void PcgBatch<T>::prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::
         Work& w = work_[i];
         const size_t m = 3 * (size_t)S.S->n_rows;
         w.r.alloc(m, s);
-        w.z.alloc(m, s);
-        w.p0.alloc(m, s);
-        w.p1.alloc(m, s);
+        const size_t m4 = 4 * (size_t)S.S->n_rows;  // z and the directions: four per node (one padding)
+        w.z.alloc(m4, s);
+        w.p0.alloc(m4, s);
+        w.p1.alloc(m4, s);
+        w.z.zero(s);
         w.q.alloc(m, s);
         w.r64.alloc(m, s);
         w.p0.zero(s);
@@ -415,6 +434,20 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
         stream_wait(s, "pcg poll");
     };
     pull();
+    // a warm-started solve (the FP64 finish of a stalled mixed one) measures its
+    // residual against the original right-hand side, not its starting residual
+    for (int i = 0; i < n; ++i) {
+        double* sc = &h_scal[(size_t)i * kNScal];
+        if (sys[i]->warm_start && sys[i]->bnorm2 > 0.0) {
+            sc[kBnorm] = sys[i]->bnorm2;
+            sc[kThresh] = rtol2 * sys[i]->bnorm2;
+            FX_CUDA_CHECK(cudaMemcpyAsync(d_scal_.ptr + (size_t)i * kNScal + kBnorm, &sc[kBnorm], sizeof(double),
+                                          cudaMemcpyHostToDevice, s));
+            FX_CUDA_CHECK(cudaMemcpyAsync(d_scal_.ptr + (size_t)i * kNScal + kThresh, &sc[kThresh], sizeof(double),
+                                          cudaMemcpyHostToDevice, s));
+        }
+        sys[i]->bnorm2_seen = sc[kBnorm];
+    }
     std::vector<char> done(n, 0);
     std::vector<double> best(n, 1e300);
     std::vector<int> stall(n, 0);

@@ -47,7 +47,8 @@ struct InstDev {
     const int32_t* cols;
     const T* vals;
     const T* minv;
-    T *r, *z, *p0, *p1, *q;
+    T *r, *q;          // three per node
+    T *z, *p0, *p1;    // four per node (the fourth is padding): one vector load per gathered node
     double* x;
     const double* r64;
     double* scal;
@@ -71,12 +72,14 @@ struct PcgSystem {
     // r64 = b - A x in FP64 (device pointers); the FP64 operator of this system
     std::function<void(const double* x, const double* b, double* r64, cudaStream_t)> residual64;
     bool warm_start = false;    // start from the given x (r0 = b - A x by residual64) instead of x = 0
+    double bnorm2 = 0.0;        // warm start: ||b||_M^2 that rtol refers to (0: the starting residual's)
     // outputs
     int status = 0;
     bool stagnated = false;     // mixed: FP64 residual stopped improving across replacements
     long long iterations = 0;
     int replacements = 0;
     double relres = 0.0;  // final ||b - A x||_M / ||b||_M
+    double bnorm2_seen = 0.0;  // the ||.||_M^2 this solve measured its residual against
 };
 
 // Multigrid defaults, from a sweep on the 417k-DOF C3D20 box (136 -> 100 CG
