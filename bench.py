@@ -51,6 +51,33 @@ def _deck():
     return decks.c3d20_box()
 
 
+# CUDA-core peaks of a B200 at its maximum SM clock (148 SMs x 1.965 GHz x 2 flop per FMA):
+# 128 FP32 lanes and 64 FP64 lanes per SM. Nominal figures (no measured copy in this repo).
+CUDA_CORE_TFLOPS = {"fp32": 148 * 128 * 2 * 1.965e9 / 1e12, "fp64": 148 * 64 * 2 * 1.965e9 / 1e12}
+
+
+def _secondary(bj_ms, bj_bytes, asm, peak_gbs):
+    """Roofline entries beside the dominant kernel: the block-Jacobi PCG SpMV and the
+    assembly kernels (element stiffness against the nominal CUDA-core peak, the gather
+    against the measured copy bandwidth), each timed standalone with CUDA events."""
+    out = [{"kernel": "k_pcg_spmv<float> (block-Jacobi PCG SpMV)", "bound": "hbm", "unit": "GB/s",
+            "achieved": bj_bytes / (bj_ms * 1e-3) / 1e9, "peak": peak_gbs,
+            "frac": bj_bytes / (bj_ms * 1e-3) / 1e9 / peak_gbs, "ms_per_launch": bj_ms,
+            "bytes_per_launch": bj_bytes}]
+    for prec, (st_ms, flops, ga_ms, ga_bytes) in asm.items():
+        t = "double" if prec == "fp64" else "float"
+        tf = flops / (st_ms * 1e-3) / 1e12
+        out.append({"kernel": f"k_stiff20<{t}> (C3D20 element stiffness, 354,780 declared flop per element)",
+                    "bound": prec + " CUDA cores", "unit": "TFLOP/s", "achieved": tf,
+                    "peak": CUDA_CORE_TFLOPS[prec], "peak_source": "nominal 148 SM x lanes x 2 x 1.965 GHz",
+                    "frac": tf / CUDA_CORE_TFLOPS[prec], "ms_per_launch": st_ms, "flops_per_launch": flops})
+        gb = ga_bytes / (ga_ms * 1e-3) / 1e9
+        out.append({"kernel": f"k_bsr_gather<{t}> (element-pair blocks into BSR3)", "bound": "hbm",
+                    "unit": "GB/s", "achieved": gb, "peak": peak_gbs, "frac": gb / peak_gbs,
+                    "ms_per_launch": ga_ms, "bytes_per_launch": ga_bytes})
+    return out
+
+
 def _config(world: int) -> dict:
     """The workload as both arms print it (the solver used is reported beside it)."""
     return {"workload": WORKLOAD, "accuracy": "1e-8 relative displacement error vs the FP64 direct solution",
@@ -602,6 +629,7 @@ def main():
     else:
         spmv_ms, spmv_bytes = project.profile_spmv(prec if prec != fx.PREC_FP64_CSR else fx.PREC_FP64, 30)
     bj_ms, bj_bytes = project.profile_spmv(fx.PREC_MIXED, 30)
+    asm = {name: project.profile_assembly(pr, 10) for name, pr in (("fp64", fx.PREC_FP64), ("fp32", fx.PREC_MIXED))}
 
     arms = {}
     if rank == 0 and not args.no_arms:
@@ -758,10 +786,7 @@ def main():
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else
                          "fallback 6650 GB/s", "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms,
                          "traffic": traffic, "traffic_source": f"profiles/{prof_name} (ncu)",
-                         "secondary": {"kernel": "k_pcg_spmv<float> (block-Jacobi PCG SpMV)",
-                                       "achieved": bj_bytes / (bj_ms * 1e-3) / 1e9,
-                                       "frac": bj_bytes / (bj_ms * 1e-3) / 1e9 / peak,
-                                       "ms_per_launch": bj_ms, "bytes_per_launch": bj_bytes}},
+                         "secondary": _secondary(bj_ms, bj_bytes, asm, peak)},
             "clocks": clk,
             "e2e": {"value": 1.0 / e2e_elapsed if e2e_elapsed else None, "unit": "solves/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

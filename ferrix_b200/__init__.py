@@ -410,6 +410,13 @@ class Project:
         """Legacy ASCII VTK of the current state (VtkWriter::write_increment, src/solver/io/vtk.rs:72-319)."""
         _check(self.lib.fx_write_vtk(self.handle, os.fsencode(path)), self.ctx)
 
+    def profile_assembly(self, precision: int = PREC_FP64, reps: int = 10):
+        """fx_profile_assembly: (stiffness ms, declared FLOPs, gather ms, gather bytes) per launch."""
+        a, b, c, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib.fx_profile_assembly(self.handle, precision, reps, C.byref(a), C.byref(b), C.byref(c),
+                                            C.byref(d)), self.ctx)
+        return a.value, b.value, c.value, d.value
+
     def profile_smoother(self, precision: int = PREC_MIXED, reps: int = 20):
         """(mean ms, compulsory bytes) of one fused fine-level multigrid smoothing step."""
         ms = C.c_double()

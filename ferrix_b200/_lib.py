@@ -140,6 +140,8 @@ SIGNATURES = {
     "fx_model_drop_cache": (C.c_int, [P]),
     "fx_profile_spmv": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_profile_smoother": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fx_profile_assembly": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_nodal_stress_strain": (C.c_int, [P, P, P]),
     "fx_write_vtk": (C.c_int, [P, C.c_char_p]),
     "fx_batch_solve": (C.c_int, [P, P, C.c_int, C.POINTER(SolveOpts), P, P]),

@@ -497,6 +497,71 @@ int fx_profile_spmv(fx_model* m, int precision, int reps, double* ms, double* by
     });
 }
 
+int fx_profile_assembly(fx_model* m, int precision, int reps, double* stiff_ms, double* stiff_flops,
+                        double* gather_ms, double* gather_bytes) {
+    if (!m || !m->ctx || !stiff_ms || !stiff_flops || !gather_ms || !gather_bytes || reps <= 0 || !m->state_ready)
+        return FX_INVALID_ARGUMENT;
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        int64_t* saved = g_launch_counter;
+        g_launch_counter = &m->ctx->launches;
+        struct R {
+            int64_t* v;
+            ~R() { g_launch_counter = v; }
+        } r{saved};
+        ensure_dense(m);
+        if (m->dense.missing_node_id >= 0)
+            fail_detail(FX_NODE_NOT_FOUND, m->dense.missing_node_error, -1, m->dense.missing_node_id, "");
+        ensure_structure(m);
+        ModelDev& d = m->dev;
+        cudaStream_t s = m->ctx->stream;
+        const bool fp64 = precision != FX_PREC_MIXED;
+        const size_t slots = (size_t)d.g4().n * kPairs4 + (size_t)d.g20().n * kPairs20;
+        const size_t tsz = fp64 ? sizeof(double) : sizeof(float);
+        auto stiff = [&] {
+            if (fp64)
+                launch_stiffness<double>(d.g4(), d.g20(), d.xyz.ptr, nullptr, d.tcur.ptr, d.mats.view(),
+                                         m->ctx->tables.view(), d.ebuf64.ptr, d.maxdiag.ptr, d.err.ptr, s);
+            else
+                launch_stiffness<float>(d.g4(), d.g20(), d.xyz.ptr, nullptr, d.tcur.ptr, d.mats.view(),
+                                        m->ctx->tables.view(), d.ebuf32.ptr, d.maxdiag.ptr, d.err.ptr, s);
+        };
+        auto gather = [&] {
+            if (fp64) launch_bsr_gather<double>(d.S, d.ebuf64.ptr, d.vals64.ptr, s);
+            else launch_bsr_gather<float>(d.S, d.ebuf32.ptr, d.vals32.ptr, s);
+        };
+        if (fp64) {
+            d.ebuf64.alloc(slots * 9 + 9, s);
+            d.vals64.alloc((size_t)d.S.n_groups * 36, s);
+        } else {
+            d.ebuf32.alloc(slots * 9 + 9, s);
+            d.vals32.alloc((size_t)d.S.n_groups * 36, s);
+        }
+        d.maxdiag.zero(s);
+        for (int k = 0; k < 2; ++k) {  // warm-up
+            stiff();
+            gather();
+        }
+        check_device_errors(m, "stiffness");
+        EventTimer t;
+        t.start(s);
+        for (int k = 0; k < reps; ++k) stiff();
+        *stiff_ms = t.stop_ms(s) / reps;
+        t.start(s);
+        for (int k = 0; k < reps; ++k) gather();
+        *gather_ms = t.stop_ms(s) / reps;
+        // declared FLOPs: 13,140 per Gauss point x 27 for C3D20 (D.B plus the symmetric upper
+        // B^T (D B)), 900 per C3D4 element
+        *stiff_flops = 354780.0 * d.g20().n + 900.0 * d.g4().n;
+        // compulsory bytes of the gather: every element-pair block read once, the sorted slot
+        // list (both orientations of every off-diagonal pair), the per-block segment offsets
+        // and every 3x3 block written once
+        *gather_bytes = (double)slots * 9.0 * tsz + 4.0 * (double)d.S.n_pairs +
+                        (double)d.S.n_blocks * (8.0 + 9.0 * tsz);
+        return FX_OK;
+    });
+}
+
 int fx_profile_smoother(fx_model* m, int precision, int reps, double* ms, double* bytes) {
     if (!m || !m->ctx || !ms || !bytes || reps <= 0 || !m->state_ready) return FX_INVALID_ARGUMENT;
     return guarded(m->ctx, [&] {

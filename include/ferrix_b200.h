@@ -340,6 +340,18 @@ int fx_profile_spmv(fx_model* model, int precision, int reps, double* ms, double
  * support for the FX_PRECOND_AMG path. */
 int fx_profile_smoother(fx_model* model, int precision, int reps, double* ms, double* bytes);
 
+/* Same measurement for the assembly (Assembler::assemble, src/solver/assembler.rs:37-151):
+ * `reps` standalone launches of the element stiffness kernels (precision
+ * FX_PREC_MIXED: FP32 element matrices, else FP64) on X with the current
+ * temperatures, then of the gather of the element-pair blocks into the BSR3
+ * values. *stiff_flops = declared FLOPs of one launch (354,780 per C3D20, 900
+ * per C3D4 element: D B and the symmetric upper B^T (D B) per Gauss point),
+ * *gather_bytes = compulsory traffic of one gather (element-pair blocks read
+ * once, slot list, segment offsets, blocks written once). Measurement support,
+ * no counterpart in the reference. */
+int fx_profile_assembly(fx_model* model, int precision, int reps, double* stiff_ms, double* stiff_flops,
+                        double* gather_ms, double* gather_bytes);
+
 /* ---- result fields ---------------------------------------------------- */
 /* StaticStep::calculate_stress_strain (src/solver/step/static_step.rs:271-379):
  * nodal-averaged stress and mechanical strain of the current state, 6 Voigt
