@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <cuda_fp16.h>
+
 #include "amg.hpp"
 
 namespace fx {
@@ -752,6 +754,9 @@ struct L0Op {
     // node (x, y, z, 0) and the new direction written into the same layout
     const float4* v4;
     float* d4_out;
+    // FP16 values of the diagonally scaled matrix S A S (S = diag(a_ii)^-1/2): sqrt(a_ii)
+    // per node; the gathered float4 vectors then hold sqrt(a_jj) v_j
+    const float4* sq4;
 };
 
 __device__ __forceinline__ void ld4v(const float* p, float o[4]) {
@@ -760,6 +765,15 @@ __device__ __forceinline__ void ld4v(const float* p, float o[4]) {
     o[1] = v.y;
     o[2] = v.z;
     o[3] = v.w;
+}
+__device__ __forceinline__ void ld4v(const __half* p, float o[4]) {
+    const uint2 v = __ldcs(reinterpret_cast<const uint2*>(p));
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
 }
 __device__ __forceinline__ void ld4v(const double* p, double o[4]) {
     const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
@@ -844,6 +858,9 @@ constexpr int kL0Unroll = FX_L0_UNROLL;  // groups of a row in flight per lane
 // them (Cheb0: the iterate), else from o.v4.
 template <typename VT, int MODE, bool G32 = false>
 __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
+    // FP16 values (of the scaled matrix): FP32 gathers of the scaled vectors, row sums
+    // scaled back by sqrt(a_ii), directions written scaled
+    constexpr bool H = std::is_same<VT, __half>::value;
     const int sub = threadIdx.x & (kL0Lanes - 1);
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> kL0LaneShift;
     const int rows_per_grid = (gridDim.x * blockDim.x) >> kL0LaneShift;
@@ -861,6 +878,8 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
         const int c = sub < 3 ? sub : 0;
         const bool epi = valid && sub < 3;
         double src3[3] = {0.0, 0.0, 0.0}, Dr[3] = {0.0, 0.0, 0.0}, vc = 0.0, xoc = 0.0, bc = 0.0, zoc = 0.0;
+        float4 sqi = make_float4(1.f, 1.f, 1.f, 0.f);
+        if (H && epi) sqi = __ldg(o.sq4 + row);
         if (epi) {
             if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
                 const double* src = MODE == kL0Cheb0 ? o.b : o.r;
@@ -872,6 +891,7 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
                 if (G32 && MODE == kL0ChebK) {
                     const float* own = reinterpret_cast<const float*>(o.v4 + row);
                     vc = (double)own[c];
+                    if (H) vc /= (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z));
                 } else {
                     vc = v[o3 + c];
                 }
@@ -913,7 +933,8 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
             const int64_t pl = (int64_t)ng * 4;
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
-                VT m0[4], m1[4], m2[4];
+                using MT = typename std::conditional<H, float, VT>::type;
+                MT m0[4], m1[4], m2[4];
                 ld4v(vb + (3 * r) * pl, m0);
                 ld4v(vb + (3 * r + 1) * pl, m1);
                 ld4v(vb + (3 * r + 2) * pl, m2);
@@ -929,6 +950,11 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
 #pragma unroll
             for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], s);
         // epilogue: lane c of the row's 8 handles component c
+        if (H) {  // (A v)_i = sqrt(a_ii) (S A S (sqrt(a_jj) v_j))_i
+            acc[0] *= (double)sqi.x;
+            acc[1] *= (double)sqi.y;
+            acc[2] *= (double)sqi.z;
+        }
         const double axc = c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]);
         __syncwarp();  // every lane's reads of r (above) are ordered before any lane writes r[c]
         if (!epi) continue;
@@ -944,7 +970,7 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
             const double z = Dr[0] * rr[0] + Dr[1] * rr[1] + Dr[2] * rr[2];
             o.r[o3 + c] = c == 0 ? rr[0] : (c == 1 ? rr[1] : rr[2]);
             const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * vc) + o.c2 * z;
-            if (G32) o.d4_out[4 * (int64_t)row + c] = (float)dn;
+            if (G32) o.d4_out[4 * (int64_t)row + c] = (float)(H ? dn * (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z)) : dn);
             else o.d_out[o3 + c] = dn;
             const double xn = (MODE == kL0Cheb0 ? vc : xoc) + dn;
             o.xo[o3 + c] = xn;
@@ -1112,6 +1138,14 @@ __global__ void __launch_bounds__(256) k_ln_op(LnOp o) {
     }
 }
 
+// FP32 copy of a node's three components for the smoother's gathers; with the FP16
+// scaled matrix (sq4 != null) multiplied by sqrt(a_ii) per component.
+__device__ __forceinline__ float4 scaled4(const double t[3], const float4* __restrict__ sq4, int i) {
+    if (!sq4) return make_float4((float)t[0], (float)t[1], (float)t[2], 0.0f);
+    const float4 q = sq4[i];
+    return make_float4((float)(t[0] * (double)q.x), (float)(t[1] * (double)q.y), (float)(t[2] * (double)q.z), 0.0f);
+}
+
 // first smoothing step from x = 0 at any level: d = c2 D^-1 b; x = d; r = b
 __global__ void k_cheb_start(int n, int bs, const double* __restrict__ dinv, const double* __restrict__ b,
                              double* __restrict__ r, double* __restrict__ d, double* __restrict__ x, double c2) {
@@ -1133,7 +1167,7 @@ __global__ void k_cheb_start(int n, int bs, const double* __restrict__ dinv, con
 // (d4 != null: the direction as float4 per node instead of d)
 __global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const double* __restrict__ b,
                                 double* __restrict__ r, double* __restrict__ d, float4* __restrict__ d4,
-                                double* __restrict__ x, double c2) {
+                                double* __restrict__ x, double c2, const float4* __restrict__ sq4) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t o3 = 3 * (int64_t)i;
@@ -1146,7 +1180,7 @@ __global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const do
         r[o3 + c] = bb[c];
         x[o3 + c] = t[c];
     }
-    if (d4) d4[i] = make_float4((float)t[0], (float)t[1], (float)t[2], 0.0f);
+    if (d4) d4[i] = scaled4(t, sq4, i);
     else
         for (int c = 0; c < 3; ++c) d[o3 + c] = t[c];
 }
@@ -1154,7 +1188,7 @@ __global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const do
 // fine level: x += Q xc (3 rows per node) and the FP32 copy of x for the smoother gathers
 __global__ void k_prolong0(int n, const int32_t* __restrict__ agg, const double* __restrict__ Q,
                            const double* __restrict__ xc, double* __restrict__ xf, float4* __restrict__ x4,
-                           double alpha) {
+                           double alpha, const float4* __restrict__ sq4) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double* x = xc + (int64_t)agg[i] * 6;
@@ -1166,7 +1200,7 @@ __global__ void k_prolong0(int n, const int32_t* __restrict__ agg, const double*
         out[k] = xf[3 * (int64_t)i + k] + alpha * t;
         xf[3 * (int64_t)i + k] = out[k];
     }
-    x4[i] = make_float4((float)out[0], (float)out[1], (float)out[2], 0.0f);
+    x4[i] = scaled4(out, sq4, i);
 }
 
 // The CG update fused with the first step of the V-cycle that follows it:
@@ -1178,7 +1212,7 @@ __global__ void __launch_bounds__(256) k_amg_update_start(int n, double* __restr
                                                           double* __restrict__ part, int* __restrict__ counter,
                                                           double* __restrict__ r0, double* __restrict__ x0,
                                                           double* __restrict__ d0, float4* __restrict__ d4,
-                                                          double c2) {
+                                                          double c2, const float4* __restrict__ sq4) {
     __shared__ double sh[32];
     __shared__ int s_last;
     const double alpha = S[5];
@@ -1200,7 +1234,7 @@ __global__ void __launch_bounds__(256) k_amg_update_start(int n, double* __restr
             t[c] = c2 * dr;
             x0[o3 + c] = t[c];
         }
-        if (d4) d4[i] = make_float4((float)t[0], (float)t[1], (float)t[2], 0.0f);
+        if (d4) d4[i] = scaled4(t, sq4, i);
         else
             for (int c = 0; c < 3; ++c) d0[o3 + c] = t[c];
     }
@@ -1224,6 +1258,52 @@ __global__ void __launch_bounds__(256) k_amg_update_start(int n, double* __restr
     if (lane == 0) {
         S[2] = tt;
         *counter = 0;
+    }
+}
+
+// sqrt of the fine matrix's diagonal per DOF (float4 per node; 1 where a node has no
+// diagonal block or a non-positive diagonal)
+__global__ void k_diag_sqrt(int n, const int32_t* __restrict__ goff, const int32_t* __restrict__ diag_k,
+                            const double* __restrict__ vals, float4* __restrict__ sq4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int kk = diag_k[i];
+    float o[3] = {1.f, 1.f, 1.f};
+    if (kk >= 0) {
+        const int64_t g0 = goff[i], ng = goff[i + 1] - g0;
+        for (int c = 0; c < 3; ++c) {
+            const double a = vals[(g0 * 9 + (int64_t)(4 * c) * ng + kk / 4) * 4 + (kk & 3)];
+            if (a > 0.0) o[c] = (float)sqrt(a);
+        }
+    }
+    sq4[i] = make_float4(o[0], o[1], o[2], 0.f);
+}
+
+// FP16 copy of the scaled matrix S A S, S = diag(sqrt(a_ii))^-1 with the float square
+// roots of k_diag_sqrt (the smoother scales its vectors by the same values): |entries| <= 1
+// for a symmetric positive definite matrix; warp per block row, lanes over column groups.
+__global__ void k_vals_to_f16(int n, const int32_t* __restrict__ goff, const int32_t* __restrict__ cols,
+                              const double* __restrict__ vals, const float4* __restrict__ sq4, __half* __restrict__ out) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const int64_t g0 = goff[row], ng = goff[row + 1] - g0;
+    const float4 sr = sq4[row];
+    const double srow[3] = {sr.x, sr.y, sr.z};
+    for (int64_t g = lane; g < ng; g += 32) {
+        const int4 cc = reinterpret_cast<const int4*>(cols)[g0 + g];
+        const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
+        double scol[4][3];
+        for (int q = 0; q < 4; ++q) {
+            const float4 t = sq4[cj[q]];
+            scol[q][0] = t.x;
+            scol[q][1] = t.y;
+            scol[q][2] = t.z;
+        }
+        for (int e = 0; e < 9; ++e)
+            for (int q = 0; q < 4; ++q) {
+                const int64_t at = (g0 * 9 + (int64_t)e * ng + g) * 4 + q;
+                out[at] = __double2half(vals[at] / (srow[e / 3] * scol[q][e % 3]));
+            }
     }
 }
 
@@ -1724,8 +1804,8 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     const int64_t nd = (int64_t)l.n * 3;
     const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
     const unsigned grid = l0_grid(l.n);
-    // FP32 values: the smoother's gathered vectors are FP32 too (float4 per node)
-    constexpr bool g32 = sizeof(VT) == 4;
+    // FP32 or FP16 values: the smoother's gathered vectors are FP32 (float4 per node)
+    constexpr bool g32 = !std::is_same<VT, double>::value;
     double* dA = l.d.ptr;
     double* dB = l.t.ptr;
     float4* dA4 = reinterpret_cast<float4*>(l.d4a.ptr);
@@ -1733,9 +1813,10 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     float4* x4 = reinterpret_cast<float4*>(l.x4.ptr);
     if (!started)
         FX_LAUNCH(k_l0_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.dinv0, b, l.r.ptr, dA, g32 ? dA4 : nullptr,
-                  l.x.ptr, k.c2_start);
+                  l.x.ptr, k.c2_start, sq4_);
     auto op = [&]() {
         L0Op<VT> o = l0_op<VT>(l, vals);
+        o.sq4 = sq4_;
         return o;
     };
     for (int st = 1; st < degree_; ++st) {
@@ -1765,7 +1846,9 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
         FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
                   l.Q.ptr, l.r.ptr, c.b.ptr, coarse_start(1));
         coarse(1, s);
-        if (g32) FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4, alpha_);
+        if (g32)
+            FX_LAUNCH(k_prolong0, grid_for(l.n), 256, 0, s, l.n, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, x4, alpha_,
+                      sq4_);
         else FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, 3, l.agg.ptr, l.Q.ptr, c.x.ptr, l.x.ptr, alpha_);
     }
     for (int st = 0; st < degree_; ++st) {
@@ -1805,7 +1888,8 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
 
 void Amg::apply(const double* r, double* z, double* S, double* part, int* counter, const double* zold,
                 cudaStream_t s, bool started) {
-    if (vals0_f32_) vcycle0<float>(vals0_f32_, r, z, S, part, counter, zold, s, started);
+    if (vals0_f16_) vcycle0<__half>(vals0_f16_, r, z, S, part, counter, zold, s, started);
+    else if (vals0_f32_) vcycle0<float>(vals0_f32_, r, z, S, part, counter, zold, s, started);
     else vcycle0<double>(L[0].vals0, r, z, S, part, counter, zold, s, started);
 }
 
@@ -1815,8 +1899,9 @@ Amg::Start0 Amg::start0() const {
     o.r = l.r.ptr;
     o.x = l.x.ptr;
     o.d = l.d.ptr;
-    o.d4 = vals0_f32_ ? reinterpret_cast<float4*>(l.d4a.ptr) : nullptr;
+    o.d4 = vals0_f32_ || vals0_f16_ ? reinterpret_cast<float4*>(l.d4a.ptr) : nullptr;
     o.c2 = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_).c2_start;
+    o.sq4 = sq4_;
     return o;
 }
 
@@ -1894,6 +1979,7 @@ void Amg::describe(ClInst& o) const {
     o.vals64 = l0.vals0;
     o.vals32 = vals0_f32_;
     o.dinv0 = l0.dinv0;
+    o.sq4 = sq4_;
     o.agg = l0.agg.ptr;
     o.agg_ptr = l0.agg_ptr.ptr;
     o.agg_nodes = l0.agg_nodes.ptr;
@@ -1945,18 +2031,26 @@ void Amg::describe(ClInst& o) const {
 }
 
 void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
-                     double cell0, const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse) {
+                     double cell0, const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse, bool persistent) {
     const int n = S.n_rows;
     const int64_t nd = 3 * (int64_t)n;
     if (opt.amg_degree < 1 || opt.amg_degree > 8) fail(FX_INVALID_ARGUMENT, "multigrid smoother degree must be 1..8");
     const float* v32 = nullptr;
-    if (opt.amg_fp32) {
+    const bool f16 = opt.amg_fp32 && opt.amg_fp16 && !persistent;
+    if (f16) {  // FP16 values of S A S and the scales; the eigenvalue estimates use the FP64 matrix
+        sq4_.alloc((size_t)n, s);
+        FX_LAUNCH(k_diag_sqrt, grid_for(n), 256, 0, s, n, S.goff.ptr, S.diag_k.ptr, vals64, sq4_.ptr);
+        vals16_.alloc((size_t)S.n_groups * 36, s);
+        FX_LAUNCH(k_vals_to_f16, grid_for((int64_t)n * 32), 256, 0, s, n, S.goff.ptr, S.cols.ptr, vals64, sq4_.ptr,
+                  vals16_.ptr);
+    } else if (opt.amg_fp32) {
         const int64_t nv = (int64_t)S.n_groups * 36;
         vals32_.alloc(nv, s);
         FX_LAUNCH(k_f64_to_f32, 148 * 8, 256, 0, s, nv, vals64, vals32_.ptr);
         v32 = vals32_.ptr;
     }
     amg.set_smoother(opt.amg_degree, v32);  // before setup: its eigenvalue estimate uses v32
+    if (f16) amg.set_smoother_f16(vals16_.ptr, sq4_.ptr);
     if (reuse && amg.built_for == S.id && !amg.L.empty() && amg.L[0].n == n) {
         amg.refresh(vals64, dinv64, s, st);
     } else {
@@ -2060,7 +2154,7 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         FX_LAUNCH((k_l0_op<double, kL0Apply>), g0, 256, 0, s, o);  // q = A p, alpha
         const Amg::Start0 s0 = amg.start0();
         FX_LAUNCH(k_amg_update_start, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
-                  counter_.ptr, s0.r, s0.x, s0.d, s0.d4, s0.c2);  // x, r, r.D^-1 r; the V-cycle's first step
+                  counter_.ptr, s0.r, s0.x, s0.d, s0.d4, s0.c2, s0.sq4);  // x, r, r.D^-1 r; the V-cycle's first step
         amg.apply(r_.ptr, zn, sc_.ptr, part_.ptr, counter_.ptr, amg.kcycle() ? zo : nullptr, s, true);  // z, r.z, beta
         FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, zn, sc_.ptr, p_.ptr);
     };

@@ -19,6 +19,8 @@
 // Application: one V-cycle per PCG iteration.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include <vector>
 
 #include "kernels.hpp"
@@ -98,6 +100,14 @@ class Amg {
     void set_smoother(int degree, const float* vals_f32) {
         degree_ = degree;
         vals0_f32_ = vals_f32;
+        vals0_f16_ = nullptr;
+        sq4_ = nullptr;
+    }
+    // FP16 values of the scaled fine matrix S A S (S = diag(a_ii)^-1/2) and sqrt(a_ii) per
+    // node for the level-0 smoothing steps, in place of FP32 values (null: off)
+    void set_smoother_f16(const __half* vals16, const float4* sq4) {
+        vals0_f16_ = vals16;
+        sq4_ = sq4;
     }
     // K-cycle at the first coarse level (true) or V-cycles throughout.
     void set_cycle(bool kcycle) { kcycle_ = kcycle; }
@@ -119,6 +129,7 @@ class Amg {
         double *r, *x, *d;
         float4* d4;
         double c2;
+        const float4* sq4;  // FP16 smoother: the float4 direction is written scaled by sqrt(a_ii)
     };
     Start0 start0() const;
     // the hierarchy, smoother coefficients and work vectors, for the persistent solve
@@ -150,6 +161,8 @@ class Amg {
     double alpha_ = 1.0, cheb_ratio_ = 30.0;
     int degree_ = 2;
     const float* vals0_f32_ = nullptr;
+    const __half* vals0_f16_ = nullptr;
+    const float4* sq4_ = nullptr;
     bool fused_coarse_ = false;
     double* gflag_ = nullptr;
     DBuf<ClInst> desc_;
@@ -184,6 +197,7 @@ struct ClInst {
     const double* vals64 = nullptr;
     const float* vals32 = nullptr;
     const double* dinv0 = nullptr;
+    const float4* sq4 = nullptr;  // FP16 smoother: the FP32 iterate copy is scaled by sqrt(a_ii)
     const int32_t *agg = nullptr, *agg_ptr = nullptr, *agg_nodes = nullptr;
     const double* Q = nullptr;
     int n_agg = 0;
@@ -228,7 +242,7 @@ class AmgPcg {
     // For the persistent solve: set up (or refresh) the hierarchy for the system and
     // allocate the CG vectors, without iterating; then describe it for the kernel.
     void prepare(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz, double cell0,
-                 const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse);
+                 const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse, bool persistent = false);
     ClInst describe(const double* b, double* x) const;
     // ||b - A x||_D / ||b||_D of the assembled FP64 system after a persistent solve
     double true_relres(const double* b, const double* x, cudaStream_t s);
@@ -245,6 +259,8 @@ class AmgPcg {
     const double* dinv64_ = nullptr;
     DBuf<double> r_, z_, z2_, p_, q_, part_, sc_;
     DBuf<float> vals32_;
+    DBuf<__half> vals16_;
+    DBuf<float4> sq4_;
     DBuf<int> counter_;
 };
 

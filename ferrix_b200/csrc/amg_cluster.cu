@@ -356,7 +356,10 @@ __device__ __noinline__ void prolong0_op(Vg g, const ClInst& I, const double* xc
             out[k] = ldv(I.lx + 3 * (int64_t)i + k) + alpha * t;
             I.lx[3 * (int64_t)i + k] = out[k];
         }
-        reinterpret_cast<float4*>(I.x4)[i] = make_float4((float)out[0], (float)out[1], (float)out[2], 0.0f);
+        float4 q = make_float4(1.f, 1.f, 1.f, 0.f);
+        if (I.sq4) q = __ldg(I.sq4 + i);  // FP16 smoother: the gathered copy is scaled by sqrt(a_ii)
+        reinterpret_cast<float4*>(I.x4)[i] = make_float4((float)(out[0] * (double)q.x), (float)(out[1] * (double)q.y),
+                                                         (float)(out[2] * (double)q.z), 0.0f);
     }
 }
 

@@ -143,6 +143,7 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->amg_cheb_ratio = 0.0;
     o->amg_persistent_max_dof = 0;
     o->amg_coarse_launches = 0;
+    o->amg_fp16_smoother = 0;
 }
 
 int fx_ctx_create(int device, fx_ctx** out) {

@@ -609,6 +609,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         po.amg_overcorrect = oc > 0.0 && oc < 2.0 ? oc : kAmgOvercorrect;
         po.amg_cheb_ratio = rs[0]->o.amg_cheb_ratio > 1.0 ? rs[0]->o.amg_cheb_ratio : kAmgChebRatio;
         po.amg_fused_coarse = rs[0]->o.amg_coarse_launches == 0;
+        po.amg_fp16 = rs[0]->o.amg_fp16_smoother == 1;
         const int pm = rs[0]->o.amg_persistent_max_dof;
         po.amg_persistent_max_dof = pm == 0 ? kClDefaultMaxDof : pm;
     }
@@ -654,7 +655,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
                     // small system: hierarchy now, its whole CG in the round's persistent launch below
                     guard(i, [&] {
                         d.amg->prepare(d.S, d.vals64.ptr, d.minv64.ptr, r.amg_xyz.ptr, r.amg_cell, po, s, &ast,
-                                       reuse);
+                                       reuse, true);
                         r.S.amg_levels = ast.levels;
                         r.S.amg_setup_ms += ast.setup_ms;
                         cluster_ids.push_back(i);

@@ -116,6 +116,7 @@ struct PcgOptions {
     double amg_cheb_ratio = kAmgChebRatio;  // lmax / lmin of the first-kind Chebyshev interval
     int64_t amg_persistent_max_dof = 0;     // systems up to this size: one persistent cluster launch (< 0: never)
     bool amg_fused_coarse = true;           // coarse part of each V-cycle as one cooperative launch
+    bool amg_fp16 = false;                  // level-0 smoothing with FP16 values of the scaled matrix
 };
 
 template <typename T>

@@ -101,6 +101,10 @@ typedef struct {
     int amg_coarse_launches;    /* FX_PRECOND_AMG, V-cycle, larger systems: 0 = the coarse part of each
                                    V-cycle (restriction, coarse levels, dense coarsest solve, prolongation)
                                    is one cooperative launch over all SMs, 1 = one launch per step */
+    int amg_fp16_smoother;      /* FX_PRECOND_AMG with FX_PREC_MIXED, larger systems: 1 = the fine-level
+                                   smoother reads FP16 values of the diagonally scaled matrix
+                                   D^-1/2 K D^-1/2 (entries within [-1, 1]) instead of FP32 values of K;
+                                   0 = FP32 */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */

@@ -441,3 +441,19 @@ def test_context_preloads_every_kernel(ctx):
         assert c2.preloaded_kernels == n
     finally:
         c2.close()
+
+
+@pytest.mark.parametrize("case", ["c3d4_cantilever", "c3d20_box_3_levels"])
+def test_amg_fp16_smoother(ctx, case):
+    """Fine-level smoothing with FP16 values of the scaled matrix D^-1/2 K D^-1/2 (the CG
+    itself stays FP64): mixed-precision bound against the oracle, and about the iteration
+    count of the FP32 smoother (multi-launch path, which is where the option applies)."""
+    text = AMG_CASES[case]()
+    ref, _ = _oracle_run(text)
+    p, st = _project(ctx, text)
+    s16 = p.steps[0].solve(1, p, st, opts=fx.solve_opts(amg_fp16_smoother=1, amg_persistent_max_dof=-1))
+    err = _err(st.displacements, ref)
+    st.initialize(p)
+    s32 = p.steps[0].solve(1, p, st, opts=fx.solve_opts(amg_persistent_max_dof=-1))
+    assert err <= TOL_MIXED, (err, s16)
+    assert s16["pcg_iterations"] <= 1.25 * s32["pcg_iterations"] + 4, (s16["pcg_iterations"], s32["pcg_iterations"])
