@@ -419,11 +419,12 @@ class Project:
                                             C.byref(d)), self.ctx)
         return a.value, b.value, c.value, d.value
 
-    def profile_smoother(self, precision: int = PREC_MIXED, reps: int = 20):
+    def profile_smoother(self, precision: int = PREC_MIXED, reps: int = 20, fp16: bool = False):
         """(mean ms, compulsory bytes) of one fused fine-level multigrid smoothing step."""
         ms = C.c_double()
         by = C.c_double()
-        _check(self.lib.fx_profile_smoother(self.handle, precision, reps, C.byref(ms), C.byref(by)), self.ctx)
+        _check(self.lib.fx_profile_smoother(self.handle, precision, int(fp16), reps, C.byref(ms), C.byref(by)),
+               self.ctx)
         return ms.value, by.value
 
     def thermal_force(self) -> np.ndarray:

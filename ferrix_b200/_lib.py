@@ -140,7 +140,7 @@ SIGNATURES = {
     "fx_solve_csr": (C.c_int, [P, C.c_int64, P, P, P, P, P, C.POINTER(SolveOpts), C.POINTER(StepStats)]),
     "fx_model_drop_cache": (C.c_int, [P]),
     "fx_profile_spmv": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
-    "fx_profile_smoother": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fx_profile_smoother": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_profile_assembly": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fx_nodal_stress_strain": (C.c_int, [P, P, P]),

@@ -1907,12 +1907,21 @@ Amg::Start0 Amg::start0() const {
 
 // ------------------------------------------------------------------ AMG-preconditioned CG (FP64)
 
-double profile_smoother_op(const BsrStructure& S, const double* vals64, const double* dinv64, bool fp32, int reps,
-                           cudaStream_t s, double* bytes) {
+double profile_smoother_op(const BsrStructure& S, const double* vals64, const double* dinv64, bool fp32, bool fp16,
+                           int reps, cudaStream_t s, double* bytes) {
+    fp32 = fp32 || fp16;
     const int n = S.n_rows;
     const int64_t nd = 3 * (int64_t)n;
     DBuf<float> v32;
-    if (fp32) {
+    DBuf<__half> v16;
+    DBuf<float4> sq4;
+    if (fp16) {
+        sq4.alloc((size_t)n, s);
+        FX_LAUNCH(k_diag_sqrt, grid_for(n), 256, 0, s, n, S.goff.ptr, S.diag_k.ptr, vals64, sq4.ptr);
+        v16.alloc((size_t)S.n_groups * 36, s);
+        FX_LAUNCH(k_vals_to_f16, grid_for((int64_t)n * 32), 256, 0, s, n, S.goff.ptr, S.cols.ptr, vals64, sq4.ptr,
+                  v16.ptr);
+    } else if (fp32) {
         const int64_t nv = (int64_t)S.n_groups * 36;
         v32.alloc(nv, s);
         FX_LAUNCH(k_f64_to_f32, 148 * 8, 256, 0, s, nv, vals64, v32.ptr);
@@ -1936,7 +1945,19 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
     l.dinv0 = dinv64;
     const unsigned grid = l0_grid(n);
     auto launch = [&]() {
-        if (fp32) {
+        if (fp16) {
+            L0Op<__half> o = l0_op<__half>(l, v16.ptr);
+            o.v = v.ptr;
+            o.v4 = reinterpret_cast<const float4*>(v4.ptr);
+            o.r = r.ptr;
+            o.d_out = d.ptr;
+            o.d4_out = d4.ptr;
+            o.xo = xo.ptr;
+            o.c1 = 0.5;
+            o.c2 = 1e-9;
+            o.sq4 = sq4.ptr;
+            FX_LAUNCH((k_l0_op<__half, kL0ChebK, true>), grid, 256, 0, s, o);
+        } else if (fp32) {
             L0Op<float> o = l0_op<float>(l, v32.ptr);
             o.v = v.ptr;
             o.v4 = reinterpret_cast<const float4*>(v4.ptr);
@@ -1966,7 +1987,9 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
     // compulsory bytes: matrix values + column indices once, row offsets, and per
     // node the gathered direction (24 B FP64 / 16 B float4), r read+write (48), the
     // new direction (24 / 16), iterate read+write (48) and the 3x3 block inverse (72)
-    *bytes = (double)S.n_blocks * (9.0 * (fp32 ? 4.0 : 8.0) + 4.0) + 4.0 * (n + 1) + (fp32 ? 200.0 : 216.0) * n;
+    // (FP16: 2-byte values, and the 16-byte scales of each row)
+    const double vb = fp16 ? 2.0 : (fp32 ? 4.0 : 8.0);
+    *bytes = (double)S.n_blocks * (9.0 * vb + 4.0) + 4.0 * (n + 1) + (fp32 ? 200.0 : 216.0) * n + (fp16 ? 16.0 * n : 0.0);
     return ms;
 }
 

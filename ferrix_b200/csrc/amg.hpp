@@ -234,7 +234,8 @@ constexpr int64_t kClDefaultMaxDof = 100000;
 // CUDA-event time (ms per launch) of the fused fine-level Chebyshev step (SpMV +
 // smoother update) on the given FP64 system, with FP32 values when fp32; bytes =
 // compulsory traffic of one launch.
-double profile_smoother_op(const BsrStructure& S, const double* vals64, const double* dinv64, bool fp32, int reps,
+double profile_smoother_op(const BsrStructure& S, const double* vals64, const double* dinv64, bool fp32, bool fp16,
+                           int reps,
                            cudaStream_t s, double* bytes);
 
 class AmgPcg {

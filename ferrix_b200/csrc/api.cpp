@@ -563,7 +563,7 @@ int fx_profile_assembly(fx_model* m, int precision, int reps, double* stiff_ms, 
     });
 }
 
-int fx_profile_smoother(fx_model* m, int precision, int reps, double* ms, double* bytes) {
+int fx_profile_smoother(fx_model* m, int precision, int fp16, int reps, double* ms, double* bytes) {
     if (!m || !m->ctx || !ms || !bytes || reps <= 0 || !m->state_ready) return FX_INVALID_ARGUMENT;
     return guarded(m->ctx, [&] {
         FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
@@ -582,7 +582,7 @@ int fx_profile_smoother(fx_model* m, int precision, int reps, double* ms, double
         DBuf<double> minv;
         minv.alloc((size_t)m->dense.n_nodes * 9, s);
         launch_block_jacobi<double>(d.S, d.vals64.ptr, minv.ptr, s);
-        *ms = profile_smoother_op(d.S, d.vals64.ptr, minv.ptr, precision == FX_PREC_MIXED, reps, s, bytes);
+        *ms = profile_smoother_op(d.S, d.vals64.ptr, minv.ptr, precision == FX_PREC_MIXED, fp16 != 0, reps, s, bytes);
         return FX_OK;
     });
 }

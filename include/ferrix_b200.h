@@ -338,11 +338,12 @@ int fx_profile_spmv(fx_model* model, int precision, int reps, double* ms, double
 /* Same measurement for the multigrid preconditioner's fine-level operator: one
  * fused Chebyshev smoothing step (BSR3 SpMV with FP64 vectors, then the
  * row-local residual / 3x3 block-Jacobi / direction / iterate update), FP32
- * matrix values when precision is FX_PREC_MIXED, FP64 otherwise; *bytes =
+ * matrix values when precision is FX_PREC_MIXED (FP16 values of the scaled
+ * matrix when fp16 != 0, as amg_fp16_smoother), FP64 otherwise; *bytes =
  * compulsory traffic (values + column indices once, row offsets, 216 B per node
  * of vector and block-inverse traffic). No reference counterpart: measurement
  * support for the FX_PRECOND_AMG path. */
-int fx_profile_smoother(fx_model* model, int precision, int reps, double* ms, double* bytes);
+int fx_profile_smoother(fx_model* model, int precision, int fp16, int reps, double* ms, double* bytes);
 
 /* Same measurement for the assembly (Assembler::assemble, src/solver/assembler.rs:37-151):
  * `reps` standalone launches of the element stiffness kernels (precision
