@@ -624,8 +624,8 @@ def main():
 
     # dominant kernel, timed standalone with CUDA events on the context stream:
     # the fused fine-level smoothing step (multigrid) or the fused PCG SpMV
-    if use_amg:
-        spmv_ms, spmv_bytes = project.profile_smoother(prec, 30)
+    if use_amg:  # with mixed precision the default smoother reads FP16 values of the scaled matrix
+        spmv_ms, spmv_bytes = project.profile_smoother(prec, 30, fp16=prec == fx.PREC_MIXED)
     else:
         spmv_ms, spmv_bytes = project.profile_spmv(prec if prec != fx.PREC_FP64_CSR else fx.PREC_FP64, 30)
     bj_ms, bj_bytes = project.profile_spmv(fx.PREC_MIXED, 30)
@@ -748,8 +748,9 @@ def main():
         try:
             import re
             prof = open(os.path.join(ROOT, "profiles", prof_name)).read()
-            if use_amg:  # one row per precision: traffic_bytes_per_launch_<precision> | N
-                m = re.search(r"traffic_bytes_per_launch_%s[^|]*\|\s*([\d,]+)" % args.precision, prof)
+            if use_amg:  # one row per smoother variant: traffic_bytes_per_launch_<fp16|fp64> | N
+                variant = "fp16" if prec == fx.PREC_MIXED else args.precision
+                m = re.search(r"traffic_bytes_per_launch_%s[^|]*\|\s*([\d,]+)" % variant, prof)
                 if m:
                     traffic = int(m.group(1).replace(",", ""))
             else:
@@ -765,7 +766,7 @@ def main():
             "metric": METRIC, "value": world * args.steps / elapsed, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": elapsed / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"fp64": "f64", "mixed": ("f64 CG, f32 smoother matrix" if use_amg else
+            "dtype": {"fp64": "f64", "mixed": ("f64 CG, f16 scaled smoother matrix" if use_amg else
                                                "f32 matrix / f64 residual"), "fp64_csr": "f64"}[args.precision],
             "data": "synthetic (seeded .inp deck generator; inputs exceed L2: BSR3 FP64 matrix ~600 MB)",
             "config": _config(world),
@@ -779,7 +780,10 @@ def main():
             "phase_ms": {k: round(s0[k], 3) for k in ("t_assembly_ms", "t_pcg_ms", "t_total_ms")},
             "arms": arms,
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": ("k_l0_op<float, ChebK> (fused fine-level SpMV + Chebyshev update)"
+            "roofline": {"bound": "hbm", "kernel": ("k_l0_op<__half, ChebK> (fused fine-level SpMV + Chebyshev update, "
+                                                    "FP16 values of the scaled matrix)" if use_amg and
+                                                    prec == fx.PREC_MIXED else
+                                                    "k_l0_op<double, ChebK> (fused fine-level SpMV + Chebyshev update)"
                                                     if use_amg else
                                                     "k_pcg_spmv (fused BSR3 SpMV + direction update + p.q)"),
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -115,7 +115,7 @@ def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 
                reference_iterative: bool = False, preconditioner: int = PRECOND_AMG,
                amg_aggregate_nodes: int = 40, amg_smoother_degree: int = 2, amg_cycle: int = 0,
                amg_smoother: int = 0, amg_overcorrect: float = 0.0, amg_cheb_ratio: float = 0.0,
-               amg_persistent_max_dof: int = 0, amg_coarse_launches: int = 0,
+               amg_persistent_max_dof: int = 0, amg_fused_coarse: int = 0,
                amg_fp16_smoother: int = 0) -> SolveOpts:
     o = SolveOpts()
     _lib.load().fx_default_solve_opts(C.byref(o))
@@ -135,7 +135,7 @@ def solve_opts(precision: int = PREC_MIXED, rtol: float = 1e-8, max_iter: int = 
     o.amg_overcorrect = float(amg_overcorrect)
     o.amg_cheb_ratio = float(amg_cheb_ratio)
     o.amg_persistent_max_dof = int(amg_persistent_max_dof)
-    o.amg_coarse_launches = int(amg_coarse_launches)
+    o.amg_fused_coarse = int(amg_fused_coarse)
     o.amg_fp16_smoother = int(amg_fp16_smoother)
     return o
 

@@ -31,7 +31,7 @@ class SolveOpts(C.Structure):
                 ("reference_iterative", C.c_int), ("preconditioner", C.c_int),
                 ("amg_aggregate_nodes", C.c_int), ("amg_smoother_degree", C.c_int), ("amg_cycle", C.c_int),
                 ("amg_smoother", C.c_int), ("amg_overcorrect", C.c_double), ("amg_cheb_ratio", C.c_double),
-                ("amg_persistent_max_dof", C.c_int), ("amg_coarse_launches", C.c_int),
+                ("amg_persistent_max_dof", C.c_int), ("amg_fused_coarse", C.c_int),
                 ("amg_fp16_smoother", C.c_int)]
 
 

@@ -142,7 +142,7 @@ void fx_default_solve_opts(fx_solve_opts* o) {
     o->amg_overcorrect = 0.0;
     o->amg_cheb_ratio = 0.0;
     o->amg_persistent_max_dof = 0;
-    o->amg_coarse_launches = 0;
+    o->amg_fused_coarse = 0;
     o->amg_fp16_smoother = 0;
 }
 

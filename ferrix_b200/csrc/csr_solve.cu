@@ -27,7 +27,7 @@ constexpr int kStagnated = -1;
 
 template <typename T>
 static int solve_csr_t(fx_ctx* ctx, int64_t n, const int64_t* ip, const int64_t* ind, const double* data,
-                       const double* b, double* x, const fx_solve_opts& o, fx_step_stats* st) {
+                       const double* b, double* x, const fx_solve_opts& o, fx_step_stats* st, double accept_rtol = 0.0) {
     cudaStream_t s = ctx->stream;
     const int64_t nb = (n + 2) / 3;  // block rows
     const int64_t n3 = 3 * nb;
@@ -117,6 +117,7 @@ static int solve_csr_t(fx_ctx* ctx, int64_t n, const int64_t* ip, const int64_t*
     };
     PcgOptions po;
     po.rtol = sizeof(T) == 4 ? o.rtol * kMixedBjResidualFactor : o.rtol;
+    po.accept_rtol = accept_rtol;
     po.max_iter = o.max_iter;
     po.poll = o.poll_interval;
     po.reliable_delta = o.reliable_delta;
@@ -220,9 +221,9 @@ extern "C" int fx_solve_csr(fx_ctx* ctx, int64_t n, const int64_t* indptr, const
         if (rc != kStagnated) return rc;
         fx_step_stats first{};
         if (stats) first = *stats;
-        fx_solve_opts o64 = o;  // the mixed solve's FP64 target
+        fx_solve_opts o64 = o;  // the mixed solve's FP64 target (accepted at the caller's rtol where it stalls)
         o64.rtol = o.rtol * kMixedBjResidualFactor;
-        const int rc64 = solve_csr_t<double>(ctx, n, indptr, indices, data, b, x, o64, stats);
+        const int rc64 = solve_csr_t<double>(ctx, n, indptr, indices, data, b, x, o64, stats, o.rtol);
         if (stats) {
             stats->pcg_iterations += first.pcg_iterations;
             stats->reliable_updates += first.reliable_updates;

@@ -608,10 +608,13 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         const double oc = rs[0]->o.amg_overcorrect;
         po.amg_overcorrect = oc > 0.0 && oc < 2.0 ? oc : kAmgOvercorrect;
         po.amg_cheb_ratio = rs[0]->o.amg_cheb_ratio > 1.0 ? rs[0]->o.amg_cheb_ratio : kAmgChebRatio;
-        po.amg_fused_coarse = rs[0]->o.amg_coarse_launches == 0;
-        po.amg_fp16 = rs[0]->o.amg_fp16_smoother == 1;
+        po.amg_fused_coarse = rs[0]->o.amg_fused_coarse == 1;
+        po.amg_fp16 = rs[0]->o.amg_fp16_smoother >= 0;
+        // persistent cluster solve: for every small system of a round that solves several (one
+        // launch advances them all), for a lone system only when it is tiny (a cluster's few
+        // SMs are latency-bound where the multi-launch path uses the whole GPU)
         const int pm = rs[0]->o.amg_persistent_max_dof;
-        po.amg_persistent_max_dof = pm == 0 ? kClDefaultMaxDof : pm;
+        po.amg_persistent_max_dof = pm != 0 ? pm : (rs.size() > 1 ? kClDefaultMaxDof : kClSingleMaxDof);
     }
     while (true) {
         bool any = false;
@@ -711,6 +714,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
             if (!v32.empty()) {
                 PcgOptions p32 = po;  // mixed: the tightened residual target, also for its FP64 finish
                 p32.rtol = po.rtol * kMixedBjResidualFactor;
+                p32.accept_rtol = po.rtol;
                 ctx->pcg32.solve(v32, p32, s, &ctx->launches);
                 std::vector<PcgSystem<double>*> fb;
                 for (size_t i : bsr_ids)

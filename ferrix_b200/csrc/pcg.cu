@@ -104,24 +104,39 @@ __device__ __forceinline__ bool cta_running(const int* status) {
     return s_st == kRun;
 }
 
-// (A) q = K p_new, p_new = z + beta p_old (fused), partial p_new . q.
+// (C) p = z + beta p (four per node), a light pass before the SpMV so that the SpMV
+// gathers one vector.
+template <typename T>
+__global__ void __launch_bounds__(kUpdThreads) k_pcg_dir(const ChunkDev* __restrict__ chunks,
+                                                         const InstDev<T>* __restrict__ insts) {
+    const ChunkDev ck = chunks[blockIdx.x];
+    const InstDev<T> I = insts[ck.inst];
+    if (!cta_running(I.status)) return;
+    const T beta = (T)I.scal[kBeta];
+    for (int row = ck.row0 + threadIdx.x; row < ck.row1; row += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t at = 4 * (int64_t)row + c;
+            I.p0[at] = I.z[at] + beta * I.p0[at];
+        }
+}
+
+// (A) q = K p, partial p . q, alpha = r.z / p.q.
 // Persistent CTAs walk the chunk list (chunk c, c + gridDim.x, ...); in a chunk,
 // 8 lanes share a block row (32 rows per pass) and each lane keeps two column
-// groups in flight; with FP32 values each 4-block group is summed in FP32 and
-// added to the FP64 row sums. 256-thread CTAs, two per SM (at most 128 registers).
+// groups in flight, gathering one 16-byte (FP32) node vector per column; with FP32
+// values each 4-block group is summed in FP32 and added to the FP64 row sums.
+// 256-thread CTAs, two per SM (at most 128 registers).
 template <typename T>
 __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __restrict__ chunks, int nchunks,
-                                                             const InstDev<T>* __restrict__ insts, int parity) {
+                                                             const InstDev<T>* __restrict__ insts) {
     __shared__ double sh[4 * 32];
     const int sub = threadIdx.x & 7, grp = threadIdx.x >> 3;
     for (int ci = blockIdx.x; ci < nchunks; ci += gridDim.x) {
         const ChunkDev ck = chunks[ci];
         const InstDev<T> I = insts[ck.inst];
         if (!cta_running(I.status)) continue;  // CTA-uniform
-        const T beta = (T)I.scal[kBeta];
-        const T* __restrict__ pold = parity ? I.p1 : I.p0;
-        T* __restrict__ pnew = parity ? I.p0 : I.p1;
-        const T* __restrict__ z = I.z;
+        const T* __restrict__ p = I.p0;
         double dot = 0.0;
         const int nrows = ck.row1 - ck.row0;
         // The trip count is uniform across the CTA so that every lane reaches the
@@ -131,13 +146,9 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
             const int row = ck.row0 + (valid ? base + grp : 0);
             const int g0 = valid ? I.goff[row] : 0;
             const int ng = valid ? I.goff[row + 1] - g0 : 0;
-            // the row's own direction, loaded ahead of the gathers (lanes 0..2: one component each)
             const int c = sub < 3 ? sub : 0;
-            T zc = 0, pc = 0;
-            if (valid && sub < 3) {
-                zc = __ldg(z + 4 * (int64_t)row + c);
-                pc = __ldg(pold + 4 * (int64_t)row + c);
-            }
+            T pc = 0;
+            if (valid && sub < 3) pc = __ldg(p + 4 * (int64_t)row + c);  // ahead of the gathers
             double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll 2
             for (int g = sub; g < ng; g += 8) {
@@ -145,13 +156,7 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
                 const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
                 T xv[4][3];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    T zq[3], pq[3];
-                    ld_node(z, cj[q], zq);
-                    ld_node(pold, cj[q], pq);
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) xv[q][k] = zq[k] + beta * pq[k];
-                }
+                for (int q = 0; q < 4; ++q) ld_node(p, cj[q], xv[q]);
                 const int64_t pl = (int64_t)ng;
                 const int64_t vb = (int64_t)g0 * 9 + g;
 #pragma unroll
@@ -171,12 +176,9 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
 #pragma unroll
                 for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
             if (valid && sub < 3) {
-                const int64_t at = 3 * (int64_t)row + c;
                 const T qc = (T)(c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]));
-                const T pn = zc + beta * pc;
-                I.q[at] = qc;
-                pnew[4 * (int64_t)row + c] = pn;
-                dot += (double)pn * (double)qc;
+                I.q[3 * (int64_t)row + c] = qc;
+                dot += (double)pc * (double)qc;
             }
         }
         double v[1] = {dot}, tot[1];
@@ -199,13 +201,13 @@ __global__ void __launch_bounds__(kSpmvThreads, 2) k_pcg_spmv(const ChunkDev* __
 // (B) x += alpha p, r -= alpha q, z = M r, partial r.z and r.r
 template <typename T>
 __global__ void __launch_bounds__(kUpdThreads) k_pcg_update(const ChunkDev* __restrict__ chunks,
-                                                            const InstDev<T>* __restrict__ insts, int parity) {
+                                                            const InstDev<T>* __restrict__ insts) {
     __shared__ double sh[4 * 32];
     const ChunkDev ck = chunks[blockIdx.x];
     const InstDev<T> I = insts[ck.inst];
     if (!cta_running(I.status)) return;
     const double alpha = I.scal[kAlpha];
-    const T* __restrict__ p = parity ? I.p0 : I.p1;
+    const T* __restrict__ p = I.p0;
     double rz = 0.0, rr = 0.0;
     for (int row = ck.row0 + threadIdx.x; row < ck.row1; row += blockDim.x) {
         const int r3 = 3 * row;
@@ -352,12 +354,10 @@ void PcgBatch<T>::prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::
         const size_t m4 = 4 * (size_t)S.S->n_rows;  // z and the directions: four per node (one padding)
         w.z.alloc(m4, s);
         w.p0.alloc(m4, s);
-        w.p1.alloc(m4, s);
         w.z.zero(s);
         w.q.alloc(m, s);
         w.r64.alloc(m, s);
         w.p0.zero(s);
-        w.p1.zero(s);
         if (S.warm_start) {
             S.residual64(S.x, S.b, w.r64.ptr, s);
         } else {
@@ -375,7 +375,6 @@ void PcgBatch<T>::prepare(std::vector<PcgSystem<T>*>& sys, cudaStream_t s, std::
         d.r = w.r.ptr;
         d.z = w.z.ptr;
         d.p0 = w.p0.ptr;
-        d.p1 = w.p1.ptr;
         d.q = w.q.ptr;
         d.x = S.x;
         d.r64 = w.r64.ptr;
@@ -400,14 +399,17 @@ double PcgBatch<T>::profile_spmv(PcgSystem<T>& sys, int reps, cudaStream_t s) {
     sys.warm_start = false;
     prepare(v, s, chunks, c0, nc);
     FX_LAUNCH(k_pcg_replace<T>, (unsigned)chunks.size(), kUpdThreads, 0, s, d_chunks_.ptr, d_inst_.ptr, 1, 0.0);
+    // p = z (beta = 0 after the first replacement): a nonzero direction, so p.q > 0 and every
+    // timed launch does its full work
+    FX_LAUNCH(k_pcg_dir<T>, (unsigned)chunks.size(), kUpdThreads, 0, s, d_chunks_.ptr, d_inst_.ptr);
     for (int k = 0; k < 3; ++k)  // warm-up
         FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(chunks.size()), kSpmvThreads, 0, s, d_chunks_.ptr, (int)chunks.size(),
-                  d_inst_.ptr, k & 1);
+                  d_inst_.ptr);
     EventTimer t;
     t.start(s);
     for (int k = 0; k < reps; ++k)
         FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(chunks.size()), kSpmvThreads, 0, s, d_chunks_.ptr, (int)chunks.size(),
-                  d_inst_.ptr, k & 1);
+                  d_inst_.ptr);
     return t.stop_ms(s) / reps;
 }
 
@@ -487,10 +489,10 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
                 g_launch_counter = nullptr;
                 FX_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 for (int k = 0; k < poll; ++k) {
+                    FX_LAUNCH(k_pcg_dir<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr);
                     FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(act.size()), kSpmvThreads, 0, s, d_act.ptr, (int)act.size(),
-                              d_inst_.ptr, k & 1);
-                    FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr,
-                              k & 1);
+                              d_inst_.ptr);
+                    FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr);
                 }
                 FX_CUDA_CHECK(cudaStreamEndCapture(s, &g));
                 g_launch_counter = saved;
@@ -505,13 +507,14 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
             int64_t* saved = g_launch_counter;
             g_launch_counter = nullptr;
             for (int k = 0; k < poll; ++k) {
+                FX_LAUNCH(k_pcg_dir<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr);
                 FX_LAUNCH(k_pcg_spmv<T>, spmv_grid(act.size()), kSpmvThreads, 0, s, d_act.ptr, (int)act.size(),
-                          d_inst_.ptr, k & 1);
-                FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr, k & 1);
+                          d_inst_.ptr);
+                FX_LAUNCH(k_pcg_update<T>, (unsigned)act.size(), kUpdThreads, 0, s, d_act.ptr, d_inst_.ptr);
             }
             g_launch_counter = saved;
         }
-        if (launches) *launches += 2 * (int64_t)poll;
+        if (launches) *launches += 3 * (int64_t)poll;
         pull();
         if (trace)
             for (int i = 0; i < n; ++i)
@@ -574,6 +577,13 @@ int PcgBatch<T>::solve(std::vector<PcgSystem<T>*>& sys, const PcgOptions& opt, c
                 }
                 const bool slow = sc[kIters] - last_improve[i] >= opt.stall_iters || sc[kIters] >= 0.25 * opt.max_iter;
                 if (rel <= opt.rtol) {
+                    done[i] = 1;
+                    set_status(i, kIdle);
+                    rebuild = true;
+                } else if (sizeof(T) == 8 && opt.accept_rtol > 0.0 && rel <= opt.accept_rtol &&
+                           stall[i] >= opt.stall_limit) {
+                    // the attainable FP64 residual lies between the tightened target and the
+                    // caller's tolerance: converged at that floor
                     done[i] = 1;
                     set_status(i, kIdle);
                     rebuild = true;

@@ -15,8 +15,8 @@
 // FP64 (T = double): the same kernels on FP64 data; the true residual is
 // checked once at the end.
 //
-// Per iteration two kernels run per batch: (A) q = K p with the direction
-// update p = z + beta p fused into the gather and the p.q partial sum, (B)
+// Per iteration three kernels run per batch: (C) p = z + beta p, (A) q = K p with
+// the p.q partial sum (one gathered vector, four values per node), (B)
 // x += alpha p, r -= alpha q, z = M r and the r.z partial sum. Scalars are
 // reduced by the last CTA of each system in a fixed order (deterministic).
 // A block of `poll_interval` iterations is captured in a CUDA graph and
@@ -48,7 +48,7 @@ struct InstDev {
     const T* vals;
     const T* minv;
     T *r, *q;          // three per node
-    T *z, *p0, *p1;    // four per node (the fourth is padding): one vector load per gathered node
+    T *z, *p0;         // four per node (the fourth is padding): one vector load per gathered node
     double* x;
     const double* r64;
     double* scal;
@@ -107,6 +107,10 @@ struct PcgOptions {
     int stall_limit = 4;  // replacements without halving the best FP64 residual before giving up (mixed)
     int replace_every = 512;  // mixed: FP64 residual replacement at least this often (iterations)
     int stall_iters = 2048;   // mixed: give up on FP32 when the FP64 residual has not halved for this long
+    // FP64 finish of a mixed solve: rtol is the tightened target; once the FP64 true residual
+    // stops improving (stall_limit replacements without halving) at or below accept_rtol (the
+    // caller's own tolerance), the solve ends converged (0: no such acceptance)
+    double accept_rtol = 0.0;
     // multigrid preconditioner
     int amg_degree = 2;       // Chebyshev smoothing steps per pre/post smoothing
     bool amg_fp32 = false;    // FP32 fine-matrix values in the level-0 smoother
@@ -134,7 +138,7 @@ class PcgBatch {
     unsigned spmv_grid(size_t nchunks) { return (unsigned)std::min<int64_t>((int64_t)nchunks, spmv_resident()); }
     int64_t resident_ = 0;
     struct Work {
-        DBuf<T> r, z, p0, p1, q;
+        DBuf<T> r, z, p0, q;
         DBuf<double> r64;
     };
     std::vector<Work> work_;

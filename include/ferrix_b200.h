@@ -96,15 +96,17 @@ typedef struct {
     double amg_cheb_ratio;   /* FX_PRECOND_AMG: lmax / lmin of the first-kind Chebyshev interval; 0 = 12 */
     int amg_persistent_max_dof; /* FX_PRECOND_AMG, V-cycle: systems of at most this many DOF run their
                                    whole CG in one persistent launch, one thread-block cluster per system
-                                   (all such systems of a batch in the same launch); 0 = 100,000,
-                                   < 0 = never (one launch per CG step and V-cycle phase) */
-    int amg_coarse_launches;    /* FX_PRECOND_AMG, V-cycle, larger systems: 0 = the coarse part of each
-                                   V-cycle (restriction, coarse levels, dense coarsest solve, prolongation)
-                                   is one cooperative launch over all SMs, 1 = one launch per step */
-    int amg_fp16_smoother;      /* FX_PRECOND_AMG with FX_PREC_MIXED, larger systems: 1 = the fine-level
-                                   smoother reads FP16 values of the diagonally scaled matrix
-                                   D^-1/2 K D^-1/2 (entries within [-1, 1]) instead of FP32 values of K;
-                                   0 = FP32 */
+                                   (all such systems of a round in the same launch); 0 = default: 100,000
+                                   when several systems are solved together (fx_batch_solve), 2,000 for a
+                                   system solved alone; < 0 = never (one launch per CG step and phase) */
+    int amg_fused_coarse;       /* FX_PRECOND_AMG, V-cycle, systems on the multi-launch path: 1 = the coarse
+                                   part of each V-cycle (restriction, coarse levels, dense coarsest solve,
+                                   prolongation) as one cooperative launch over all SMs; 0 = one launch
+                                   per step (default; measured faster on B200) */
+    int amg_fp16_smoother;      /* FX_PRECOND_AMG with FX_PREC_MIXED, systems on the multi-launch path: the
+                                   fine-level smoother reads FP16 values of the diagonally scaled matrix
+                                   D^-1/2 K D^-1/2 (entries within [-1, 1]); 0 = default (FP16), 1 = FP16,
+                                   -1 = FP32 values of K */
 } fx_solve_opts;
 
 /* Preconditioner of the BSR3 PCG. */

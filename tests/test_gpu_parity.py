@@ -181,8 +181,13 @@ def test_nlgeom_thermal_beam(ctx):
 
 @pytest.mark.parametrize("pc", [fx.PRECOND_BLOCK_JACOBI, fx.PRECOND_AMG])
 def test_batch_matches_single(ctx, pc):
+    """A system's arithmetic does not depend on the others in its batch: alone and batched on
+    the same path (multigrid: the persistent cluster launch, threshold set for both) it gives
+    the same bits. (With the default options a lone multigrid system above 2,000 DOF takes the
+    multi-launch path instead; test_batch_default_options checks that case to the tolerance.)"""
     pop = decks.batch_population(6, seed=11, dof_lo=500, dof_hi=6000, c3d20_fraction=0.3)
-    o = fx.solve_opts(preconditioner=pc, precision=fx.PREC_MIXED)
+    o = fx.solve_opts(preconditioner=pc, precision=fx.PREC_MIXED,
+                      amg_persistent_max_dof=100000 if pc == fx.PRECOND_AMG else 0)
     singles = []
     for text, _ in pop:
         p, st = _project(ctx, text)
@@ -199,6 +204,25 @@ def test_batch_matches_single(ctx, pc):
         ref, _ = _oracle_run(text)
         err = _err(u, ref)
         assert err <= TOL_MIXED, err
+
+
+def test_batch_default_options(ctx):
+    """Default options: the batch's multigrid systems share one persistent launch, each system
+    alone takes the multi-launch path; both meet the mixed bound against the oracle."""
+    pop = decks.batch_population(4, seed=13, dof_lo=3000, dof_hi=20000, c3d20_fraction=0.5)
+    projs = [_project(ctx, text)[0] for text, _ in pop]
+    status, stats = fx.batch_solve(ctx, projs, fx.solve_opts())
+    assert np.all(status == 0)
+    for p, (text, _) in zip(projs, pop):
+        st = fx.SolutionState(p.num_dofs, p.num_nodes)
+        st.project = p
+        ub = st.displacements
+        q, sq = _project(ctx, text)
+        q.steps[0].solve(1, q, sq)
+        ref, _ = _oracle_run(text)
+        for u in (ub, sq.displacements):
+            err = _err(u, ref)
+            assert err <= TOL_MIXED, err
 
 
 def test_solve_csr_seam(ctx):
@@ -454,6 +478,6 @@ def test_amg_fp16_smoother(ctx, case):
     s16 = p.steps[0].solve(1, p, st, opts=fx.solve_opts(amg_fp16_smoother=1, amg_persistent_max_dof=-1))
     err = _err(st.displacements, ref)
     st.initialize(p)
-    s32 = p.steps[0].solve(1, p, st, opts=fx.solve_opts(amg_persistent_max_dof=-1))
+    s32 = p.steps[0].solve(1, p, st, opts=fx.solve_opts(amg_fp16_smoother=-1, amg_persistent_max_dof=-1))
     assert err <= TOL_MIXED, (err, s16)
     assert s16["pcg_iterations"] <= 1.25 * s32["pcg_iterations"] + 4, (s16["pcg_iterations"], s32["pcg_iterations"])

@@ -1,8 +1,9 @@
 """The persistent multigrid-CG launch (one thread-block cluster per system) against
 the multi-launch path and the oracle's FP64 direct solution.
 
-Small systems (up to amg_persistent_max_dof DOF, 100,000 by default) run their
-whole CG in one launch; amg_persistent_max_dof = -1 forces one launch per step.
+Systems up to amg_persistent_max_dof DOF run their whole CG in one launch (by
+default the small systems of a batch, and a lone system only when tiny); the tests
+set the threshold explicitly, and -1 forces one launch per step.
 Both paths implement the same algorithm, so their iteration counts agree to a
 few iterations and both meet the accuracy bounds of the other parity tests
 (1e-8 relative displacement error for the mixed solver, 1e-10 for FP64)."""
@@ -51,7 +52,7 @@ CASES = {
 def test_persistent_matches_multi_launch_and_oracle(ctx, case, prec, tol):
     text = CASES[case]()
     ref = _oracle_run(text)
-    u1, s1 = _solve(ctx, text, precision=prec)                                # persistent (small system)
+    u1, s1 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=100000)  # persistent
     u2, s2 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1)     # one launch per step
     e1 = float(np.linalg.norm(u1 - ref) / np.linalg.norm(ref))
     e2 = float(np.linalg.norm(u2 - ref) / np.linalg.norm(ref))
@@ -66,15 +67,15 @@ def test_persistent_matches_multi_launch_and_oracle(ctx, case, prec, tol):
 
 def test_persistent_solve_is_repeatable(ctx):
     text = CASES["c3d20_3_levels"]()
-    a, _ = _solve(ctx, text)
-    b, _ = _solve(ctx, text)
+    a, _ = _solve(ctx, text, amg_persistent_max_dof=100000)
+    b, _ = _solve(ctx, text, amg_persistent_max_dof=100000)
     assert np.array_equal(a, b)
 
 
 def test_persistent_iteration_cap_and_breakdown(ctx):
     text = decks.c3d4_cantilever(3, 3, 6)
     with pytest.raises(fx.FerrixError) as e:
-        _solve(ctx, text, max_iter=2)
+        _solve(ctx, text, max_iter=2, amg_persistent_max_dof=100000)
     assert e.value.kind == "ConvergenceError"
     # a model without boundary conditions: singular, found by the multigrid setup or the CG
     lines, keep, skip = text.split("\n"), [], False
@@ -87,18 +88,18 @@ def test_persistent_iteration_cap_and_breakdown(ctx):
         skip = False
         keep.append(line)
     with pytest.raises(fx.FerrixError) as e:
-        _solve(ctx, "\n".join(keep))
+        _solve(ctx, "\n".join(keep), amg_persistent_max_dof=100000)
     assert e.value.kind == "NumericalError"
 
 
 @pytest.mark.parametrize("prec", [fx.PREC_MIXED, fx.PREC_FP64])
 def test_fused_coarse_cycle_matches_per_step_launches(ctx, prec):
-    """The multi-launch path's coarse V-cycle part as one cooperative launch (default)
-    and as one launch per coarse-level step compute every row the same way: the
+    """The multi-launch path's coarse V-cycle part as one cooperative launch and as one
+    launch per coarse-level step (default) compute every row the same way: the
     displacements agree bit for bit, and both match the oracle."""
     text = CASES["c3d20_3_levels"]()
-    u1, s1 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1)
-    u2, s2 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1, amg_coarse_launches=1)
+    u1, s1 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1, amg_fused_coarse=1)
+    u2, s2 = _solve(ctx, text, precision=prec, amg_persistent_max_dof=-1)
     assert s1["amg_levels"] >= 3
     assert np.array_equal(u1, u2) and s1["pcg_iterations"] == s2["pcg_iterations"]
     ref = _oracle_run(text)
