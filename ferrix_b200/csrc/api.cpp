@@ -184,6 +184,8 @@ int fx_ctx_create(int device, fx_ctx** out) {
 
 void fx_ctx_destroy(fx_ctx* ctx) {
     if (!ctx) return;
+    for (fx_ctx* w : ctx->workers) fx_ctx_destroy(w);
+    ctx->workers.clear();
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaStream_t s = ctx->stream;

@@ -764,8 +764,9 @@ int step_solve(fx_model* m, int k, const fx_solve_opts& o, fx_step_stats* st) {
     return FX_OK;
 }
 
-int batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts& o, int* status_out,
-                fx_step_stats* stats) {
+// The batch on one context: every model's step advanced in lockstep rounds on its stream.
+static int batch_solve_on(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts& o, int* status_out,
+                          fx_step_stats* stats) {
     int64_t* saved = g_launch_counter;
     g_launch_counter = &ctx->launches;
     struct Restore {
@@ -809,6 +810,86 @@ int batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts
         if (st != FX_OK && rc == FX_OK) rc = st;
     }
     if (rc != FX_OK) ctx->last_error = first_msg;
+    return rc;
+}
+
+// A batch of several models is spread over kBatchWorkers worker contexts of the
+// caller's context (own streams and host threads; balanced by DOF, largest first):
+// each worker runs its models' rounds (assembly, multigrid setup with its host
+// round trips, one persistent launch for its small systems) while the others do
+// theirs. The persistent-solve threshold is decided for the whole batch, so a model
+// takes the same path whichever worker it lands on.
+constexpr int kBatchWorkers = 4;
+
+int batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts& o_in, int* status_out,
+                fx_step_stats* stats) {
+    fx_solve_opts o = o_in;
+    if (n > 1 && o.amg_persistent_max_dof == 0) o.amg_persistent_max_dof = (int)kClDefaultMaxDof;
+    const int K = std::min(kBatchWorkers, n);
+    if (K <= 1) return batch_solve_on(ctx, models, n, o, status_out, stats);
+    for (int i = 0; i < n; ++i)
+        if (!models[i] || models[i]->ctx != ctx) {
+            ctx->last_error = "model not bound to this context";
+            return FX_INVALID_ARGUMENT;
+        }
+    while ((int)ctx->workers.size() < K) {
+        fx_ctx* w = nullptr;
+        const int rc = fx_ctx_create(ctx->device, &w);
+        if (rc != FX_OK) fail(rc, "batch worker context creation failed");
+        ctx->workers.push_back(w);
+    }
+    FX_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));  // the models' uploads on this stream are done
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        ensure_dense(models[a]);
+        ensure_dense(models[b]);
+        return models[a]->dense.n_nodes > models[b]->dense.n_nodes;
+    });
+    std::vector<std::vector<int>> part(K);
+    std::vector<int64_t> load(K, 0);
+    for (int i : order) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        part[k].push_back(i);
+        load[k] += models[i]->dense.n_nodes;
+    }
+    std::vector<int> rcs(K, FX_OK);
+    std::vector<std::string> errs(K);
+    std::vector<int64_t> launches0(K);
+    std::vector<std::thread> threads;
+    for (int k = 0; k < K; ++k) {
+        threads.emplace_back([&, k] {
+            fx_ctx* w = ctx->workers[k];
+            launches0[k] = w->launches;
+            cudaSetDevice(w->device);
+            std::vector<fx_model*> ms;
+            for (int i : part[k]) {
+                models[i]->ctx = w;
+                ms.push_back(models[i]);
+            }
+            std::vector<int> st(ms.size(), FX_OK);
+            std::vector<fx_step_stats> ss(ms.size());
+            rcs[k] = guarded(w, [&] {
+                return batch_solve_on(w, ms.data(), (int)ms.size(), o, st.data(), ss.data());
+            });
+            if (rcs[k] != FX_OK) errs[k] = w->last_error;
+            cudaStreamSynchronize(w->stream);
+            for (size_t j = 0; j < ms.size(); ++j) {
+                ms[j]->ctx = ctx;
+                if (status_out) status_out[part[k][j]] = st[j];
+                if (stats) stats[part[k][j]] = ss[j];
+            }
+        });
+    }
+    for (auto& t : threads) t.join();
+    int rc = FX_OK;
+    for (int k = 0; k < K; ++k) {
+        ctx->launches += ctx->workers[k]->launches - launches0[k];
+        if (rc == FX_OK && rcs[k] != FX_OK) {
+            rc = rcs[k];
+            ctx->last_error = errs[k];
+        }
+    }
     return rc;
 }
 

@@ -5,6 +5,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "kernels.hpp"
 #include "model.hpp"
@@ -23,6 +24,9 @@ struct fx_ctx {
     fx::PcgBatch<float> pcg32;
     fx::PcgBatch<double> pcg64;
     fx::CsrPcg pcgcsr;
+    // fx_batch_solve's worker contexts on the same device (own streams; created at the first
+    // batch, destroyed with this context, after its models)
+    std::vector<fx_ctx*> workers;
 };
 
 namespace fx {
