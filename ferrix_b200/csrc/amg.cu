@@ -9,6 +9,7 @@
 #include <cuda_fp16.h>
 
 #include "amg.hpp"
+#include "coarse_row.cuh"
 
 namespace fx {
 
@@ -1092,16 +1093,7 @@ __global__ void __launch_bounds__(256) k_ln_op(LnOp o) {
     // 30 lanes walk (block, block row) items: lane l always handles block row l % 6
     // of blocks l / 6 + 5 m, so consecutive lanes read consecutive 48-B block rows
     const int b0 = o.row_ptr[row], items = 6 * (o.row_ptr[row + 1] - b0);
-    double t = 0.0;
-    if (lane < 30)
-        for (int it = lane; it < items; it += 30) {
-            const int kb = it / 6;
-            const int64_t blk = b0 + kb;
-            const double2* vr = reinterpret_cast<const double2*>(o.vals + blk * 36 + (it - 6 * kb) * 6);
-            const double* xx = o.v + 6 * (int64_t)o.cols[blk];
-            const double2 a0 = vr[0], a1 = vr[1], a2 = vr[2];
-            t += a0.x * xx[0] + a0.y * xx[1] + a1.x * xx[2] + a1.y * xx[3] + a2.x * xx[4] + a2.y * xx[5];
-        }
+    double t = coarse_row_part<false>(o.cols, o.vals, o.v, b0, items, lane);
     // lanes r, r+6, ..., r+24 hold block-row r partial sums: fixed-order tree into lanes 0..5
     // (a source lane past 31 returns the caller's own value, hence the lane conditions)
     double u = __shfl_down_sync(0xffffffffu, t, 24);

@@ -23,6 +23,7 @@
 #include <cmath>
 
 #include "amg.hpp"
+#include "coarse_row.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -233,17 +234,7 @@ __device__ __noinline__ void ln_op(const ClLevel& L, Vg g, const double* v, cons
             }
         }
         const int b0 = __ldg(L.row_ptr + row), items = 6 * (__ldg(L.row_ptr + row + 1) - b0);
-        double t = 0.0;
-        if (lane < 30)
-            for (int it = lane; it < items; it += 30) {
-                const int kb = it / 6;
-                const int64_t blk = b0 + kb;
-                const double2* vr = reinterpret_cast<const double2*>(L.vals + blk * 36 + (it - 6 * kb) * 6);
-                const double* xx = v + 6 * (int64_t)__ldg(L.cols + blk);
-                const double2 a0 = __ldg(vr), a1 = __ldg(vr + 1), a2 = __ldg(vr + 2);
-                t += a0.x * ldv(xx) + a0.y * ldv(xx + 1) + a1.x * ldv(xx + 2) + a1.y * ldv(xx + 3) +
-                     a2.x * ldv(xx + 4) + a2.y * ldv(xx + 5);
-            }
+        double t = coarse_row_part<true>(L.cols, L.vals, v, b0, items, lane);
         double u = __shfl_down_sync(0xffffffffu, t, 24);
         if (lane < 8) t += u;
         u = __shfl_down_sync(0xffffffffu, t, 12);

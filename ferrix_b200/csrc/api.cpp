@@ -37,8 +37,11 @@ static double profile_t(fx_model* m, int reps, double* bytes) {
     sys.x = d.du.ptr;
     PcgBatch<T> batch;
     double ms = batch.profile_spmv(sys, reps, s);
+    // compulsory bytes of one k_pcg_spmv launch: every block's 9 values and column id, the
+    // row offsets, the direction p read once (3 components per node; the fourth, padding
+    // lane of its node-aligned layout excluded) and q written once
     const double nb = (double)d.S.n_blocks, n3 = 3.0 * (double)nn;
-    *bytes = nb * (9.0 * sizeof(T) + 4.0) + 4.0 * (nn + 1) + 4.0 * sizeof(T) * n3;
+    *bytes = nb * (9.0 * sizeof(T) + 4.0) + 4.0 * (nn + 1) + 2.0 * sizeof(T) * n3;
     return ms;
 }
 
