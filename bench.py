@@ -160,9 +160,10 @@ def _batch_figure(ctx, stream):
     """64 C3D4 box decks of the batched workload's population (DOF log-uniform [2k, 60k],
     E log-uniform, random load), built from arrays (fx_model_from_arrays, no text) and
     solved by one fx_batch_solve with the default options: each deck's first step
-    (pattern, assembly, multigrid setup, CG to 1e-8, Newton re-check); the small
-    systems' CG iterations all run in one persistent launch. Device time, mean of two
-    timed batches after one untimed."""
+    (pattern, assembly, multigrid setup, CG to 1e-8, Newton re-check), the decks spread
+    over the context's four worker streams. Device time, mean of two timed batches after
+    one untimed. Beside it, the same 64 decks submitted at once to the request loop
+    (fx_server, 4 slots): its span from the first submission to the last completion."""
     import numpy as np
     import torch
     import ferrix_b200 as fx
@@ -192,11 +193,16 @@ def _batch_figure(ctx, stream):
         for p in ps:
             p.close()
     ms = float(np.mean(times))
+    from ferrix_b200 import serving
+    loop = serving.run_stream([kw for kw, _ in pop], 1e6, BATCH_DECKS, opts, device=torch.cuda.current_device(),
+                              slots=4, seed=1, each_once=True)
     return {"decks": BATCH_DECKS, "total_dofs": int(sum(d for _, d in pop)), "device_ms": ms,
             "solves_per_s": BATCH_DECKS / (ms * 1e-3), "failed": int(np.sum(status != 0)),
             "pcg_iterations_max": int(max(s["pcg_iterations"] for s in stats)),
-            "solver": "default (mixed multigrid CG; systems up to 100k DOF in one persistent cluster launch)",
-            "input": "fx_model_from_arrays"}, first
+            "solver": "default (mixed multigrid CG, multi-launch per system; four worker streams)",
+            "input": "fx_model_from_arrays",
+            "request_loop_same_decks": {"slots": 4, "completed": loop["completed"], "span_s": loop["span_s"],
+                                        "solves_per_s": loop["completed"] / loop["span_s"]}}, first
 
 
 def _batch_oracle_errors(first):

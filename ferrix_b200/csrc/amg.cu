@@ -842,6 +842,16 @@ __device__ __forceinline__ void cta_dot_finalize(double v, double v2, int mode, 
 #define FX_L0_MIN_BLOCKS 2
 #endif
 constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per SM (2: at most 128 registers)
+// FP16 values: 3 CTAs per SM (at most 85 registers). Its loads are half as wide, so it
+// needs more warps in flight (54.5 against 57.7 us per Chebyshev step on the 417k-DOF
+// C3D20 box); the FP32 / FP64 forms spill and slow down at that budget.
+#ifndef FX_L0_LATE_EPI_H
+#define FX_L0_LATE_EPI_H 0
+#endif
+#ifndef FX_L0_MIN_BLOCKS_H
+#define FX_L0_MIN_BLOCKS_H 3
+#endif
+constexpr int kL0MinBlocksH = FX_L0_MIN_BLOCKS_H;
 
 #ifndef FX_L0_LANES
 #define FX_L0_LANES 8
@@ -858,10 +868,14 @@ constexpr int kL0Unroll = FX_L0_UNROLL;  // groups of a row in flight per lane
 // o.d4_out; the row's own FP64 values still come from o.v where the mode needs
 // them (Cheb0: the iterate), else from o.v4.
 template <typename VT, int MODE, bool G32 = false>
-__global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
+__global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinBlocksH : kL0MinBlocks)
+    k_l0_op(L0Op<VT> o) {
     // FP16 values (of the scaled matrix): FP32 gathers of the scaled vectors, row sums
     // scaled back by sqrt(a_ii), directions written scaled
     constexpr bool H = std::is_same<VT, __half>::value;
+    // FP16 values: the row-local epilogue operands are loaded after the gathers
+    // (FX_L0_LATE_EPI_H), which frees their registers during the gather loop
+    constexpr bool kL0LateEpi = H && FX_L0_LATE_EPI_H;
     const int sub = threadIdx.x & (kL0Lanes - 1);
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> kL0LaneShift;
     const int rows_per_grid = (gridDim.x * blockDim.x) >> kL0LaneShift;
@@ -880,6 +894,7 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
         const bool epi = valid && sub < 3;
         double src3[3] = {0.0, 0.0, 0.0}, Dr[3] = {0.0, 0.0, 0.0}, vc = 0.0, xoc = 0.0, bc = 0.0, zoc = 0.0;
         float4 sqi = make_float4(1.f, 1.f, 1.f, 0.f);
+        auto load_epi = [&]() {
         if (H && epi) sqi = __ldg(o.sq4 + row);
         if (epi) {
             if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
@@ -907,6 +922,8 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
                 src3[0] = o.r[o3 + c];
             }
         }
+        };
+        if (!kL0LateEpi) load_epi();
         double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll kL0Unroll
         for (int g = sub; g < ng; g += kL0Lanes) {
@@ -950,6 +967,7 @@ __global__ void __launch_bounds__(256, kL0MinBlocks) k_l0_op(L0Op<VT> o) {
         for (int s = kL0Lanes / 2; s > 0; s >>= 1)
 #pragma unroll
             for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], s);
+        if (kL0LateEpi) load_epi();
         // epilogue: lane c of the row's 8 handles component c
         if (H) {  // (A v)_i = sqrt(a_ii) (S A S (sqrt(a_jj) v_j))_i
             acc[0] *= (double)sqi.x;
@@ -1308,19 +1326,23 @@ __global__ void k_f64_to_f32(int64_t n, const double* __restrict__ a, float* __r
 
 // ------------------------------------------------------------------ host side
 
-// Grid of the level-0 operators: at most one wave of resident CTAs (grid-stride rows).
-static unsigned l0_grid(int n) {
-    thread_local int cached_dev = -1, cached_cap = 0;  // per host thread: contexts live on one thread each
+// Grid of the level-0 operators: at most one wave of resident CTAs (grid-stride rows);
+// h: the FP16-value kernels, which have their own register budget.
+static unsigned l0_grid(int n, bool h = false) {
+    thread_local int cached_dev = -1, cached_cap[2] = {0, 0};  // per host thread: contexts live on one thread each
     int dev = 0;
     FX_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev != cached_dev) {
-        int sms = 0, per_sm = 0;
+        int sms = 0, per_sm = 0, per_sm_h = 0;
         FX_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_l0_op<double, kL0ChebK>, 256, 0));
-        cached_cap = std::max(1, sms * std::max(1, per_sm));
+        FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_h, k_l0_op<__half, kL0ChebK, true>, 256,
+                                                                    0));
+        cached_cap[0] = std::max(1, sms * std::max(1, per_sm));
+        cached_cap[1] = std::max(1, sms * std::max(1, per_sm_h));
         cached_dev = dev;
     }
-    return (unsigned)std::min<int64_t>(grid_for((int64_t)n * kL0Lanes), cached_cap);
+    return (unsigned)std::min<int64_t>(grid_for((int64_t)n * kL0Lanes), cached_cap[h ? 1 : 0]);
 }
 
 template <typename VT>
@@ -1795,7 +1817,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     AmgLevel& c = L[1];
     const int64_t nd = (int64_t)l.n * 3;
     const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
-    const unsigned grid = l0_grid(l.n);
+    const unsigned grid = l0_grid(l.n, std::is_same<VT, __half>::value);
     // FP32 or FP16 values: the smoother's gathered vectors are FP32 (float4 per node)
     constexpr bool g32 = !std::is_same<VT, double>::value;
     double* dA = l.d.ptr;
@@ -1935,7 +1957,7 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
     l.S0 = &S;
     l.vals0 = vals64;
     l.dinv0 = dinv64;
-    const unsigned grid = l0_grid(n);
+    const unsigned grid = l0_grid(n, fp16);
     auto launch = [&]() {
         if (fp16) {
             L0Op<__half> o = l0_op<__half>(l, v16.ptr);

@@ -227,13 +227,12 @@ void launch_amg_cluster(const ClInst* insts, ClResult* res, int n, bool fp32, do
 // as one cooperative launch over all SMs; *flag = 1 when a barrier wait ran out.
 void launch_coarse_grid(const ClInst* inst, GridBarState* st, double* flag, bool fp32, int degree, double alpha,
                         cudaStream_t s);
-// Systems of at most this many DOF are solved by the persistent launch by default: in a
-// batch of several systems (measured on B200: 64 C3D4 decks of 2k-60k DOF in 275 ms against
-// 378 ms one system after another), and alone only when tiny (alone, a cluster is slower
-// than the multi-launch path from about 3,600 DOF on: 3.9 ms against 3.3 ms there, 17 ms
-// against 7 ms at 15k DOF).
-constexpr int64_t kClDefaultMaxDof = 100000;
-constexpr int64_t kClSingleMaxDof = 2000;
+// Systems of at most this many DOF are solved by the persistent launch by default, alone
+// or in a batch. Alone, a cluster is slower than the multi-launch path from about 3,600 DOF
+// on (3.9 ms against 3.3 ms there, 17 ms against 7 ms at 15k DOF); in a batch of 64 C3D4
+// decks of 2k-60k DOF spread over four worker streams, one persistent launch per worker
+// took 243-324 ms against 183 ms for the multi-launch path on every stream (B200).
+constexpr int64_t kClDefaultMaxDof = 2000;
 
 // CG on the FP64 BSR3 system preconditioned by one V-cycle per iteration.
 // CUDA-event time (ms per launch) of the fused fine-level Chebyshev step (SpMV +

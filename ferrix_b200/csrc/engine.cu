@@ -610,11 +610,10 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
         po.amg_cheb_ratio = rs[0]->o.amg_cheb_ratio > 1.0 ? rs[0]->o.amg_cheb_ratio : kAmgChebRatio;
         po.amg_fused_coarse = rs[0]->o.amg_fused_coarse == 1;
         po.amg_fp16 = rs[0]->o.amg_fp16_smoother >= 0;
-        // persistent cluster solve: for every small system of a round that solves several (one
-        // launch advances them all), for a lone system only when it is tiny (a cluster's few
-        // SMs are latency-bound where the multi-launch path uses the whole GPU)
+        // persistent cluster solve for tiny systems (a cluster's few SMs are latency-bound
+        // where the multi-launch path uses the whole GPU); all of a round's in one launch
         const int pm = rs[0]->o.amg_persistent_max_dof;
-        po.amg_persistent_max_dof = pm != 0 ? pm : (rs.size() > 1 ? kClDefaultMaxDof : kClSingleMaxDof);
+        po.amg_persistent_max_dof = pm != 0 ? pm : kClDefaultMaxDof;
     }
     while (true) {
         bool any = false;
@@ -815,16 +814,18 @@ static int batch_solve_on(fx_ctx* ctx, fx_model* const* models, int n, const fx_
 
 // A batch of several models is spread over kBatchWorkers worker contexts of the
 // caller's context (own streams and host threads; balanced by DOF, largest first):
-// each worker runs its models' rounds (assembly, multigrid setup with its host
-// round trips, one persistent launch for its small systems) while the others do
-// theirs. The persistent-solve threshold is decided for the whole batch, so a model
-// takes the same path whichever worker it lands on.
-constexpr int kBatchWorkers = 4;
+// each worker runs its models' rounds (assembly, multigrid setup with its host round
+// trips, the multi-launch CG of each system, one persistent launch for its tiny ones)
+// while the others do theirs, so the kernels of up to kBatchWorkers systems share the
+// GPU. A model takes the same path whichever worker it lands on.
+#ifndef FX_BATCH_WORKERS
+#define FX_BATCH_WORKERS 4
+#endif
+constexpr int kBatchWorkers = FX_BATCH_WORKERS;
 
 int batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts& o_in, int* status_out,
                 fx_step_stats* stats) {
-    fx_solve_opts o = o_in;
-    if (n > 1 && o.amg_persistent_max_dof == 0) o.amg_persistent_max_dof = (int)kClDefaultMaxDof;
+    const fx_solve_opts& o = o_in;
     const int K = std::min(kBatchWorkers, n);
     if (K <= 1) return batch_solve_on(ctx, models, n, o, status_out, stats);
     for (int i = 0; i < n; ++i)

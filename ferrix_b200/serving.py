@@ -44,14 +44,22 @@ def _host_model(entry) -> Project:
 
 
 def run_stream(pool: List[str], rate: float, n_requests: int, opts, device: int = 0, slots: int = 4,
-               seed: int = 0, hbm_budget_bytes: float = 0.0, keep: Optional[List[int]] = None) -> Dict:
+               seed: int = 0, hbm_budget_bytes: float = 0.0, keep: Optional[List[int]] = None,
+               each_once: bool = False) -> Dict:
     """Submits n_requests at Poisson arrival times (rate per second) and waits for all.
 
-    Returns latency percentiles (ms), throughput (solves/s, first submission to
-    last completion) and per-request records; `keep` lists pool indices whose
+    The decks are drawn from `pool` at random (with replacement), or with each_once
+    every deck of the pool once in a random order (n_requests = len(pool)). Returns
+    latency percentiles (ms), throughput (solves/s, first submission to last
+    completion) and per-request records; `keep` lists pool indices whose
     displacements are returned (for accuracy checks)."""
     rng = np.random.default_rng(seed)
-    order = rng.integers(0, len(pool), size=n_requests)
+    if each_once:
+        if n_requests != len(pool):
+            raise ValueError("each_once needs n_requests == len(pool)")
+        order = rng.permutation(len(pool))
+    else:
+        order = rng.integers(0, len(pool), size=n_requests)
     gaps = rng.exponential(1.0 / rate, size=n_requests)
     arrivals = np.cumsum(gaps) - gaps[0]
     models = [_host_model(pool[i]) for i in order]

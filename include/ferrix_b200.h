@@ -96,9 +96,8 @@ typedef struct {
     double amg_cheb_ratio;   /* FX_PRECOND_AMG: lmax / lmin of the first-kind Chebyshev interval; 0 = 12 */
     int amg_persistent_max_dof; /* FX_PRECOND_AMG, V-cycle: systems of at most this many DOF run their
                                    whole CG in one persistent launch, one thread-block cluster per system
-                                   (all such systems of a round in the same launch); 0 = default: 100,000
-                                   when several systems are solved together (fx_batch_solve), 2,000 for a
-                                   system solved alone; < 0 = never (one launch per CG step and phase) */
+                                   (all such systems of a round in the same launch); 0 = default (2,000);
+                                   < 0 = never (one launch per CG step and phase) */
     int amg_fused_coarse;       /* FX_PRECOND_AMG, V-cycle, systems on the multi-launch path: 1 = the coarse
                                    part of each V-cycle (restriction, coarse levels, dense coarsest solve,
                                    prolongation) as one cooperative launch over all SMs; 0 = one launch

@@ -2,6 +2,7 @@
 
     python tests/golden/make_fixtures.py decks <path-to-ferrix-checkout>
     python tests/golden/make_fixtures.py box
+    python tests/golden/make_fixtures.py beam
 
 `decks` (needs a FerriX checkout, passed explicitly) writes
   decks/<name>.inp.gz   gzip copies of the reference's four test decks
@@ -19,6 +20,15 @@
                         .c3d20_box() with its default seed), plus the deck's
                         SHA-256 so a test can tell when the generator changed.
                         One oracle run: about 70 s on 16 cores, ~10 GB of RAM.
+
+`beam` (no checkout needed) writes
+  oracle_c3d4_nlgeom_beam.npz  the oracle's FP64 Cholesky Newton run of the full
+                        NLGEOM beam the benchmark times (ferrix_b200.decks
+                        .c3d4_nlgeom_beam() with its defaults: 240,000 C3D4,
+                        133,623 DOF, E(T), initial temperature gradient, amplitude
+                        ramp over 10 increments; default initial temperature 20.0):
+                        displacements after the step, increments and Newton
+                        iterations, and the deck's SHA-256. About an hour on 8 cores.
 """
 from __future__ import annotations
 
@@ -49,6 +59,7 @@ CALCULIX = {
 }
 
 BOX_FIXTURE = "oracle_c3d20_box.npz"
+BEAM_FIXTURE = "oracle_c3d4_nlgeom_beam.npz"
 
 
 def make_decks(ref: str) -> None:
@@ -92,10 +103,30 @@ def make_box() -> None:
     print(BOX_FIXTURE, "dof", len(u), f"{time.perf_counter() - t0:.1f} s")
 
 
+def beam_deck() -> str:
+    from ferrix_b200 import decks
+    return decks.c3d4_nlgeom_beam()
+
+
+def make_beam() -> None:
+    text = beam_deck()
+    t0 = time.perf_counter()
+    p = inp.parse_inp_text(text)
+    p.default_initial_temperature = 20.0
+    r = static_step.Runner(p)
+    u = r.run().displacements
+    np.savez_compressed(os.path.join(HERE, BEAM_FIXTURE), u=u, deck_sha256=np.array(deck_digest(text)),
+                        increments=np.array(len(r.log)),
+                        residual_checks=np.array([len(rec.residuals) for rec in r.log]))
+    print(BEAM_FIXTURE, "dof", len(u), "increments", len(r.log), f"{time.perf_counter() - t0:.1f} s")
+
+
 if __name__ == "__main__":
     if len(sys.argv) == 3 and sys.argv[1] == "decks":
         make_decks(sys.argv[2])
     elif len(sys.argv) == 2 and sys.argv[1] == "box":
         make_box()
+    elif len(sys.argv) == 2 and sys.argv[1] == "beam":
+        make_beam()
     else:
         sys.exit(__doc__)

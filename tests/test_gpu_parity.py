@@ -183,8 +183,8 @@ def test_nlgeom_thermal_beam(ctx):
 def test_batch_matches_single(ctx, pc):
     """A system's arithmetic does not depend on the others in its batch: alone and batched on
     the same path (multigrid: the persistent cluster launch, threshold set for both) it gives
-    the same bits. (With the default options a lone multigrid system above 2,000 DOF takes the
-    multi-launch path instead; test_batch_default_options checks that case to the tolerance.)"""
+    the same bits. (With the default options a multigrid system above 2,000 DOF takes the
+    multi-launch path alone and batched; test_batch_default_options checks that case.)"""
     pop = decks.batch_population(6, seed=11, dof_lo=500, dof_hi=6000, c3d20_fraction=0.3)
     o = fx.solve_opts(preconditioner=pc, precision=fx.PREC_MIXED,
                       amg_persistent_max_dof=100000 if pc == fx.PRECOND_AMG else 0)
@@ -207,8 +207,9 @@ def test_batch_matches_single(ctx, pc):
 
 
 def test_batch_default_options(ctx):
-    """Default options: the batch's multigrid systems share one persistent launch, each system
-    alone takes the multi-launch path; both meet the mixed bound against the oracle."""
+    """Default options: the batch's multigrid systems (3k-20k DOF) take the multi-launch path on
+    the context's worker streams, as each does alone, so batched and alone give the same bits;
+    both meet the mixed bound against the oracle."""
     pop = decks.batch_population(4, seed=13, dof_lo=3000, dof_hi=20000, c3d20_fraction=0.5)
     projs = [_project(ctx, text)[0] for text, _ in pop]
     status, stats = fx.batch_solve(ctx, projs, fx.solve_opts())
@@ -219,6 +220,7 @@ def test_batch_default_options(ctx):
         ub = st.displacements
         q, sq = _project(ctx, text)
         q.steps[0].solve(1, q, sq)
+        assert np.array_equal(ub, sq.displacements)
         ref, _ = _oracle_run(text)
         for u in (ub, sq.displacements):
             err = _err(u, ref)
