@@ -776,6 +776,16 @@ __device__ __forceinline__ void ld4v(const __half* p, float o[4]) {
     o[2] = b.x;
     o[3] = b.y;
 }
+__device__ __forceinline__ void unpack_h4(uint2 v, float o[4]) {
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = b.x;
+    o[3] = b.y;
+}
+template <typename T>
+__device__ __forceinline__ void unpack_h4(uint2, T*) {}
 __device__ __forceinline__ void ld4v(const double* p, double o[4]) {
     const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
     const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
@@ -842,14 +852,21 @@ __device__ __forceinline__ void cta_dot_finalize(double v, double v2, int mode, 
 #define FX_L0_MIN_BLOCKS 2
 #endif
 constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per SM (2: at most 128 registers)
-// FP16 values: 3 CTAs per SM (at most 85 registers). Its loads are half as wide, so it
-// needs more warps in flight (54.5 against 57.7 us per Chebyshev step on the 417k-DOF
-// C3D20 box); the FP32 / FP64 forms spill and slow down at that budget.
+// FP16 values: its loads are half as wide as the FP32 form's, so it is latency-bound and
+// needs more warps and more loads in flight. Measured per Chebyshev step on the 417k-DOF
+// C3D20 box (B200): 57.7 us at 2 CTAs per SM; 54.8 at 3 (85 registers); 61.5 at 4 with
+// spills; 50.5 at 4 with the row's epilogue operands loaded after the gathers (no spills
+// at 64 registers); 48.1 with, in addition, each group's nine plane loads issued before
+// its column ids (FX_L0_VFIRST_H). The FP32 / FP64 forms spill and slow down at those
+// budgets, so they keep 2 CTAs per SM.
+#ifndef FX_L0_VFIRST_H
+#define FX_L0_VFIRST_H 1
+#endif
 #ifndef FX_L0_LATE_EPI_H
-#define FX_L0_LATE_EPI_H 0
+#define FX_L0_LATE_EPI_H 1
 #endif
 #ifndef FX_L0_MIN_BLOCKS_H
-#define FX_L0_MIN_BLOCKS_H 3
+#define FX_L0_MIN_BLOCKS_H 4
 #endif
 constexpr int kL0MinBlocksH = FX_L0_MIN_BLOCKS_H;
 
@@ -876,6 +893,7 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
     // FP16 values: the row-local epilogue operands are loaded after the gathers
     // (FX_L0_LATE_EPI_H), which frees their registers during the gather loop
     constexpr bool kL0LateEpi = H && FX_L0_LATE_EPI_H;
+    constexpr bool kL0VFirst = H && FX_L0_VFIRST_H;
     const int sub = threadIdx.x & (kL0Lanes - 1);
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> kL0LaneShift;
     const int rows_per_grid = (gridDim.x * blockDim.x) >> kL0LaneShift;
@@ -927,6 +945,15 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
         double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll kL0Unroll
         for (int g = sub; g < ng; g += kL0Lanes) {
+            // FP16 values (kL0VFirst): the group's nine 8-byte plane loads are issued before
+            // the column ids and the gathers that depend on them
+            uint2 raw[kL0VFirst ? 9 : 1];
+            if constexpr (kL0VFirst) {
+                const __half* vh = reinterpret_cast<const __half*>(o.vals) + ((int64_t)g0 * 9 + g) * 4;
+#pragma unroll
+                for (int k = 0; k < 9; ++k)
+                    raw[k] = __ldcs(reinterpret_cast<const uint2*>(vh + (int64_t)k * ng * 4));
+            }
             const int4 cc = __ldg(reinterpret_cast<const int4*>(o.cols) + g0 + g);
             const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
             // FP32 values with FP32 gathered vectors: the group's 4 blocks are summed in
@@ -953,9 +980,15 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
             for (int r = 0; r < 3; ++r) {
                 using MT = typename std::conditional<H, float, VT>::type;
                 MT m0[4], m1[4], m2[4];
-                ld4v(vb + (3 * r) * pl, m0);
-                ld4v(vb + (3 * r + 1) * pl, m1);
-                ld4v(vb + (3 * r + 2) * pl, m2);
+                if constexpr (kL0VFirst) {
+                    unpack_h4(raw[3 * r], m0);
+                    unpack_h4(raw[3 * r + 1], m1);
+                    unpack_h4(raw[3 * r + 2], m2);
+                } else {
+                    ld4v(vb + (3 * r) * pl, m0);
+                    ld4v(vb + (3 * r + 1) * pl, m1);
+                    ld4v(vb + (3 * r + 2) * pl, m2);
+                }
                 GT t = 0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
@@ -1069,6 +1102,14 @@ __global__ void __launch_bounds__(1024) k_kcycle2(int64_t n, const double* __res
 // ---- coarse levels (row-major 6x6 block CSR): SpMV fused with the smoother
 // update, one warp per block row, lanes over the row's blocks; the same modes as
 // the fine-level operator (kL0Resid, kL0RUpd, kL0Cheb0, kL0ChebK).
+// Column-gather chains in flight per lane of the coarse-level operators (2: 64 registers;
+// on the 417k-DOF box a default solve took 54.6-55.0 ms against 55.0-55.7 with 4 and
+// 55.5-55.9 with 1).
+#ifndef FX_LN_IN_FLIGHT
+#define FX_LN_IN_FLIGHT 2
+#endif
+constexpr int kLnInFlight = FX_LN_IN_FLIGHT;
+
 struct LnOp {
     int n;
     const int32_t* row_ptr;
@@ -1111,7 +1152,7 @@ __global__ void __launch_bounds__(256) k_ln_op(LnOp o) {
     // 30 lanes walk (block, block row) items: lane l always handles block row l % 6
     // of blocks l / 6 + 5 m, so consecutive lanes read consecutive 48-B block rows
     const int b0 = o.row_ptr[row], items = 6 * (o.row_ptr[row + 1] - b0);
-    double t = coarse_row_part<false>(o.cols, o.vals, o.v, b0, items, lane);
+    double t = coarse_row_part<false, kLnInFlight>(o.cols, o.vals, o.v, b0, items, lane);
     // lanes r, r+6, ..., r+24 hold block-row r partial sums: fixed-order tree into lanes 0..5
     // (a source lane past 31 returns the caller's own value, hence the lane conditions)
     double u = __shfl_down_sync(0xffffffffu, t, 24);
@@ -1344,6 +1385,10 @@ static unsigned l0_grid(int n, bool h = false) {
     }
     return (unsigned)std::min<int64_t>(grid_for((int64_t)n * kL0Lanes), cached_cap[h ? 1 : 0]);
 }
+
+// Slots of the partial-sum buffer a level-0 operator with a dot product needs: two per CTA
+// of the largest level-0 grid (the FP16 kernels run more CTAs per SM than the others).
+static int64_t l0_part_slots(int n) { return 2 * (int64_t)std::max(l0_grid(n, false), l0_grid(n, true)); }
 
 template <typename VT>
 static L0Op<VT> l0_op(const AmgLevel& l, const VT* vals) {
@@ -2107,8 +2152,7 @@ void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* 
     p_.alloc(nd, s);
     q_.alloc(nd, s);
     const int nb = 296;
-    const unsigned g0 = l0_grid(n);
-    part_.alloc(std::max<int64_t>(nb, 2 * (int64_t)g0), s);
+    part_.alloc(std::max<int64_t>(nb, l0_part_slots(n)), s);
     sc_.alloc(8, s);
     sc_.zero(s);
     counter_.alloc(1, s);

@@ -234,7 +234,7 @@ __device__ __noinline__ void ln_op(const ClLevel& L, Vg g, const double* v, cons
             }
         }
         const int b0 = __ldg(L.row_ptr + row), items = 6 * (__ldg(L.row_ptr + row + 1) - b0);
-        double t = coarse_row_part<true>(L.cols, L.vals, v, b0, items, lane);
+        double t = coarse_row_part<true, 4>(L.cols, L.vals, v, b0, items, lane);
         double u = __shfl_down_sync(0xffffffffu, t, 24);
         if (lane < 8) t += u;
         u = __shfl_down_sync(0xffffffffu, t, 12);
