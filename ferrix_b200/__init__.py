@@ -147,6 +147,40 @@ class SolverTime:
     """Marker mirroring src/solver/time.rs; the running time lives in the model."""
 
 
+@dataclass
+class IncResult:
+    """A converged increment as Step.solve hands it to a writer's write_increment
+    (IncResult, src/solver/results.rs; handed over at src/solver/step/static_step.rs:219-248):
+    1-based step id, the step's increment counter (failed attempts included) and the global
+    time. While write_increment runs, `project` holds that increment's displacements."""
+    step_id: int
+    inc_id: int
+    time: float
+    project: "Project"
+
+
+class VtkWriter:
+    """VtkWriter (src/solver/io/vtk.rs:19-334) as a Step.solve writer: init() creates
+    `directory` and its results.vtk.series, write_increment() writes the increment's
+    step_<step_id>_<inc_id>.vtk (displacements, temperatures, nodal stress / strain, Mises,
+    Tresca) and its series entry, finish() closes the series."""
+
+    def __init__(self, project: "Project", directory: str):
+        self.project = project
+        self.directory = directory
+
+    def init(self) -> None:
+        _check(_lib.load().fx_vtk_series_init(os.fsencode(self.directory)))
+
+    def write_increment(self, inc: IncResult, timer: Optional[SolverTime] = None) -> None:
+        name = f"step_{inc.step_id}_{inc.inc_id}.vtk"
+        self.project.write_vtk(os.path.join(self.directory, name))
+        _check(_lib.load().fx_vtk_series_add(os.fsencode(self.directory), name.encode(), float(inc.time)))
+
+    def finish(self) -> None:
+        _check(_lib.load().fx_vtk_series_finish(os.fsencode(self.directory)))
+
+
 class _Mesh:
     def __init__(self, project: "Project"):
         self._p = project
@@ -193,10 +227,25 @@ class Step:
             raise ValueError("step_id must be the 1-based position of the step")
         st = StepStats()
         o = opts if opts is not None else solve_opts()
-        _check(project.lib.fx_step_solve(project.handle, self.index, C.byref(o), C.byref(st)), project.ctx)
-        self.last_stats = st.as_dict()
         if writer is not None and hasattr(writer, "write_increment"):
-            writer.write_increment(self.last_stats, timer)
+            # the writer sees every converged increment, as ResultWriter::write_increment does
+            errors = []
+
+            def on_increment(user, model, step, inc, t):
+                try:
+                    writer.write_increment(IncResult(step, inc, t, project), timer)
+                    return 0
+                except Exception as e:  # ends the step (FX_GENERIC_IO); re-raised below
+                    errors.append(e)
+                    return 1
+            cb = _lib.IncrementCallback(on_increment)
+            rc = project.lib.fx_step_solve_cb(project.handle, self.index, C.byref(o), C.byref(st), cb, None)
+            if errors:
+                raise errors[0]
+            _check(rc, project.ctx)
+        else:
+            _check(project.lib.fx_step_solve(project.handle, self.index, C.byref(o), C.byref(st)), project.ctx)
+        self.last_stats = st.as_dict()
         return self.last_stats
 
     def records(self, bcs: bool = False):

@@ -109,6 +109,9 @@ class MeshDesc(C.Structure):
 # name -> (restype, argtypes); every symbol of include/ferrix_b200.h
 P = C.c_void_p
 I64P = C.POINTER(C.c_int64)
+# fx_increment_cb: int (*)(void* user, fx_model* model, int step_id, int inc_id, double global_time)
+IncrementCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double)
+
 SIGNATURES = {
     "fx_default_solve_opts": (None, [C.POINTER(SolveOpts)]),
     "fx_ctx_create": (C.c_int, [C.c_int, C.POINTER(P)]),
@@ -134,6 +137,10 @@ SIGNATURES = {
     "fx_state_get_temperatures": (C.c_int, [P, P, P]),
     "fx_state_set_temperatures": (C.c_int, [P, P, P]),
     "fx_step_solve": (C.c_int, [P, C.c_int, C.POINTER(SolveOpts), C.POINTER(StepStats)]),
+    "fx_step_solve_cb": (C.c_int, [P, C.c_int, C.POINTER(SolveOpts), C.POINTER(StepStats), IncrementCallback, P]),
+    "fx_vtk_series_init": (C.c_int, [C.c_char_p]),
+    "fx_vtk_series_add": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double]),
+    "fx_vtk_series_finish": (C.c_int, [C.c_char_p]),
     "fx_assemble_csr": (C.c_int, [P, P, C.c_int, I64P, P, P, P, C.POINTER(C.c_double)]),
     "fx_internal_force": (C.c_int, [P, P, P, P]),
     "fx_thermal_force": (C.c_int, [P, P]),

@@ -1102,6 +1102,11 @@ __global__ void __launch_bounds__(1024) k_kcycle2(int64_t n, const double* __res
 // ---- coarse levels (row-major 6x6 block CSR): SpMV fused with the smoother
 // update, one warp per block row, lanes over the row's blocks; the same modes as
 // the fine-level operator (kL0Resid, kL0RUpd, kL0Cheb0, kL0ChebK).
+// Threads per CTA of the coarse-level kernels (warp per block row / aggregate).
+#ifndef FX_LN_THREADS
+#define FX_LN_THREADS 128
+#endif
+constexpr int kLnThreads = FX_LN_THREADS;
 // Column-gather chains in flight per lane of the coarse-level operators (2: 64 registers;
 // on the 417k-DOF box a default solve took 54.6-55.0 ms against 55.0-55.7 with 4 and
 // 55.5-55.9 with 1).
@@ -1778,12 +1783,12 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s, bool starte
     AmgLevel& l = L[lev];
     const int64_t nd = (int64_t)l.n * l.bs;
     if (l.coarsest) {
-        FX_LAUNCH(k_dense_matvec, grid_for(nd * 32), 256, 0, s, (int)nd, l.dense_inv.ptr, b, x);
+        FX_LAUNCH(k_dense_matvec, grid_for(nd * 32, kLnThreads), kLnThreads, 0, s, (int)nd, l.dense_inv.ptr, b, x);
         return;
     }
     AmgLevel& c = L[lev + 1];
     const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
-    const unsigned grid = grid_for((int64_t)l.n * 32);
+    const unsigned grid = grid_for((int64_t)l.n * 32, kLnThreads);
     double* dA = l.d.ptr;
     double* dB = l.t.ptr;
     double* xs = l.xs.ptr;
@@ -1797,16 +1802,16 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s, bool starte
         o.xo = xs;
         o.c1 = k.c1[st];
         o.c2 = k.c2[st];
-        FX_LAUNCH(k_ln_op<kL0ChebK>, grid, 256, 0, s, o);
+        FX_LAUNCH(k_ln_op<kL0ChebK>, grid, kLnThreads, 0, s, o);
         std::swap(dA, dB);
     }
     {
         LnOp o = ln_op(l);
         o.v = dA;
         o.r = l.r.ptr;
-        FX_LAUNCH(k_ln_op<kL0RUpd>, grid, 256, 0, s, o);  // r = b - A xs
+        FX_LAUNCH(k_ln_op<kL0RUpd>, grid, kLnThreads, 0, s, o);  // r = b - A xs
     }
-    FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs,
+    FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32, kLnThreads), kLnThreads, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, l.bs,
               l.Q.ptr, l.r.ptr, c.b.ptr, coarse_start(lev + 1));
     coarse(lev + 1, s);
     FX_LAUNCH(k_prolong, grid_for(nd), 256, 0, s, (int)nd, l.bs, l.agg.ptr, l.Q.ptr, c.x.ptr, xs, alpha_);
@@ -1818,7 +1823,7 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s, bool starte
         o.d_out = dA;
         o.xo = x;
         o.c2 = k.c2_start;
-        FX_LAUNCH(k_ln_op<kL0Cheb0>, grid, 256, 0, s, o);
+        FX_LAUNCH(k_ln_op<kL0Cheb0>, grid, kLnThreads, 0, s, o);
     }
     for (int st = 1; st < degree_; ++st) {
         LnOp o = ln_op(l);
@@ -1828,7 +1833,7 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s, bool starte
         o.xo = x;
         o.c1 = k.c1[st];
         o.c2 = k.c2[st];
-        FX_LAUNCH(k_ln_op<kL0ChebK>, grid, 256, 0, s, o);
+        FX_LAUNCH(k_ln_op<kL0ChebK>, grid, kLnThreads, 0, s, o);
         std::swap(dA, dB);
     }
 }
@@ -1902,7 +1907,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     if (fused_coarse_ && !kcycle_ && desc_.ptr) {  // restriction, coarse levels, prolongation: one launch
         launch_coarse_grid(desc_.ptr, gbar_.ptr, gflag_, g32, degree_, alpha_, s);
     } else {
-        FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32), 256, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
+        FX_LAUNCH(k_restrict, grid_for((int64_t)l.n_agg * 32, kLnThreads), kLnThreads, 0, s, l.n_agg, l.agg_ptr.ptr, l.agg_nodes.ptr, 3,
                   l.Q.ptr, l.r.ptr, c.b.ptr, coarse_start(1));
         coarse(1, s);
         if (g32)
@@ -1930,6 +1935,8 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
             o.c2 = k.c2[st];
         }
         if (st == degree_ - 1 && S) {
+            if (2 * (int64_t)grid > part_slots_)
+                fail(FX_GENERIC, "multigrid: partial-sum buffer smaller than the smoother grid");
             o.dot = 2;
             o.zold = zold;
             o.part = part;
@@ -2112,6 +2119,11 @@ void Amg::describe(ClInst& o) const {
     }
 }
 
+#ifndef FX_AMG_EST32
+#define FX_AMG_EST32 1
+#endif
+constexpr bool kAmgEst32 = FX_AMG_EST32 != 0;
+
 void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
                      double cell0, const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse, bool persistent) {
     const int n = S.n_rows;
@@ -2125,7 +2137,11 @@ void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* 
         vals16_.alloc((size_t)S.n_groups * 36, s);
         FX_LAUNCH(k_vals_to_f16, grid_for((int64_t)n * 32), 256, 0, s, n, S.goff.ptr, S.cols.ptr, vals64, sq4_.ptr,
                   vals16_.ptr);
-    } else if (opt.amg_fp32) {
+    }
+    // FP32 values: the FP32 smoother's; with the FP16 smoother they still serve the level-0
+    // eigenvalue estimates (kAmgEst32), whose power iterations read them instead of the
+    // FP64 values
+    if (opt.amg_fp32 && (!f16 || kAmgEst32)) {
         const int64_t nv = (int64_t)S.n_groups * 36;
         vals32_.alloc(nv, s);
         FX_LAUNCH(k_f64_to_f32, 148 * 8, 256, 0, s, nv, vals64, vals32_.ptr);
@@ -2153,6 +2169,7 @@ void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* 
     q_.alloc(nd, s);
     const int nb = 296;
     part_.alloc(std::max<int64_t>(nb, l0_part_slots(n)), s);
+    amg.set_part_slots((int64_t)part_.n);
     sc_.alloc(8, s);
     sc_.zero(s);
     counter_.alloc(1, s);
@@ -2206,6 +2223,7 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     prepare(S, vals64, dinv64, xyz, cell0, opt, s, st, reuse);
     const int nb = 296;
     const unsigned g0 = l0_grid(n);
+    if (2 * (int64_t)g0 > (int64_t)part_.n) fail(FX_GENERIC, "multigrid: partial-sum buffer smaller than the CG grid");
     FX_CUDA_CHECK(cudaMemsetAsync(x, 0, nd * sizeof(double), s));
     FX_CUDA_CHECK(cudaMemcpyAsync(r_.ptr, b, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
     // ||b||_D, z = V(b) with r.z, p = z

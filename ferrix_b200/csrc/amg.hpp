@@ -123,6 +123,8 @@ class Amg {
     // started: the level-0 start (r0 = b, x = d = c2 D^-1 b) was done by the caller, into start0()
     void apply(const double* r, double* z, double* S, double* part, int* counter, const double* zold,
                cudaStream_t s, bool started = false);
+    // slots of the `part` buffer apply() reduces into (two per CTA of the reducing launch)
+    void set_part_slots(int64_t n) { part_slots_ = n; }
     // where the level-0 start writes: the smoother's residual, iterate and first direction
     // (FP32 float4 per node when the smoother is FP32, else FP64), and its coefficient
     struct Start0 {
@@ -157,6 +159,7 @@ class Amg {
     void vcycle0(const VT* vals, const double* b, double* z, double* S, double* part, int* counter,
                  const double* zold, cudaStream_t s, bool started);
     bool kcycle_ = false;
+    int64_t part_slots_ = 0;
     int cheb_kind_ = 0;
     double alpha_ = 1.0, cheb_ratio_ = 30.0;
     int degree_ = 2;

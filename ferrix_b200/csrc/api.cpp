@@ -379,6 +379,18 @@ int fx_step_solve(fx_model* m, int k, const fx_solve_opts* opts, fx_step_stats* 
     });
 }
 
+int fx_step_solve_cb(fx_model* m, int k, const fx_solve_opts* opts, fx_step_stats* st, fx_increment_cb cb,
+                     void* user) {
+    if (!m || !m->ctx) return FX_INVALID_ARGUMENT;
+    fx_solve_opts o;
+    if (opts) o = *opts;
+    else fx_default_solve_opts(&o);
+    return guarded(m->ctx, [&] {
+        FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        return step_solve(m, k, o, st, cb, user);
+    });
+}
+
 int fx_assemble_csr(fx_model* m, const double* u, int precision, int64_t* nnz, int64_t* indptr, int64_t* indices,
                     double* data, double* maxdiag) {
     if (!m || !nnz) return FX_INVALID_ARGUMENT;

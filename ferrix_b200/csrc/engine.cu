@@ -70,7 +70,8 @@ static void upload_mats(const MatTableHost& h, MatTableDev& d, cudaStream_t s) {
 double model_footprint(const DenseModel& D) {
     const double e20 = (double)D.g20.size(), e4 = (double)D.g4.size(), n = (double)D.n_nodes;
     const double blocks = 240.0 * e20 + 2.8 * e4;
-    return e20 * 32.0e3 + e4 * 1.6e3 + blocks * 120.0 + n * 1.0e3 + 64.0e6;
+    // per 3x3 block: FP64, FP32 and FP16 values (126 B), column ids and group padding
+    return e20 * 32.0e3 + e4 * 1.6e3 + blocks * 136.0 + n * 1.0e3 + 64.0e6;
 }
 
 // Spare pool memory to hold before a model's work is queued: 50 % over the
@@ -285,6 +286,9 @@ struct StepRunner {
     int it = 0;
     enum { kNewInc, kIter, kDone } state = kNewInc;
     bool need_solve = false;
+    // host callback after every converged increment (fx_step_solve_cb), else null
+    fx_increment_cb inc_cb = nullptr;
+    void* inc_user = nullptr;
     fx_step_stats S{};
     double nrm[2] = {0, 0};
     int err_flag = 0;
@@ -435,6 +439,13 @@ struct StepRunner {
                                           m->ctx->stream));
             state = kNewInc;
             need_solve = false;
+            if (inc_cb) {  // the converged increment's result (static_step.rs:219-248: write_increment)
+                FX_CUDA_CHECK(cudaMemcpyAsync(m->dev.u.ptr, m->dev.ustart.ptr, n3 * sizeof(double),
+                                              cudaMemcpyDeviceToDevice, m->ctx->stream));
+                stream_wait(m->ctx->stream, "increment result");
+                const int rc = inc_cb(inc_user, m, step_id, (int)n_inc, m->timer.global);
+                if (rc != 0) fail(FX_GENERIC_IO, "Generic IO error: increment callback returned " + std::to_string(rc));
+            }
         } else {
             need_solve = true;
         }
@@ -739,7 +750,7 @@ static void run_rounds(fx_ctx* ctx, std::vector<StepRunner*>& rs, std::vector<in
     stream_wait(s, "stream");
 }
 
-int step_solve(fx_model* m, int k, const fx_solve_opts& o, fx_step_stats* st) {
+int step_solve(fx_model* m, int k, const fx_solve_opts& o, fx_step_stats* st, fx_increment_cb cb, void* user) {
     fx_ctx* ctx = m->ctx;
     int64_t* saved = g_launch_counter;
     g_launch_counter = &ctx->launches;
@@ -753,6 +764,8 @@ int step_solve(fx_model* m, int k, const fx_solve_opts& o, fx_step_stats* st) {
     tot.start(ctx->stream);
     StepRunner r;
     r.begin(m, k, o);
+    r.inc_cb = cb;
+    r.inc_user = user;
     std::vector<StepRunner*> rs{&r};
     std::vector<int> status;
     std::vector<std::string> msgs;

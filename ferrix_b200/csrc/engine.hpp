@@ -154,7 +154,8 @@ void compute_thermal_force(fx_model* m, double* d_out);
 // assembles K (precision) at X (+d_u) into dev.vals32/vals64; returns maxdiag (host copy)
 double assemble(fx_model* m, const double* d_u, bool fp64);
 void check_device_errors(fx_model* m, const char* where);
-int step_solve(fx_model* m, int step_index, const fx_solve_opts& opts, fx_step_stats* stats);
+int step_solve(fx_model* m, int step_index, const fx_solve_opts& opts, fx_step_stats* stats,
+               fx_increment_cb cb = nullptr, void* user = nullptr);
 int batch_solve(fx_ctx* ctx, fx_model* const* models, int n, const fx_solve_opts& opts, int* status,
                 fx_step_stats* stats);
 

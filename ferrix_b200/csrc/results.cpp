@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <string>
 #include <vector>
 
@@ -211,5 +212,43 @@ int fx_write_vtk(fx_model* m, const char* path) {
         return FX_OK;
     });
 }
+
+// results.vtk.series (src/solver/io/vtk.rs:46-70, 305-333), byte for byte: the header of
+// init, one entry per written increment, the footer of finish.
+static int series_write(const char* dir, const char* mode, const std::string& text) {
+    if (!dir) return FX_INVALID_ARGUMENT;
+    return guarded(nullptr, [&] {
+        const std::string path = std::string(dir) + "/results.vtk.series";
+        FILE* f = std::fopen(path.c_str(), mode);
+        if (!f) fail(FX_GENERIC_IO, "Generic IO error: cannot open " + path);
+        const size_t w = std::fwrite(text.data(), 1, text.size(), f);
+        const int c = std::fclose(f);
+        if (w != text.size() || c != 0) fail(FX_GENERIC_IO, "Generic IO error: write failed: " + path);
+        return FX_OK;
+    });
+}
+
+int fx_vtk_series_init(const char* dir) {
+    if (!dir) return FX_INVALID_ARGUMENT;
+    std::error_code ec;
+    std::filesystem::create_directories(dir, ec);
+    if (ec) {
+        fx::thread_error().set(FX_GENERIC_IO, std::string("Generic IO error: cannot create ") + dir);
+        return FX_GENERIC_IO;
+    }
+    return series_write(dir, "wb", "{\n          \"file-series-version\" : \"1.0\",\n          \"files\" : [\n");
+}
+
+int fx_vtk_series_add(const char* dir, const char* name, double time) {
+    if (!dir || !name) return FX_INVALID_ARGUMENT;
+    // the reference's "{}" of an f64: the shortest decimal that reads back to the same
+    // value, never in exponent form
+    char buf[512];
+    const auto r = std::to_chars(buf, buf + sizeof(buf), time, std::chars_format::fixed);
+    const std::string t = r.ec == std::errc() ? std::string(buf, r.ptr) : std::to_string(time);
+    return series_write(dir, "ab", std::string("{ \"name\" : \"") + name + "\", \"time\" : " + t + " },\n");
+}
+
+int fx_vtk_series_finish(const char* dir) { return series_write(dir, "ab", "  ]\n}\n"); }
 
 }  // extern "C"

@@ -298,6 +298,19 @@ int fx_state_set_temperatures(fx_model* model, const double* t_init /* N */, con
  * stats may be NULL; opts NULL = fx_default_solve_opts. */
 int fx_step_solve(fx_model* model, int step_index, const fx_solve_opts* opts, fx_step_stats* stats);
 
+/* Called on the host after every converged increment of fx_step_solve_cb, where the
+ * reference hands the increment's result to ResultWriter::write_increment
+ * (src/solver/step/static_step.rs:219-248, src/solver/io/writer.rs:7-34): step_id (1-based),
+ * inc_id (the step's increment counter, failed attempts included, as the reference counts
+ * them) and global_time (SolverTime::global_time, src/solver/time.rs:51-55). While it runs,
+ * the model's displacements and temperatures are that increment's, so the callback may
+ * read them (fx_state_get_displacements, fx_nodal_stress_strain, fx_write_vtk, ...); it must
+ * not solve on the same model. A nonzero return ends the step with FX_GENERIC_IO. */
+typedef int (*fx_increment_cb)(void* user, fx_model* model, int step_id, int inc_id, double global_time);
+/* fx_step_solve with cb called after every converged increment (cb NULL: fx_step_solve). */
+int fx_step_solve_cb(fx_model* model, int step_index, const fx_solve_opts* opts, fx_step_stats* stats,
+                     fx_increment_cb cb, void* user);
+
 /* ---- lower-level seams (parity tests, Rust shims) -------------------- */
 /* Stiffness on X (+u when u != NULL) with the current temperatures, as the
  * expanded CSR of the 3x3 block structure (explicit zeros kept), FP64 values
@@ -373,6 +386,15 @@ int fx_nodal_stress_strain(fx_model* model, double* S, double* E);
  * follows its hash-map order). The series file and directory layout stay
  * with the caller. */
 int fx_write_vtk(fx_model* model, const char* path);
+/* The ParaView time series of the reference's VtkWriter (src/solver/io/vtk.rs:46-70,
+ * 305-333): fx_vtk_series_init creates `dir` (and its parents) and writes the header of
+ * dir/results.vtk.series; fx_vtk_series_add appends { "name" : name, "time" : time } (the
+ * reference writes step_<step_id>_<inc_id>.vtk beside it, with fx_write_vtk here);
+ * fx_vtk_series_finish closes the list. The bytes match the reference's file, including the
+ * comma after the last entry. FX_GENERIC_IO when a file cannot be created or written. */
+int fx_vtk_series_init(const char* dir);
+int fx_vtk_series_add(const char* dir, const char* name, double time);
+int fx_vtk_series_finish(const char* dir);
 
 /* ---- batched decks ---------------------------------------------------- */
 /* Runs the first step of every model (each fx_state_initialize'd) with all

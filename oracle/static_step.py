@@ -87,8 +87,11 @@ def jacobi_pcg(K: sp.csr_matrix, b: np.ndarray, tol: float = 1e-8, max_iter: int
 class Runner:
     """Holds the dense model view, the ordering and timings across steps."""
 
-    def __init__(self, project: Project, verbose: bool = False):
+    def __init__(self, project: Project, verbose: bool = False, on_increment=None):
         self.p = project
+        # on_increment(step_id, inc_id, global_time, displacements): called after every
+        # converged increment, where static_step.rs:219-248 hands the result to the writer
+        self.on_increment = on_increment
         self.m: ModelArrays = model_arrays(project)
         self.mf: Optional[MultifrontalCholesky] = None
         self.verbose = verbose
@@ -192,6 +195,8 @@ class Runner:
             if converged:
                 cur += dt
                 u_start = u.copy()
+                if self.on_increment is not None:
+                    self.on_increment(step_id, n_inc, timer.global_, u_start.copy())
             else:
                 dt /= 2.0
                 if dt < inc.min_time_increment:
