@@ -105,7 +105,11 @@ def _oracle_job(out_path: str, q, go=None) -> None:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms. The sampler starts before
+    the warm-up steps and stops after all GPU measurements: starting and stopping nvidia-smi
+    (NVML initialisation and teardown) stalled the CUDA work beside it by up to ~0.5 s on
+    these hosts, which must not fall inside a timed region. mark() delimits the samples
+    that the summary covers (those taken during the timed region)."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -115,6 +119,17 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.proc = None
+        self.span = None
+
+    def mark(self):
+        """Row count now: call at the start and at the end of the timed region."""
+        return len(self.rows)
+
+    def summary(self, i0: int, i1: int):
+        """Median SM clock and throttle reasons of the samples taken between two marks (the
+        neighbouring sample on each side when none fell inside a short region)."""
+        self.span = (max(0, i0 - 1), i1 + 1) if i1 <= i0 else (i0, i1)
+        return self._summarise(self.rows[self.span[0]:self.span[1]])
 
     def start(self):
         try:
@@ -132,15 +147,19 @@ class ClockSampler:
 
     def stop(self):
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+
+    def _summarise(self, rows):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+        for r in rows:
             try:
                 sm.append(float(r[0]))
                 mx = float(r[1])
@@ -603,23 +622,24 @@ def main():
         project.drop_cache()
         return project.steps[0].solve(1, project, state, opts=opts)
 
+    clocks = ClockSampler(local)
+    clocks.start()  # before the warm-up: nvidia-smi's start-up stall lands there
     for _ in range(max(3, args.warmup)):
         one_step()
-    clocks = ClockSampler(local)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = ctx.kernel_launches
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    clocks.start()
+    mark0 = clocks.mark()
     ev0.record(stream)
     stats = []
     for _ in range(args.steps):
         stats.append(one_step())
     ev1.record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = clocks.summary(mark0, clocks.mark())
     elapsed = ev0.elapsed_time(ev1) / 1e3
     launches = ctx.kernel_launches - launches0
     u_gpu = state.displacements
@@ -715,6 +735,7 @@ def main():
         serving_line["solver"] = "mixed multigrid CG"
         serving_line["pool"] = "16 seeded boxes, 60% C3D4 / 40% C3D20, DOF log-uniform [5k, 500k]"
         serving_line["input"] = "fx_model_from_arrays"
+    clocks.stop()  # after every GPU measurement (its teardown must not overlap one)
 
     cpu = None
     rel_err = None

@@ -1337,29 +1337,37 @@ __global__ void k_diag_sqrt(int n, const int32_t* __restrict__ goff, const int32
 
 // FP16 copy of the scaled matrix S A S, S = diag(sqrt(a_ii))^-1 with the float square
 // roots of k_diag_sqrt (the smoother scales its vectors by the same values): |entries| <= 1
-// for a symmetric positive definite matrix; warp per block row, lanes over column groups.
+// for a symmetric positive definite matrix. Warp per block row; lane `it` takes plane
+// e = it / ng of group g = it % ng, whose 4 values are the row's vec4 number it (planar
+// layout), so a warp reads consecutive 32-byte vectors; the scale is an FP32 reciprocal
+// of sqrt(a_ii) sqrt(a_jj) (its rounding, ~6e-8, is far below FP16's).
 __global__ void k_vals_to_f16(int n, const int32_t* __restrict__ goff, const int32_t* __restrict__ cols,
                               const double* __restrict__ vals, const float4* __restrict__ sq4, __half* __restrict__ out) {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (row >= n) return;
-    const int64_t g0 = goff[row], ng = goff[row + 1] - g0;
+    const int64_t g0 = goff[row];
+    const int ng = goff[row + 1] - (int)g0;
     const float4 sr = sq4[row];
-    const double srow[3] = {sr.x, sr.y, sr.z};
-    for (int64_t g = lane; g < ng; g += 32) {
-        const int4 cc = reinterpret_cast<const int4*>(cols)[g0 + g];
+    for (int it = lane; it < 9 * ng; it += 32) {
+        const int e = it / ng, g = it - e * ng;
+        const int4 cc = __ldg(reinterpret_cast<const int4*>(cols) + g0 + g);
         const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
-        double scol[4][3];
+        const int cr = e / 3, ccomp = e - 3 * cr;
+        const float si = cr == 0 ? sr.x : (cr == 1 ? sr.y : sr.z);
+        const double2* src = reinterpret_cast<const double2*>(vals + (g0 * 9 + it) * 4);
+        const double2 v01 = __ldcs(src), v23 = __ldcs(src + 1);
+        const double v[4] = {v01.x, v01.y, v23.x, v23.y};
+        __half h[4];
+#pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const float4 t = sq4[cj[q]];
-            scol[q][0] = t.x;
-            scol[q][1] = t.y;
-            scol[q][2] = t.z;
+            const float4 t = __ldg(sq4 + cj[q]);
+            const float sj = ccomp == 0 ? t.x : (ccomp == 1 ? t.y : t.z);
+            h[q] = __double2half(v[q] * (double)(1.0f / (si * sj)));
         }
-        for (int e = 0; e < 9; ++e)
-            for (int q = 0; q < 4; ++q) {
-                const int64_t at = (g0 * 9 + (int64_t)e * ng + g) * 4 + q;
-                out[at] = __double2half(vals[at] / (srow[e / 3] * scol[q][e % 3]));
-            }
+        uint2 packed;
+        packed.x = (uint32_t)__half_as_ushort(h[0]) | ((uint32_t)__half_as_ushort(h[1]) << 16);
+        packed.y = (uint32_t)__half_as_ushort(h[2]) | ((uint32_t)__half_as_ushort(h[3]) << 16);
+        reinterpret_cast<uint2*>(out)[g0 * 9 + it] = packed;
     }
 }
 
