@@ -31,6 +31,11 @@ bool debug_sync() {
     return on;
 }
 
+#ifndef FX_WAIT_SPIN_US
+#define FX_WAIT_SPIN_US 5000
+#endif
+constexpr double kWaitSpinS = FX_WAIT_SPIN_US * 1e-6;
+
 void stream_wait(cudaStream_t s, const char* what, double timeout_s) {
     auto t0 = std::chrono::steady_clock::now();
     while (true) {
@@ -39,7 +44,10 @@ void stream_wait(cudaStream_t s, const char* what, double timeout_s) {
         if (e != cudaErrorNotReady) fail(FX_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
         double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (dt > timeout_s) fail(FX_TIMEOUT, std::string("device work did not finish in time: ") + what);
-        std::this_thread::sleep_for(std::chrono::microseconds(dt < 0.01 ? 2 : 200));
+        // The first kWaitSpinS of a wait poll without sleeping: a short sleep lasts the kernel's
+        // timer slack (~50 us on Linux), which the GPU spent idle after every CG replay (~2 ms
+        // of work) before the host could launch the next; longer waits sleep between polls.
+        if (dt >= kWaitSpinS) std::this_thread::sleep_for(std::chrono::microseconds(dt < 0.05 ? 20 : 200));
     }
     if (debug_sync()) std::fprintf(stderr, "[sync] %s ok\n", what);
 }
