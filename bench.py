@@ -488,7 +488,7 @@ def run_batch(args, rank: int, local: int) -> None:
                                               "wall_s": wall_s,
                                               "failed": int(multi.sum_over_ranks(float(np.sum(st != 0)), "cuda")),
                                               "pcg_iterations_max": int(max(s["pcg_iterations"] for s in stats))}
-    o_amg = fx.solve_opts(rtol=1e-8)  # default: mixed multigrid (solved one system at a time inside the rounds)
+    o_amg = fx.solve_opts(rtol=1e-8)  # default: mixed multigrid, the decks spread over four worker streams
     for rep in range(2):
         ps = projects()
         (st_a, _), dev_s, wall_s = timed(lambda: fx.batch_solve(ctx, ps, o_amg))
@@ -518,7 +518,7 @@ def run_batch(args, rank: int, local: int) -> None:
     from ferrix_b200 import serving
     res = serving.run_stream(texts, 1e6, len(texts), fx.solve_opts(precision=fx.PREC_MIXED,
                                                                   preconditioner=fx.PRECOND_AMG, rtol=1e-8),
-                             device=local, slots=4, seed=1)
+                             device=local, slots=4, seed=1, each_once=True)
     span = multi.max_over_ranks(res["span_s"], device="cuda")
     out["arms"]["request_loop_mixed_amg_4_slots"] = {"solves_per_s": len(pop) / span, "wall_s": span,
                                                      "failed": int(multi.sum_over_ranks(
