@@ -869,15 +869,6 @@ constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per 
 #define FX_L0_MIN_BLOCKS_H 4
 #endif
 constexpr int kL0MinBlocksH = FX_L0_MIN_BLOCKS_H;
-// FP16 values, two block rows per 8-lane group (k_l0h_pair) instead of one
-#ifndef FX_L0_PAIR_H
-#define FX_L0_PAIR_H 0
-#endif
-constexpr bool kL0PairH = FX_L0_PAIR_H != 0;
-#ifndef FX_L0_MIN_BLOCKS_HP
-#define FX_L0_MIN_BLOCKS_HP 3
-#endif
-constexpr int kL0MinBlocksHP = FX_L0_MIN_BLOCKS_HP;
 
 #ifndef FX_L0_LANES
 #define FX_L0_LANES 8
@@ -1033,131 +1024,6 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
             const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * vc) + o.c2 * z;
             if (G32) o.d4_out[4 * (int64_t)row + c] = (float)(H ? dn * (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z)) : dn);
             else o.d_out[o3 + c] = dn;
-            const double xn = (MODE == kL0Cheb0 ? vc : xoc) + dn;
-            o.xo[o3 + c] = xn;
-            if (o.dot) {
-                dsum += bc * xn;
-                dsum2 += bc * zoc;
-            }
-        }
-    }
-    if (o.dot) cta_dot_finalize(dsum, dsum2, o.dot, o.part, o.counter, o.S);
-}
-
-// FP16 fine-level operator with two block rows per 8-lane group (kL0PairH): rows 2p and
-// 2p + 1 are consecutive, so their column groups are too (cols index g0 + j for the j-th
-// group of the pair); the 8 lanes split the pair's ng_A + ng_B groups, which halves the
-// row passes per warp (each a chain of dependent loads) and evens out rows of different
-// length. Lanes 0-2 then finish row A's components and lanes 3-5 row B's. Same modes,
-// operands and arithmetic per row as k_l0_op<__half, MODE, true>.
-template <int MODE>
-__global__ void __launch_bounds__(256, kL0MinBlocksHP) k_l0h_pair(L0Op<__half> o) {
-    const int sub = threadIdx.x & 7;
-    const int grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const int groups_per_grid = (gridDim.x * blockDim.x) >> 3;
-    const int npair = (o.n + 1) >> 1;
-    const int npair_w = ((npair + 3) >> 2) << 2;  // uniform trip count per warp (4 groups)
-    double dsum = 0.0, dsum2 = 0.0;
-    for (int pbase = grp - (grp & 3); pbase < npair_w; pbase += groups_per_grid) {
-        const int pr = pbase + (grp & 3);
-        const int rA = 2 * pr, rB = rA + 1;
-        const bool vA = rA < o.n, vB = rB < o.n;
-        const int gA0 = vA ? o.goff[rA] : 0;
-        const int gA1 = vA ? o.goff[rA + 1] : 0;
-        const int gB1 = vB ? o.goff[rB + 1] : gA1;
-        const int ngA = gA1 - gA0, ngB = gB1 - gA1, ngt = ngA + ngB;
-        double accA[3] = {0.0, 0.0, 0.0}, accB[3] = {0.0, 0.0, 0.0};
-#pragma unroll 2
-        for (int j = sub; j < ngt; j += 8) {
-            const bool inA = j < ngA;
-            const int64_t vbase = inA ? (int64_t)gA0 * 9 + j : (int64_t)gA1 * 9 + (j - ngA);
-            const int64_t pl = inA ? ngA : ngB;
-            const __half* vh = reinterpret_cast<const __half*>(o.vals) + vbase * 4;
-            uint2 raw[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) raw[k] = __ldcs(reinterpret_cast<const uint2*>(vh + (int64_t)k * pl * 4));
-            const int4 cc = __ldg(reinterpret_cast<const int4*>(o.cols) + gA0 + j);
-            const int cj[4] = {cc.x, cc.y, cc.z, cc.w};
-            float xv[4][3];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float4 t = __ldg(o.v4 + cj[q]);
-                xv[q][0] = t.x;
-                xv[q][1] = t.y;
-                xv[q][2] = t.z;
-            }
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                float m0[4], m1[4], m2[4];
-                unpack_h4(raw[3 * r], m0);
-                unpack_h4(raw[3 * r + 1], m1);
-                unpack_h4(raw[3 * r + 2], m2);
-                float t = 0.0f;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) t += m0[q] * xv[q][0] + m1[q] * xv[q][1] + m2[q] * xv[q][2];
-                if (inA) accA[r] += (double)t;
-                else accB[r] += (double)t;
-            }
-        }
-#pragma unroll
-        for (int s = 4; s > 0; s >>= 1)
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                accA[r] += __shfl_xor_sync(0xffffffffu, accA[r], s);
-                accB[r] += __shfl_xor_sync(0xffffffffu, accB[r], s);
-            }
-        // epilogue: lanes 0-2 row A, lanes 3-5 row B, component c each (lanes 6, 7 idle)
-        const bool isA = sub < 3;
-        const int row = isA ? rA : rB;
-        const int c = isA ? sub : (sub < 6 ? sub - 3 : 0);
-        const bool epi = (isA && vA) || (sub >= 3 && sub < 6 && vB);
-        const int64_t o3 = 3 * (int64_t)row;
-        double acc[3];
-#pragma unroll
-        for (int r = 0; r < 3; ++r) acc[r] = isA ? accA[r] : accB[r];
-        double src3[3] = {0.0, 0.0, 0.0}, Dr[3] = {0.0, 0.0, 0.0}, vc = 0.0, xoc = 0.0, bc = 0.0, zoc = 0.0;
-        float4 sqi = make_float4(1.f, 1.f, 1.f, 0.f);
-        if (epi) {
-            sqi = __ldg(o.sq4 + row);
-            if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
-                const double* src = MODE == kL0Cheb0 ? o.b : o.r;
-#pragma unroll
-                for (int kk = 0; kk < 3; ++kk) {
-                    src3[kk] = src[o3 + kk];
-                    Dr[kk] = o.dinv[9 * (int64_t)row + 3 * c + kk];
-                }
-                if (MODE == kL0ChebK) {
-                    const float* own = reinterpret_cast<const float*>(o.v4 + row);
-                    vc = (double)own[c] / (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z));
-                    xoc = o.xo[o3 + c];
-                } else {
-                    vc = o.v[o3 + c];
-                }
-                if (o.dot) bc = o.b[o3 + c];
-                if (o.dot && o.zold) zoc = o.zold[o3 + c];
-            } else if (MODE == kL0Resid) {
-                bc = o.b ? o.b[o3 + c] : 0.0;
-            } else {
-                src3[0] = o.r[o3 + c];
-            }
-        }
-        // (A v)_i = sqrt(a_ii) (S A S (sqrt(a_jj) v_j))_i
-        acc[0] *= (double)sqi.x;
-        acc[1] *= (double)sqi.y;
-        acc[2] *= (double)sqi.z;
-        const double axc = c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]);
-        __syncwarp();  // every lane's reads of r (above) are ordered before any lane writes r[c]
-        if (!epi) continue;
-        if (MODE == kL0Resid) {
-            o.y[o3 + c] = o.b ? bc - axc : axc;
-        } else if (MODE == kL0RUpd) {
-            o.r[o3 + c] = src3[0] - axc;
-        } else {  // Chebyshev steps
-            const double rr[3] = {src3[0] - acc[0], src3[1] - acc[1], src3[2] - acc[2]};
-            const double z = Dr[0] * rr[0] + Dr[1] * rr[1] + Dr[2] * rr[2];
-            o.r[o3 + c] = c == 0 ? rr[0] : (c == 1 ? rr[1] : rr[2]);
-            const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * vc) + o.c2 * z;
-            o.d4_out[4 * (int64_t)row + c] = (float)(dn * (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z)));
             const double xn = (MODE == kL0Cheb0 ? vc : xoc) + dn;
             o.xo[o3 + c] = xn;
             if (o.dot) {
@@ -1524,23 +1390,13 @@ static unsigned l0_grid(int n, bool h = false) {
         int sms = 0, per_sm = 0, per_sm_h = 0;
         FX_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_l0_op<double, kL0ChebK>, 256, 0));
-        if constexpr (kL0PairH)
-            FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_h, k_l0h_pair<kL0ChebK>, 256, 0));
-        else
-            FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_h, k_l0_op<__half, kL0ChebK, true>,
-                                                                        256, 0));
+        FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_h, k_l0_op<__half, kL0ChebK, true>, 256,
+                                                                    0));
         cached_cap[0] = std::max(1, sms * std::max(1, per_sm));
         cached_cap[1] = std::max(1, sms * std::max(1, per_sm_h));
         cached_dev = dev;
     }
     return (unsigned)std::min<int64_t>(grid_for((int64_t)n * kL0Lanes), cached_cap[h ? 1 : 0]);
-}
-
-// A level-0 operator launch: FP16 values take the two-rows-per-group kernel when kL0PairH.
-template <typename VT, int MODE, bool G32>
-static void launch_l0(unsigned grid, cudaStream_t s, const L0Op<VT>& o) {
-    if constexpr (std::is_same<VT, __half>::value && kL0PairH) FX_LAUNCH(k_l0h_pair<MODE>, grid, 256, 0, s, o);
-    else FX_LAUNCH((k_l0_op<VT, MODE, G32>), grid, 256, 0, s, o);
 }
 
 // Slots of the partial-sum buffer a level-0 operator with a dot product needs: two per CTA
@@ -2045,7 +1901,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
         o.xo = l.x.ptr;
         o.c1 = k.c1[st];
         o.c2 = k.c2[st];
-        launch_l0<VT, kL0ChebK, g32>(grid, s, o);
+        FX_LAUNCH((k_l0_op<VT, kL0ChebK, g32>), grid, 256, 0, s, o);
         std::swap(dA, dB);
         std::swap(dA4, dB4);
     }
@@ -2054,7 +1910,7 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
         o.v = dA;
         o.v4 = dA4;
         o.r = l.r.ptr;
-        launch_l0<VT, kL0RUpd, g32>(grid, s, o);  // r = b - A x
+        FX_LAUNCH((k_l0_op<VT, kL0RUpd, g32>), grid, 256, 0, s, o);  // r = b - A x
     }
     if (fused_coarse_ && !kcycle_ && desc_.ptr) {  // restriction, coarse levels, prolongation: one launch
         launch_coarse_grid(desc_.ptr, gbar_.ptr, gflag_, g32, degree_, alpha_, s);
@@ -2095,9 +1951,9 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
             o.counter = counter;
             o.S = S;
         }
-        if (st == 0) launch_l0<VT, kL0Cheb0, g32>(grid, s, o);
+        if (st == 0) FX_LAUNCH((k_l0_op<VT, kL0Cheb0, g32>), grid, 256, 0, s, o);
         else {
-            launch_l0<VT, kL0ChebK, g32>(grid, s, o);
+            FX_LAUNCH((k_l0_op<VT, kL0ChebK, g32>), grid, 256, 0, s, o);
             std::swap(dA, dB);
             std::swap(dA4, dB4);
         }
@@ -2174,7 +2030,7 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
             o.c1 = 0.5;
             o.c2 = 1e-9;
             o.sq4 = sq4.ptr;
-            launch_l0<__half, kL0ChebK, true>(grid, s, o);
+            FX_LAUNCH((k_l0_op<__half, kL0ChebK, true>), grid, 256, 0, s, o);
         } else if (fp32) {
             L0Op<float> o = l0_op<float>(l, v32.ptr);
             o.v = v.ptr;
