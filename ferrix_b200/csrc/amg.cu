@@ -758,6 +758,9 @@ struct L0Op {
     // FP16 values of the diagonally scaled matrix S A S (S = diag(a_ii)^-1/2): sqrt(a_ii)
     // per node; the gathered float4 vectors then hold sqrt(a_jj) v_j
     const float4* sq4;
+    // FP16 smoother directions (kL0H16Vec): {2^k, 2^-k}, the V-cycle's scale of the
+    // stored directions (null: 1)
+    const float* hs;
 };
 
 __device__ __forceinline__ void ld4v(const float* p, float o[4]) {
@@ -869,6 +872,37 @@ constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per 
 #define FX_L0_MIN_BLOCKS_H 4
 #endif
 constexpr int kL0MinBlocksH = FX_L0_MIN_BLOCKS_H;
+// FP16 smoother: the Chebyshev directions as four halves per node (8 bytes) instead of
+// a float4 (the prolongated iterate stays FP32). The directions shrink with the outer
+// CG's residual, by 1e8 and more over a solve, so unscaled they fall below FP16's
+// subnormal range and the smoothing stops; they are stored times a power of two taken
+// from the residual the V-cycle smooths.
+#ifndef FX_L0_H16VEC
+#define FX_L0_H16VEC 1
+#endif
+constexpr bool kL0H16Vec = FX_L0_H16VEC != 0;
+// the stored directions' 2-norm is about 2^kH16Exp: a direction entry overflows only if the
+// residual grows by about 2^(15 - kH16Exp) from one outer iteration to the next, and the
+// entries of a vector of 1e7 nodes still sit ~10 binades above the smallest normal FP16
+constexpr int kH16Exp = 8;
+
+// {2^k, 2^-k} with 2^k sqrt(rdr) in [2^(kH16Exp-1), 2^kH16Exp), rdr = r.D^-1 r of the
+// residual the V-cycle smooths: the smoother's directions c D^-1 r scaled by sqrt(a_ii)
+// have a 2-norm of about sqrt(rdr). A power of two scales exactly, so the FP16 roundings
+// are those of an FP16 whose range is centred on the vector.
+__device__ __forceinline__ float2 h16_scale(double rdr) {
+    if (!(rdr > 0.0) || !isfinite(rdr)) return make_float2(1.0f, 1.0f);
+    int e;
+    frexp(sqrt(rdr), &e);
+    const int k = max(-100, min(100, kH16Exp - e));
+    return make_float2(ldexpf(1.0f, k), ldexpf(1.0f, -k));
+}
+
+// FP16 bits of x rounded to nearest, clamped to the finite range (a direction that
+// outgrows the lagged scale saturates instead of turning the smoother's sums into inf)
+__device__ __forceinline__ uint32_t h16_bits(float x) {
+    return __half_as_ushort(__float2half_rn(fminf(fmaxf(x, -65504.0f), 65504.0f)));
+}
 
 #ifndef FX_L0_LANES
 #define FX_L0_LANES 8
@@ -894,6 +928,10 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
     // (FX_L0_LATE_EPI_H), which frees their registers during the gather loop
     constexpr bool kL0LateEpi = H && FX_L0_LATE_EPI_H;
     constexpr bool kL0VFirst = H && FX_L0_VFIRST_H;
+    // FP16 directions: written by the Chebyshev steps, gathered by all but the step from
+    // the (FP32) iterate; 2^-k is applied to the row sums, after the gathers
+    constexpr bool kH16 = H && G32 && kL0H16Vec;
+    constexpr bool kH16g = kH16 && MODE != kL0Cheb0;
     const int sub = threadIdx.x & (kL0Lanes - 1);
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> kL0LaneShift;
     const int rows_per_grid = (gridDim.x * blockDim.x) >> kL0LaneShift;
@@ -912,8 +950,10 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
         const bool epi = valid && sub < 3;
         double src3[3] = {0.0, 0.0, 0.0}, Dr[3] = {0.0, 0.0, 0.0}, vc = 0.0, xoc = 0.0, bc = 0.0, zoc = 0.0;
         float4 sqi = make_float4(1.f, 1.f, 1.f, 0.f);
+        float2 hsc = make_float2(1.f, 1.f);  // {2^k, 2^-k}: .x is read where the direction is stored
         auto load_epi = [&]() {
         if (H && epi) sqi = __ldg(o.sq4 + row);
+        if (kH16g && epi && o.hs) hsc.y = __ldg(o.hs + 1);
         if (epi) {
             if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
                 const double* src = MODE == kL0Cheb0 ? o.b : o.r;
@@ -924,7 +964,10 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
                 }
                 if (G32 && MODE == kL0ChebK) {
                     const float* own = reinterpret_cast<const float*>(o.v4 + row);
-                    vc = (double)own[c];
+                    if constexpr (kH16)
+                        vc = (double)(__half2float(reinterpret_cast<const __half*>(o.v4)[4 * (int64_t)row + c]) *
+                                      hsc.y);
+                    else vc = (double)own[c];
                     if (H) vc /= (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z));
                 } else {
                     vc = v[o3 + c];
@@ -963,10 +1006,18 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
             if (G32) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const float4 t = __ldg(o.v4 + cj[q]);
-                    xv[q][0] = t.x;
-                    xv[q][1] = t.y;
-                    xv[q][2] = t.z;
+                    if constexpr (kH16g) {
+                        const uint2 u = __ldg(reinterpret_cast<const uint2*>(o.v4) + cj[q]);
+                        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+                        xv[q][0] = a.x;
+                        xv[q][1] = a.y;
+                        xv[q][2] = __half2float(__ushort_as_half((unsigned short)(u.y & 0xffffu)));
+                    } else {
+                        const float4 t = __ldg(o.v4 + cj[q]);
+                        xv[q][0] = t.x;
+                        xv[q][1] = t.y;
+                        xv[q][2] = t.z;
+                    }
                 }
             } else {
 #pragma unroll
@@ -1002,10 +1053,11 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
             for (int r = 0; r < 3; ++r) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], s);
         if (kL0LateEpi) load_epi();
         // epilogue: lane c of the row's 8 handles component c
-        if (H) {  // (A v)_i = sqrt(a_ii) (S A S (sqrt(a_jj) v_j))_i
-            acc[0] *= (double)sqi.x;
-            acc[1] *= (double)sqi.y;
-            acc[2] *= (double)sqi.z;
+        if (H) {  // (A v)_i = sqrt(a_ii) (S A S (sqrt(a_jj) v_j))_i; FP16 directions: times 2^-k
+            const double u = kH16g ? (double)hsc.y : 1.0;
+            acc[0] *= (double)sqi.x * u;
+            acc[1] *= (double)sqi.y * u;
+            acc[2] *= (double)sqi.z * u;
         }
         const double axc = c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]);
         __syncwarp();  // every lane's reads of r (above) are ordered before any lane writes r[c]
@@ -1022,7 +1074,11 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
             const double z = Dr[0] * rr[0] + Dr[1] * rr[1] + Dr[2] * rr[2];
             o.r[o3 + c] = c == 0 ? rr[0] : (c == 1 ? rr[1] : rr[2]);
             const double dn = (MODE == kL0Cheb0 ? 0.0 : o.c1 * vc) + o.c2 * z;
-            if (G32) o.d4_out[4 * (int64_t)row + c] = (float)(H ? dn * (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z)) : dn);
+            if (kH16) {
+                if (o.hs) hsc.x = __ldg(o.hs);
+                reinterpret_cast<unsigned short*>(o.d4_out)[4 * (int64_t)row + c] = (unsigned short)h16_bits(
+                    (float)(dn * (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z))) * hsc.x);
+            } else if (G32) o.d4_out[4 * (int64_t)row + c] = (float)(H ? dn * (double)(c == 0 ? sqi.x : (c == 1 ? sqi.y : sqi.z)) : dn);
             else o.d_out[o3 + c] = dn;
             const double xn = (MODE == kL0Cheb0 ? vc : xoc) + dn;
             o.xo[o3 + c] = xn;
@@ -1202,6 +1258,21 @@ __device__ __forceinline__ float4 scaled4(const double t[3], const float4* __res
     return make_float4((float)(t[0] * (double)q.x), (float)(t[1] * (double)q.y), (float)(t[2] * (double)q.z), 0.0f);
 }
 
+// Stores node i of a smoother direction: float4 per node, or with the FP16 scaled matrix
+// (sq4 != null) and kL0H16Vec four halves per node (8 bytes), times hs = 2^k, in the same buffer.
+__device__ __forceinline__ void store_dir4(float4* __restrict__ base, int i, const double t[3],
+                                           const float4* __restrict__ sq4, float hs) {
+    const float4 f = scaled4(t, sq4, i);
+    if (kL0H16Vec && sq4) {
+        uint2 u;
+        u.x = h16_bits(f.x * hs) | (h16_bits(f.y * hs) << 16);
+        u.y = h16_bits(f.z * hs);
+        reinterpret_cast<uint2*>(base)[i] = u;
+    } else {
+        base[i] = f;
+    }
+}
+
 // first smoothing step from x = 0 at any level: d = c2 D^-1 b; x = d; r = b
 __global__ void k_cheb_start(int n, int bs, const double* __restrict__ dinv, const double* __restrict__ b,
                              double* __restrict__ r, double* __restrict__ d, double* __restrict__ x, double c2) {
@@ -1220,12 +1291,19 @@ __global__ void k_cheb_start(int n, int bs, const double* __restrict__ dinv, con
 }
 
 // first pre-smoothing step from x = 0: d = c2 D^-1 b; x = d; r = b
-// (d4 != null: the direction as float4 per node instead of d)
+// (d4 != null: the direction as float4 per node instead of d; hs != null: FP16 directions,
+// whose scale for this V-cycle is taken from *rdr = b.D^-1 b and published in hs)
 __global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const double* __restrict__ b,
                                 double* __restrict__ r, double* __restrict__ d, float4* __restrict__ d4,
-                                double* __restrict__ x, double c2, const float4* __restrict__ sq4) {
+                                double* __restrict__ x, double c2, const float4* __restrict__ sq4,
+                                const double* __restrict__ rdr, float* __restrict__ hs) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const float2 hsc = hs ? h16_scale(*rdr) : make_float2(1.0f, 1.0f);
+    if (hs && i == 0) {  // read by the V-cycle's later launches only
+        hs[0] = hsc.x;
+        hs[1] = hsc.y;
+    }
     const int64_t o3 = 3 * (int64_t)i;
     const double bb[3] = {b[o3], b[o3 + 1], b[o3 + 2]};
     const double* D = dinv + 9 * (int64_t)i;
@@ -1236,7 +1314,7 @@ __global__ void k_l0_cheb_start(int n, const double* __restrict__ dinv, const do
         r[o3 + c] = bb[c];
         x[o3 + c] = t[c];
     }
-    if (d4) d4[i] = scaled4(t, sq4, i);
+    if (d4) store_dir4(d4, i, t, sq4, hsc.x);
     else
         for (int c = 0; c < 3; ++c) d[o3 + c] = t[c];
 }
@@ -1261,17 +1339,22 @@ __global__ void k_prolong0(int n, const int32_t* __restrict__ agg, const double*
 
 // The CG update fused with the first step of the V-cycle that follows it:
 // x += alpha p, r -= alpha q, r.D^-1 r reduced by the last CTA into S[2], and
-// with b = the new r: r0 = b, x0 = d = c2 D^-1 b (what k_l0_cheb_start does)
+// with b = the new r: r0 = b, x0 = d = c2 D^-1 b (what k_l0_cheb_start does).
+// hs != null (FP16 directions): the V-cycle's scale comes from S[2] as this launch
+// finds it, the previous residual's r.D^-1 r (the new one is reduced only at the end),
+// and the last CTA publishes it in hs for the V-cycle's later launches.
 __global__ void __launch_bounds__(256) k_amg_update_start(int n, double* __restrict__ S, const double* __restrict__ p,
                                                           const double* __restrict__ q, double* __restrict__ x,
                                                           double* __restrict__ r, const double* __restrict__ dinv,
                                                           double* __restrict__ part, int* __restrict__ counter,
                                                           double* __restrict__ r0, double* __restrict__ x0,
                                                           double* __restrict__ d0, float4* __restrict__ d4,
-                                                          double c2, const float4* __restrict__ sq4) {
+                                                          double c2, const float4* __restrict__ sq4,
+                                                          float* __restrict__ hs) {
     __shared__ double sh[32];
     __shared__ int s_last;
     const double alpha = S[5];
+    const float2 hsc = hs ? h16_scale(S[2]) : make_float2(1.0f, 1.0f);
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int64_t o3 = 3 * (int64_t)i;
@@ -1290,7 +1373,7 @@ __global__ void __launch_bounds__(256) k_amg_update_start(int n, double* __restr
             t[c] = c2 * dr;
             x0[o3 + c] = t[c];
         }
-        if (d4) d4[i] = scaled4(t, sq4, i);
+        if (d4) store_dir4(d4, i, t, sq4, hsc.x);
         else
             for (int c = 0; c < 3; ++c) d0[o3 + c] = t[c];
     }
@@ -1314,6 +1397,10 @@ __global__ void __launch_bounds__(256) k_amg_update_start(int n, double* __restr
     if (lane == 0) {
         S[2] = tt;
         *counter = 0;
+        if (hs) {
+            hs[0] = hsc.x;
+            hs[1] = hsc.y;
+        }
     }
 }
 
@@ -1876,8 +1963,10 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     const int64_t nd = (int64_t)l.n * 3;
     const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
     const unsigned grid = l0_grid(l.n, std::is_same<VT, __half>::value);
-    // FP32 or FP16 values: the smoother's gathered vectors are FP32 (float4 per node)
+    // FP32 or FP16 values: the smoother's gathered vectors are FP32 (float4 per node),
+    // with FP16 values FP16 directions (kL0H16Vec) scaled by the V-cycle's power of two
     constexpr bool g32 = !std::is_same<VT, double>::value;
+    float* hs = std::is_same<VT, __half>::value ? h16_scale_slot() : nullptr;
     double* dA = l.d.ptr;
     double* dB = l.t.ptr;
     float4* dA4 = reinterpret_cast<float4*>(l.d4a.ptr);
@@ -1885,10 +1974,11 @@ void Amg::vcycle0(const VT* vals, const double* b, double* z, double* S, double*
     float4* x4 = reinterpret_cast<float4*>(l.x4.ptr);
     if (!started)
         FX_LAUNCH(k_l0_cheb_start, grid_for(l.n), 256, 0, s, l.n, l.dinv0, b, l.r.ptr, dA, g32 ? dA4 : nullptr,
-                  l.x.ptr, k.c2_start, sq4_);
+                  l.x.ptr, k.c2_start, sq4_, rdr_, hs);
     auto op = [&]() {
         L0Op<VT> o = l0_op<VT>(l, vals);
         o.sq4 = sq4_;
+        o.hs = hs;
         return o;
     };
     for (int st = 1; st < degree_; ++st) {
@@ -1976,8 +2066,12 @@ Amg::Start0 Amg::start0() const {
     o.d4 = vals0_f32_ || vals0_f16_ ? reinterpret_cast<float4*>(l.d4a.ptr) : nullptr;
     o.c2 = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_).c2_start;
     o.sq4 = sq4_;
+    o.hs = vals0_f16_ ? h16_scale_slot() : nullptr;
     return o;
 }
+
+// the scale slot of FP16 smoother directions (null: the directions are FP32, or unscaled)
+float* Amg::h16_scale_slot() const { return kL0H16Vec && rdr_ ? hs_ : nullptr; }
 
 // ------------------------------------------------------------------ AMG-preconditioned CG (FP64)
 
@@ -2061,9 +2155,11 @@ double profile_smoother_op(const BsrStructure& S, const double* vals64, const do
     // compulsory bytes: matrix values + column indices once, row offsets, and per
     // node the gathered direction (24 B FP64 / 16 B float4), r read+write (48), the
     // new direction (24 / 16), iterate read+write (48) and the 3x3 block inverse (72)
-    // (FP16: 2-byte values, and the 16-byte scales of each row)
+    // (FP16: 2-byte values, the 16-byte scales of each row, and with kL0H16Vec 8-byte
+    // directions gathered and written)
     const double vb = fp16 ? 2.0 : (fp32 ? 4.0 : 8.0);
-    *bytes = (double)S.n_blocks * (9.0 * vb + 4.0) + 4.0 * (n + 1) + (fp32 ? 200.0 : 216.0) * n + (fp16 ? 16.0 * n : 0.0);
+    const double per_node = fp16 && kL0H16Vec ? 184.0 : (fp32 ? 200.0 : 216.0);
+    *bytes = (double)S.n_blocks * (9.0 * vb + 4.0) + 4.0 * (n + 1) + per_node * n + (fp16 ? 16.0 * n : 0.0);
     return ms;
 }
 
@@ -2180,6 +2276,8 @@ void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* 
     amg.set_part_slots((int64_t)part_.n);
     sc_.alloc(8, s);
     sc_.zero(s);
+    hs_.alloc(2, s);
+    amg.set_smoother_scale(f16 ? sc_.ptr + 2 : nullptr, f16 ? hs_.ptr : nullptr);  // S[2] = r.D^-1 r
     counter_.alloc(1, s);
     counter_.zero(s);
     // the fused coarse cycle reads the hierarchy from a device descriptor, re-uploaded
@@ -2261,7 +2359,7 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         FX_LAUNCH((k_l0_op<double, kL0Apply>), g0, 256, 0, s, o);  // q = A p, alpha
         const Amg::Start0 s0 = amg.start0();
         FX_LAUNCH(k_amg_update_start, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
-                  counter_.ptr, s0.r, s0.x, s0.d, s0.d4, s0.c2, s0.sq4);  // x, r, r.D^-1 r; the V-cycle's first step
+                  counter_.ptr, s0.r, s0.x, s0.d, s0.d4, s0.c2, s0.sq4, s0.hs);  // x, r, r.D^-1 r; the V-cycle's first step
         amg.apply(r_.ptr, zn, sc_.ptr, part_.ptr, counter_.ptr, amg.kcycle() ? zo : nullptr, s, true);  // z, r.z, beta
         FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, zn, sc_.ptr, p_.ptr);
     };

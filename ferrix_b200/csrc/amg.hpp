@@ -109,6 +109,13 @@ class Amg {
         vals0_f16_ = vals16;
         sq4_ = sq4;
     }
+    // FP16 smoother directions: where the V-cycle started from x = 0 finds r.D^-1 r of its
+    // right-hand side (rdr) and the two floats where each V-cycle publishes its power-of-two
+    // scale of the stored directions (hs); null: unscaled
+    void set_smoother_scale(const double* rdr, float* hs) {
+        rdr_ = rdr;
+        hs_ = hs;
+    }
     // K-cycle at the first coarse level (true) or V-cycles throughout.
     void set_cycle(bool kcycle) { kcycle_ = kcycle; }
     // Chebyshev smoother: 0 = first kind on [lmax/30, lmax], 1 = fourth kind
@@ -132,6 +139,7 @@ class Amg {
         float4* d4;
         double c2;
         const float4* sq4;  // FP16 smoother: the float4 direction is written scaled by sqrt(a_ii)
+        float* hs;          // FP16 directions: where the start publishes the V-cycle's scale (else null)
     };
     Start0 start0() const;
     // the hierarchy, smoother coefficients and work vectors, for the persistent solve
@@ -166,6 +174,9 @@ class Amg {
     const float* vals0_f32_ = nullptr;
     const __half* vals0_f16_ = nullptr;
     const float4* sq4_ = nullptr;
+    const double* rdr_ = nullptr;
+    float* hs_ = nullptr;
+    float* h16_scale_slot() const;
     bool fused_coarse_ = false;
     double* gflag_ = nullptr;
     DBuf<ClInst> desc_;
@@ -269,6 +280,7 @@ class AmgPcg {
     DBuf<float> vals32_;
     DBuf<__half> vals16_;
     DBuf<float4> sq4_;
+    DBuf<float> hs_;  // FP16 smoother directions: the current V-cycle's {2^k, 2^-k}
     DBuf<int> counter_;
 };
 
