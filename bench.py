@@ -710,8 +710,11 @@ def main():
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         ke = max(1, args.steps)  # as many steps as the device-resident timing
+        e2e_steps = []  # host wall time of each step (each ends with the D2H read of u)
         for _ in range(ke):
+            h0 = time.perf_counter()
             e2e_step()
+            e2e_steps.append((time.perf_counter() - h0) * 1e3)
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_elapsed = e0.elapsed_time(e1) / 1e3 / ke
@@ -821,7 +824,11 @@ def main():
             "clocks": clk,
             "e2e": {"value": 1.0 / e2e_elapsed if e2e_elapsed else None, "unit": "solves/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "ms_per_step": e2e_elapsed * 1e3 if e2e_elapsed else None},
+                    "ms_per_step": e2e_elapsed * 1e3 if e2e_elapsed else None,
+                    # the spread shows a stall of the shared host (one slow step) apart from a slow path
+                    "step_ms": {"median": round(statistics.median(e2e_steps), 2),
+                                "min": round(min(e2e_steps), 2), "max": round(max(e2e_steps), 2)}
+                    if e2e_elapsed else None},
             "cpu_baseline": cpu,
             "batch": batch_line,
             "serving": serving_line,

@@ -617,9 +617,7 @@ __global__ void k_dense_matvec(int nd, const double* __restrict__ A, const doubl
                                double* __restrict__ y) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= nd) return;
-    double t = 0.0;
-    for (int c = lane; c < nd; c += 32) t += A[(int64_t)warp * nd + c] * x[c];
-    t = warp_sum(t);
+    const double t = dense_row_dot<false>(A + (int64_t)warp * nd, x, nd, lane);
     if (lane == 0) y[warp] = t;
 }
 
@@ -1156,20 +1154,26 @@ __global__ void __launch_bounds__(1024) k_kcycle2(int64_t n, const double* __res
 }
 
 // ---- coarse levels (row-major 6x6 block CSR): SpMV fused with the smoother
-// update, one warp per block row, lanes over the row's blocks; the same modes as
-// the fine-level operator (kL0Resid, kL0RUpd, kL0Cheb0, kL0ChebK).
+// update, one warp per block row, a lane per block of the row (coarse_row6); the
+// same modes as the fine-level operator (kL0Resid, kL0RUpd, kL0Cheb0, kL0ChebK).
 // Threads per CTA of the coarse-level kernels (warp per block row / aggregate).
 #ifndef FX_LN_THREADS
 #define FX_LN_THREADS 128
 #endif
 constexpr int kLnThreads = FX_LN_THREADS;
-// Column-gather chains in flight per lane of the coarse-level operators (2: 64 registers;
-// on the 417k-DOF box a default solve took 54.6-55.0 ms against 55.0-55.7 with 4 and
-// 55.5-55.9 with 1).
-#ifndef FX_LN_IN_FLIGHT
-#define FX_LN_IN_FLIGHT 2
+// CTAs per SM the coarse-level operators are compiled for: 4 x 128 threads leaves 128
+// registers, enough for a lane's whole 6x6 block and its gathered 6-vector in flight
+// without spills. On the 417k-DOF box a default solve took 51.9-52.4 ms with 4, against
+// 52.9-53.2 with 6 (80 registers), 52.5-53.2 with 7 (72, spilling) and 52.3-52.5 with 8
+// (64, the epilogue operands loaded after the row sums, FX_LN_LATE_EPI).
+#ifndef FX_LN_MIN_BLOCKS
+#define FX_LN_MIN_BLOCKS 4
 #endif
-constexpr int kLnInFlight = FX_LN_IN_FLIGHT;
+constexpr int kLnMinBlocks = FX_LN_MIN_BLOCKS;
+#ifndef FX_LN_LATE_EPI
+#define FX_LN_LATE_EPI 0
+#endif
+constexpr bool kLnLateEpi = FX_LN_LATE_EPI != 0;  // epilogue operands loaded after the row sums
 
 struct LnOp {
     int n;
@@ -1187,14 +1191,15 @@ struct LnOp {
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(256) k_ln_op(LnOp o) {
+__global__ void __launch_bounds__(kLnThreads, kLnMinBlocks) k_ln_op(LnOp o) {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (row >= o.n) return;  // warp-uniform
     const int64_t o6 = 6 * (int64_t)row;
     const int c = lane < 6 ? lane : 0;
     const bool epi = lane < 6;
     double src6[6] = {0, 0, 0, 0, 0, 0}, Dr[6] = {0, 0, 0, 0, 0, 0}, vc = 0.0, xoc = 0.0, bc = 0.0;
-    if (epi) {  // row-local operands, loaded before the gathers
+    auto load_epi = [&]() {  // row-local operands of the epilogue
+    if (epi) {
         if (MODE == kL0Cheb0 || MODE == kL0ChebK) {
             const double* src = MODE == kL0Cheb0 ? o.b : o.r;
 #pragma unroll
@@ -1210,21 +1215,13 @@ __global__ void __launch_bounds__(256) k_ln_op(LnOp o) {
             src6[0] = o.r[o6 + c];
         }
     }
-    // 30 lanes walk (block, block row) items: lane l always handles block row l % 6
-    // of blocks l / 6 + 5 m, so consecutive lanes read consecutive 48-B block rows
-    const int b0 = o.row_ptr[row], items = 6 * (o.row_ptr[row + 1] - b0);
-    double t = coarse_row_part<false, kLnInFlight>(o.cols, o.vals, o.v, b0, items, lane);
-    // lanes r, r+6, ..., r+24 hold block-row r partial sums: fixed-order tree into lanes 0..5
-    // (a source lane past 31 returns the caller's own value, hence the lane conditions)
-    double u = __shfl_down_sync(0xffffffffu, t, 24);
-    if (lane < 8) t += u;  // lanes 0..5 += 24..29 (6, 7 += 30, 31, which carry 0)
-    u = __shfl_down_sync(0xffffffffu, t, 12);
-    if (lane < 12) t += u;  // lanes 0..11 += 12..23
-    u = __shfl_down_sync(0xffffffffu, t, 6);
-    if (lane < 6) t += u;  // lanes 0..5 += 6..11
+    };
+    if (!kLnLateEpi) load_epi();
+    // lanes over the row's blocks; every lane ends with the six row sums
+    const int b0 = o.row_ptr[row];
     double acc[6];
-#pragma unroll
-    for (int r = 0; r < 6; ++r) acc[r] = __shfl_sync(0xffffffffu, t, r);
+    coarse_row6<false>(o.cols, o.vals, o.v, b0, o.row_ptr[row + 1] - b0, lane, acc);
+    if (kLnLateEpi) load_epi();
     double axc = acc[0];
 #pragma unroll
     for (int r = 1; r < 6; ++r)
@@ -1882,6 +1879,10 @@ void Amg::cycle(int lev, const double* b, double* x, cudaStream_t s, bool starte
         return;
     }
     AmgLevel& c = L[lev + 1];
+    // coarse_row6 reads the 6x6 blocks and the gathered 6-vectors as 16-byte pairs
+    if ((reinterpret_cast<uintptr_t>(l.vals.ptr) | reinterpret_cast<uintptr_t>(l.d.ptr) |
+         reinterpret_cast<uintptr_t>(l.t.ptr) | reinterpret_cast<uintptr_t>(l.xs.ptr)) & 15)
+        fail(FX_GENERIC, "multigrid: coarse-level buffers not 16-byte aligned");
     const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
     const unsigned grid = grid_for((int64_t)l.n * 32, kLnThreads);
     double* dA = l.d.ptr;
@@ -2212,6 +2213,10 @@ void Amg::describe(ClInst& o) const {
         c.d = l.d.ptr;
         c.t = l.t.ptr;
         c.xs = l.xs.ptr;
+        for (const void* q : {(const void*)c.vals, (const void*)c.x, (const void*)c.b, (const void*)c.d,
+                              (const void*)c.t, (const void*)c.xs})
+            if (reinterpret_cast<uintptr_t>(q) & 15)  // coarse_row6's 16-byte loads
+                fail(FX_GENERIC, "multigrid: coarse-level buffers not 16-byte aligned");
         if (!l.coarsest) {
             const ChebCoef k = cheb_coef(l.lmax, degree_, cheb_kind_, cheb_ratio_);
             c.c2_start = k.c2_start;

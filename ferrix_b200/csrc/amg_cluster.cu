@@ -233,17 +233,9 @@ __device__ __noinline__ void ln_op(const ClLevel& L, Vg g, const double* v, cons
                 src6[0] = ldv(r + o6 + c);
             }
         }
-        const int b0 = __ldg(L.row_ptr + row), items = 6 * (__ldg(L.row_ptr + row + 1) - b0);
-        double t = coarse_row_part<true, 4>(L.cols, L.vals, v, b0, items, lane);
-        double u = __shfl_down_sync(0xffffffffu, t, 24);
-        if (lane < 8) t += u;
-        u = __shfl_down_sync(0xffffffffu, t, 12);
-        if (lane < 12) t += u;
-        u = __shfl_down_sync(0xffffffffu, t, 6);
-        if (lane < 6) t += u;
+        const int b0 = __ldg(L.row_ptr + row);
         double acc[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) acc[k] = __shfl_sync(0xffffffffu, t, k);
+        coarse_row6<true>(L.cols, L.vals, v, b0, __ldg(L.row_ptr + row + 1) - b0, lane, acc);
         double axc = acc[0];
 #pragma unroll
         for (int k = 1; k < 6; ++k)
@@ -357,9 +349,7 @@ __device__ __noinline__ void prolong0_op(Vg g, const ClInst& I, const double* xc
 __device__ __noinline__ void dense_op(Vg g, int nd, const double* A, const double* x, double* y) {
     const int lane = g.t & 31;
     for (int row = g.t >> 5; row < nd; row += g.nt >> 5) {
-        double t = 0.0;
-        for (int c = lane; c < nd; c += 32) t += __ldg(A + (int64_t)row * nd + c) * ldv(x + c);
-        t = warp_sum(t);
+        const double t = dense_row_dot<true>(A + (int64_t)row * nd, x, nd, lane);
         if (lane == 0) y[row] = t;
     }
 }
