@@ -853,6 +853,13 @@ __device__ __forceinline__ void cta_dot_finalize(double v, double v2, int mode, 
 #define FX_L0_MIN_BLOCKS 2
 #endif
 constexpr int kL0MinBlocks = FX_L0_MIN_BLOCKS;  // 256-thread CTAs resident per SM (2: at most 128 registers)
+// The outer CG's q = K p (FP64 values, mode kL0Apply) compiled for its own CTAs per SM (2: on
+// the 417k-DOF box a default solve took 51.5-51.7 ms, against 53.4 with 3 (80 registers)
+// and 55.0 with 4 (64 registers, spilling))
+#ifndef FX_L0_MIN_BLOCKS_APPLY
+#define FX_L0_MIN_BLOCKS_APPLY 2
+#endif
+constexpr int kL0MinBlocksApply = FX_L0_MIN_BLOCKS_APPLY;
 // FP16 values: its loads are half as wide as the FP32 form's, so it is latency-bound and
 // needs more warps and more loads in flight. Measured per Chebyshev step on the 417k-DOF
 // C3D20 box (B200): 57.7 us at 2 CTAs per SM; 54.8 at 3 (85 registers); 61.5 at 4 with
@@ -879,6 +886,13 @@ constexpr int kL0MinBlocksH = FX_L0_MIN_BLOCKS_H;
 #define FX_L0_H16VEC 1
 #endif
 constexpr bool kL0H16Vec = FX_L0_H16VEC != 0;
+// With the FP16 smoother, the level-0 eigenvalue estimate's products also come from the FP16
+// scaled matrix (1); else from an FP32 copy of the FP64 values made for it (0). On the
+// 417k-DOF box: multigrid setup 5.17 -> 4.92 ms, the same 100 CG iterations.
+#ifndef FX_AMG_EST_F16
+#define FX_AMG_EST_F16 1
+#endif
+constexpr bool kAmgEstF16 = FX_AMG_EST_F16 != 0;
 // the stored directions' 2-norm is about 2^kH16Exp: a direction entry overflows only if the
 // residual grows by about 2^(15 - kH16Exp) from one outer iteration to the next, and the
 // entries of a vector of 1e7 nodes still sit ~10 binades above the smallest normal FP16
@@ -917,7 +931,8 @@ constexpr int kL0Unroll = FX_L0_UNROLL;  // groups of a row in flight per lane
 // o.d4_out; the row's own FP64 values still come from o.v where the mode needs
 // them (Cheb0: the iterate), else from o.v4.
 template <typename VT, int MODE, bool G32 = false>
-__global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinBlocksH : kL0MinBlocks)
+__global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinBlocksH
+                                      : (MODE == kL0Apply ? kL0MinBlocksApply : kL0MinBlocks))
     k_l0_op(L0Op<VT> o) {
     // FP16 values (of the scaled matrix): FP32 gathers of the scaled vectors, row sums
     // scaled back by sqrt(a_ii), directions written scaled
@@ -929,7 +944,7 @@ __global__ void __launch_bounds__(256, std::is_same<VT, __half>::value ? kL0MinB
     // FP16 directions: written by the Chebyshev steps, gathered by all but the step from
     // the (FP32) iterate; 2^-k is applied to the row sums, after the gathers
     constexpr bool kH16 = H && G32 && kL0H16Vec;
-    constexpr bool kH16g = kH16 && MODE != kL0Cheb0;
+    constexpr bool kH16g = kH16 && (MODE == kL0ChebK || MODE == kL0RUpd);
     const int sub = threadIdx.x & (kL0Lanes - 1);
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) >> kL0LaneShift;
     const int rows_per_grid = (gridDim.x * blockDim.x) >> kL0LaneShift;
@@ -1270,6 +1285,15 @@ __device__ __forceinline__ void store_dir4(float4* __restrict__ base, int i, con
     }
 }
 
+// x4[i] = the float4 of node i's three components scaled by sqrt(a_ii) (the FP16
+// operator's gathered vector), from an FP64 vector
+__global__ void k_scaled4(int n, const double* __restrict__ x, const float4* __restrict__ sq4, float4* __restrict__ x4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double t[3] = {x[3 * (int64_t)i], x[3 * (int64_t)i + 1], x[3 * (int64_t)i + 2]};
+    x4[i] = scaled4(t, sq4, i);
+}
+
 // first smoothing step from x = 0 at any level: d = c2 D^-1 b; x = d; r = b
 __global__ void k_cheb_start(int n, int bs, const double* __restrict__ dinv, const double* __restrict__ b,
                              double* __restrict__ r, double* __restrict__ d, double* __restrict__ x, double c2) {
@@ -1465,27 +1489,32 @@ __global__ void k_f64_to_f32(int64_t n, const double* __restrict__ a, float* __r
 // ------------------------------------------------------------------ host side
 
 // Grid of the level-0 operators: at most one wave of resident CTAs (grid-stride rows);
-// h: the FP16-value kernels, which have their own register budget.
-static unsigned l0_grid(int n, bool h = false) {
-    thread_local int cached_dev = -1, cached_cap[2] = {0, 0};  // per host thread: contexts live on one thread each
+// h: the FP16-value kernels, which have their own register budget; apply: the outer CG's
+// FP64 q = K p (kL0MinBlocksApply).
+static unsigned l0_grid(int n, bool h = false, bool apply = false) {
+    thread_local int cached_dev = -1, cached_cap[3] = {0, 0, 0};  // per host thread: contexts live on one thread each
     int dev = 0;
     FX_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev != cached_dev) {
-        int sms = 0, per_sm = 0, per_sm_h = 0;
+        int sms = 0, per_sm = 0, per_sm_h = 0, per_sm_a = 0;
         FX_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_l0_op<double, kL0ChebK>, 256, 0));
         FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_h, k_l0_op<__half, kL0ChebK, true>, 256,
                                                                     0));
+        FX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, k_l0_op<double, kL0Apply>, 256, 0));
         cached_cap[0] = std::max(1, sms * std::max(1, per_sm));
         cached_cap[1] = std::max(1, sms * std::max(1, per_sm_h));
+        cached_cap[2] = std::max(1, sms * std::max(1, per_sm_a));
         cached_dev = dev;
     }
-    return (unsigned)std::min<int64_t>(grid_for((int64_t)n * kL0Lanes), cached_cap[h ? 1 : 0]);
+    return (unsigned)std::min<int64_t>(grid_for((int64_t)n * kL0Lanes), cached_cap[apply ? 2 : (h ? 1 : 0)]);
 }
 
 // Slots of the partial-sum buffer a level-0 operator with a dot product needs: two per CTA
 // of the largest level-0 grid (the FP16 kernels run more CTAs per SM than the others).
-static int64_t l0_part_slots(int n) { return 2 * (int64_t)std::max(l0_grid(n, false), l0_grid(n, true)); }
+static int64_t l0_part_slots(int n) {
+    return 2 * (int64_t)std::max({l0_grid(n, false), l0_grid(n, true), l0_grid(n, false, true)});
+}
 
 template <typename VT>
 static L0Op<VT> l0_op(const AmgLevel& l, const VT* vals) {
@@ -1521,10 +1550,12 @@ static void dot_dev(const double* a, const double* b, int64_t n, DBuf<double>& r
 
 // Largest eigenvalue of D^-1 A by 12 power iterations from a fixed hashed start
 // vector, normalised on the device; one host read at the end.
-// (vals32: FP32 copy of the fine matrix, used for the products at level 0 when given)
+// (level 0: with vals16 / sq4 the products come from the FP16 scaled matrix the smoother
+// reads, through float4 copies of x in l.x4; else from vals32, an FP32 copy, when given)
 // warm: start from the vector the previous estimate on this level ended with (a
 // refresh after a small change of the matrix) and iterate 4 times instead of 12.
-static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const float* vals32, bool warm) {
+static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const float* vals32, bool warm,
+                          const __half* vals16 = nullptr, const float4* sq4 = nullptr) {
     const int64_t nd = (int64_t)l.n * l.bs;
     const int nb = 296;
     const bool from_ev = warm && l.ev.n == (size_t)nd;
@@ -1536,7 +1567,15 @@ static void estimate_lmax(AmgLevel& l, DBuf<double>& red, cudaStream_t s, const 
     FX_LAUNCH(k_normalize, grid_for(nd), 256, 0, s, nd, red.ptr + nb, l.x.ptr, l.x.ptr);
     const int iters = from_ev ? 4 : 12;
     for (int it = 0; it < iters; ++it) {
-        if (l.S0 && vals32) {  // t = A x, |x| = 1
+        if (l.S0 && vals16 && sq4) {  // t = A x, |x| = 1, from the FP16 scaled matrix
+            float4* x4 = reinterpret_cast<float4*>(l.x4.ptr);
+            FX_LAUNCH(k_scaled4, grid_for(l.n), 256, 0, s, l.n, l.x.ptr, sq4, x4);
+            L0Op<__half> o = l0_op<__half>(l, vals16);
+            o.v4 = x4;
+            o.y = l.t.ptr;
+            o.sq4 = sq4;
+            FX_LAUNCH((k_l0_op<__half, kL0Resid, true>), l0_grid(l.n, true), 256, 0, s, o);
+        } else if (l.S0 && vals32) {  // t = A x, |x| = 1
             L0Op<float> o = l0_op<float>(l, vals32);
             o.v = l.x.ptr;
             o.y = l.t.ptr;
@@ -1664,7 +1703,8 @@ void Amg::setup(const BsrStructure& S0, const double* vals0, const double* dinv0
             coarsest_inverse(l, s);
             break;
         }
-        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr, false);
+        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr, false,
+                      lev == 0 && kAmgEstF16 ? vals0_f16_ : nullptr, sq4_);
         // ---- aggregation by cells
         DBuf<uint64_t> keys, keys_s;
         DBuf<int32_t> ids, ids_s, head, rank1;
@@ -1796,7 +1836,8 @@ void Amg::refresh(const double* vals0, const double* dinv0, cudaStream_t s, AmgS
             coarsest_inverse(l, s);
             break;
         }
-        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr, true);
+        estimate_lmax(l, red_, s, lev == 0 ? vals0_f32_ : nullptr, true,
+                      lev == 0 && kAmgEstF16 ? vals0_f16_ : nullptr, sq4_);
         galerkin(l, L[lev + 1], s);
     }
     if (st) {
@@ -2228,11 +2269,6 @@ void Amg::describe(ClInst& o) const {
     }
 }
 
-#ifndef FX_AMG_EST32
-#define FX_AMG_EST32 1
-#endif
-constexpr bool kAmgEst32 = FX_AMG_EST32 != 0;
-
 void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* dinv64, const double* xyz,
                      double cell0, const PcgOptions& opt, cudaStream_t s, AmgStats* st, bool reuse, bool persistent) {
     const int n = S.n_rows;
@@ -2240,17 +2276,16 @@ void AmgPcg::prepare(const BsrStructure& S, const double* vals64, const double* 
     if (opt.amg_degree < 1 || opt.amg_degree > 8) fail(FX_INVALID_ARGUMENT, "multigrid smoother degree must be 1..8");
     const float* v32 = nullptr;
     const bool f16 = opt.amg_fp32 && opt.amg_fp16 && !persistent;
-    if (f16) {  // FP16 values of S A S and the scales; the eigenvalue estimates use the FP64 matrix
+    if (f16) {  // FP16 values of S A S and the scales
         sq4_.alloc((size_t)n, s);
         FX_LAUNCH(k_diag_sqrt, grid_for(n), 256, 0, s, n, S.goff.ptr, S.diag_k.ptr, vals64, sq4_.ptr);
         vals16_.alloc((size_t)S.n_groups * 36, s);
         FX_LAUNCH(k_vals_to_f16, grid_for((int64_t)n * 32), 256, 0, s, n, S.goff.ptr, S.cols.ptr, vals64, sq4_.ptr,
                   vals16_.ptr);
     }
-    // FP32 values: the FP32 smoother's; with the FP16 smoother they still serve the level-0
-    // eigenvalue estimates (kAmgEst32), whose power iterations read them instead of the
-    // FP64 values
-    if (opt.amg_fp32 && (!f16 || kAmgEst32)) {
+    // FP32 values: the FP32 smoother's; with the FP16 smoother only when the level-0
+    // eigenvalue estimate reads them (kAmgEstF16 off) instead of the FP16 values
+    if (opt.amg_fp32 && (!f16 || !kAmgEstF16)) {
         const int64_t nv = (int64_t)S.n_groups * 36;
         vals32_.alloc(nv, s);
         FX_LAUNCH(k_f64_to_f32, 148 * 8, 256, 0, s, nv, vals64, vals32_.ptr);
@@ -2333,7 +2368,7 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     const int64_t nd = 3 * (int64_t)n;
     prepare(S, vals64, dinv64, xyz, cell0, opt, s, st, reuse);
     const int nb = 296;
-    const unsigned g0 = l0_grid(n);
+    const unsigned g0 = l0_grid(n, false, true);  // q = K p
     if (2 * (int64_t)g0 > (int64_t)part_.n) fail(FX_GENERIC, "multigrid: partial-sum buffer smaller than the CG grid");
     FX_CUDA_CHECK(cudaMemsetAsync(x, 0, nd * sizeof(double), s));
     FX_CUDA_CHECK(cudaMemcpyAsync(r_.ptr, b, nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
