@@ -11,6 +11,11 @@
 // error. Case folding is ASCII (decks are ASCII).
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -219,6 +224,92 @@ double Record::eval(const SolverTime& t, int64_t current_step) const {  // ampli
     return y * value;
 }
 
+// ------------------------------------------------------------------ host workers
+// The parser's parallel loops run on worker threads that are started once per process
+// (up to 15) and kept, instead of threads started and joined per loop (five loops per
+// deck, each paying for its threads' creation). A loop is a job whose tasks are claimed
+// through an atomic counter by the calling thread, which always works on its own job,
+// and by the workers that take one of its helper entries from the queue; so concurrent
+// callers (request-loop slots) share the workers, and a caller finishes its job even
+// when no worker is free (or, in a forked child, none exists).
+namespace {
+struct HostJob {
+    std::function<void(size_t)> f;
+    size_t ntasks = 0;
+    std::atomic<size_t> next{0}, done{0};
+    std::mutex m;
+    std::condition_variable cv;
+    void work() {
+        for (size_t t; (t = next.fetch_add(1)) < ntasks;) {
+            f(t);
+            if (done.fetch_add(1) + 1 == ntasks) {
+                std::lock_guard<std::mutex> g(m);
+                cv.notify_all();
+            }
+        }
+    }
+};
+
+class HostPool {
+   public:
+    static HostPool& get() {
+        static HostPool* p = new HostPool();  // never destroyed: its workers wait on it until exit
+        return *p;
+    }
+    size_t threads() const { return 1 + nworkers_; }
+    // f(0 .. ntasks-1), each once, on the caller and up to max_threads - 1 workers
+    void run(size_t ntasks, size_t max_threads, std::function<void(size_t)> f) {
+        if (ntasks == 0) return;
+        auto job = std::make_shared<HostJob>();
+        job->f = std::move(f);
+        job->ntasks = ntasks;
+        const size_t helpers = std::min<size_t>({max_threads, ntasks, threads()}) - 1;
+        if (helpers) {
+            std::lock_guard<std::mutex> g(m_);
+            for (size_t k = 0; k < helpers; ++k) q_.push_back(job);
+            cv_.notify_all();
+        }
+        job->work();
+        std::unique_lock<std::mutex> g(job->m);
+        job->cv.wait(g, [&] { return job->done.load() == ntasks; });
+    }
+
+   private:
+    HostPool() {
+        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        nworkers_ = hw - 1;
+        for (size_t k = 0; k < nworkers_; ++k) std::thread([this] { loop(); }).detach();
+    }
+    void loop() {
+        for (;;) {
+            std::shared_ptr<HostJob> job;
+            {
+                std::unique_lock<std::mutex> g(m_);
+                cv_.wait(g, [&] { return !q_.empty(); });
+                job = std::move(q_.front());
+                q_.pop_front();
+            }
+            job->work();
+        }
+    }
+    size_t nworkers_ = 0;
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::deque<std::shared_ptr<HostJob>> q_;
+};
+}  // namespace
+
+// Runs f(0..ntasks-1), each task once, on up to max_threads threads (the calling thread
+// works too; the pool has at most 16).
+template <typename F>
+static void parallel_tasks(size_t ntasks, F&& f, size_t max_threads = 16) {
+    if (ntasks <= 1 || max_threads <= 1) {
+        for (size_t t = 0; t < ntasks; ++t) f(t);
+        return;
+    }
+    HostPool::get().run(ntasks, max_threads, std::function<void(size_t)>(std::ref(f)));
+}
+
 // ------------------------------------------------------------------ preprocess
 
 // Trimmed, comment-free, upper-cased lines of text[begin, end) (a range of
@@ -354,16 +445,7 @@ static void preprocess_lines(std::string_view text, std::unique_ptr<char[]>& sto
     store.reset(new char[n + 1]);  // a chunk's output is never longer than its input (+1 for the last)
     char* out = store.get();
     std::vector<size_t> len(nthreads, 0), nlines(nthreads, 0), first(nthreads + 1, 0);
-    auto run = [&](auto&& fn) {
-        if (nthreads == 1) {
-            fn((size_t)0);
-            return;
-        }
-        std::vector<std::thread> th;
-        for (size_t t = 1; t < nthreads; ++t) th.emplace_back(fn, t);
-        fn((size_t)0);
-        for (auto& x : th) x.join();
-    };
+    auto run = [&](auto&& fn) { parallel_tasks(nthreads, fn, nthreads); };
     run([&](size_t t) {
         len[t] = preprocess_range(text, cut[t], cut[t + 1], out, cut[t]) - cut[t];
         len[t] = substitute_solvers(out + cut[t], len[t]);
@@ -403,25 +485,6 @@ struct PreBlock {
     RawVec<std::array<double, 3>> xyz;  // *NODE
     RawVec<int64_t> conn;               // *ELEMENT: npe per line
 };
-
-// Runs f(0..ntasks-1) on up to 16 threads, each task once (the calling thread works too).
-template <typename F>
-static void parallel_tasks(size_t ntasks, F&& f) {
-    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const size_t nthreads = std::min<size_t>(hw, ntasks);
-    std::atomic<size_t> next{0};
-    auto work = [&]() {
-        for (size_t t; (t = next.fetch_add(1)) < ntasks;) f(t);
-    };
-    if (nthreads <= 1) {
-        work();
-        return;
-    }
-    std::vector<std::thread> th;
-    for (size_t t = 1; t < nthreads; ++t) th.emplace_back(work);
-    work();
-    for (auto& x : th) x.join();
-}
 
 // Parses every block's lines into its arrays: tasks of up to 2,048 lines of
 // any block, taken in turn by up to 16 threads (each writes only its lines'
