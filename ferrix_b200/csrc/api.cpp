@@ -340,6 +340,7 @@ int fx_state_set_displacements(fx_model* m, const double* u) {
     if (!m || !u || !m->state_ready) return FX_INVALID_ARGUMENT;
     return guarded(m->ctx, [&] {
         FX_CUDA_CHECK(cudaSetDevice(m->ctx->device));
+        m->dev.u_zero = false;
         FX_CUDA_CHECK(cudaMemcpyAsync(m->dev.u.ptr, u, 3 * (size_t)m->dense.n_nodes * sizeof(double),
                                       cudaMemcpyHostToDevice, m->ctx->stream));
         FX_CUDA_CHECK(cudaStreamSynchronize(m->ctx->stream));

@@ -192,6 +192,7 @@ void state_initialize(fx_model* m) {
     } else {
         upload_model(m);
     }
+    m->dev.u_zero = true;
     m->state_ready = true;
 }
 
@@ -292,6 +293,7 @@ struct StepRunner {
     double cur = 0.0, dt = 0.0;
     int64_t n_inc = 0;
     int it = 0;
+    bool ustart_zero = false;  // no increment has converged yet and the step started from u = 0
     enum { kNewInc, kIter, kDone } state = kNewInc;
     bool need_solve = false;
     // host callback after every converged increment (fx_step_solve_cb), else null
@@ -379,6 +381,7 @@ struct StepRunner {
         n_inc = 0;
         dt = step->inc.initial;
         FX_CUDA_CHECK(cudaMemcpyAsync(d.ustart.ptr, d.u.ptr, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        ustart_zero = d.u_zero;
         state = kNewInc;
     }
 
@@ -426,7 +429,14 @@ struct StepRunner {
             compute_thermal_force(m, d.ftmp.ptr);
             launch_axpby((int64_t)n3, 1.0, d.fext.ptr, 1.0, d.ftmp.ptr, d.fext.ptr, s);
         }
-        compute_internal_force(m, ucur.ptr, step->nlgeom ? ucur.ptr : nullptr, d.fint.ptr);
+        if (it == 0 && ustart_zero && !step->nlgeom && !m->dense.any_expansion) {
+            // ucur is a copy of the all-zero ustart and no strain is thermal: every term of
+            // f_int = sum B^T D (B u - eps_th) is a zero, so the element pass is skipped (R =
+            // f_ext - f_int has the same bits for either sign of those zeros)
+            d.fint.zero(s);
+        } else {
+            compute_internal_force(m, ucur.ptr, step->nlgeom ? ucur.ptr : nullptr, d.fint.ptr);
+        }
         launch_axpby((int64_t)n3, 1.0, d.fext.ptr, -1.0, d.fint.ptr, d.R.ptr, s);
         launch_masked_norms((int64_t)n3, d.R.ptr, d.fext.ptr, bc.d_mask.ptr, d.norm_part.ptr, d.norm_out.ptr, s);
         FX_CUDA_CHECK(cudaMemcpyAsync(nrm, d.norm_out.ptr, sizeof(nrm), cudaMemcpyDeviceToHost, s));
@@ -445,11 +455,13 @@ struct StepRunner {
             const size_t n3 = 3 * (size_t)m->dense.n_nodes;
             FX_CUDA_CHECK(cudaMemcpyAsync(m->dev.ustart.ptr, ucur.ptr, n3 * sizeof(double), cudaMemcpyDeviceToDevice,
                                           m->ctx->stream));
+            ustart_zero = false;
             state = kNewInc;
             need_solve = false;
             if (inc_cb) {  // the converged increment's result (static_step.rs:219-248: write_increment)
                 FX_CUDA_CHECK(cudaMemcpyAsync(m->dev.u.ptr, m->dev.ustart.ptr, n3 * sizeof(double),
                                               cudaMemcpyDeviceToDevice, m->ctx->stream));
+                m->dev.u_zero = false;
                 stream_wait(m->ctx->stream, "increment result");
                 const int rc = inc_cb(inc_user, m, step_id, (int)n_inc, m->timer.global);
                 if (rc != 0) fail(FX_GENERIC_IO, "Generic IO error: increment callback returned " + std::to_string(rc));
@@ -589,6 +601,7 @@ struct StepRunner {
         const size_t n3 = 3 * (size_t)m->dense.n_nodes;
         FX_CUDA_CHECK(cudaMemcpyAsync(m->dev.u.ptr, m->dev.ustart.ptr, n3 * sizeof(double),
                                       cudaMemcpyDeviceToDevice, m->ctx->stream));
+        m->dev.u_zero = false;
         S.bsr_blocks = m->dev.S.n_blocks;
         state = kDone;
     }

@@ -61,6 +61,7 @@ struct ModelDev {
     DBuf<float> ebuf32, vals32, minv32;
     DBuf<double> ebuf64, vals64, minv64;
     DBuf<double> fe, u, ustart, du, fext, ftmp, fint, R, r64, ax;
+    bool u_zero = false;  // u is all zeros: set by the state reset, cleared by every other write of u
     DBuf<unsigned long long> maxdiag;
     DBuf<int> err;
     DBuf<double> norm_part, norm_out;
