@@ -135,6 +135,17 @@ static bool parse_usize_sv(std::string_view s, int64_t* out) {  // usize::from_s
 
 // f64::from_str without allocation: same accepted forms as parse_f64 below.
 static bool parse_f64_sv(std::string_view s, double* out) {
+    // the usual decimal forms: a complete, finite from_chars parse (no leading '+', which
+    // from_chars does not take; inf / nan spellings and out-of-range values are not finite
+    // or fail, and go through the checks below)
+    if (!s.empty() && s.size() <= 64 && s[0] != '+') {
+        double v = 0.0;
+        const auto r = std::from_chars(s.data(), s.data() + s.size(), v);
+        if (r.ec == std::errc() && r.ptr == s.data() + s.size() && std::isfinite(v)) {
+            *out = v;
+            return true;
+        }
+    }
     if (s.empty() || s.size() > 64) {
         if (s.empty()) return false;
         return parse_f64_slow(std::string(s), out);

@@ -64,7 +64,7 @@ def _compare(text):
     if m is not None:
         assert np.array_equal(p.mesh.index_to_node_id, m.node_ids)
         xyz, groups = p.export()
-        assert np.array_equal(xyz, m.xyz)
+        assert np.array_equal(xyz, m.xyz, equal_nan=True)
         for npe in (4, 20):
             conn, mat = groups[npe]
             if npe in m.groups:
@@ -206,6 +206,14 @@ EDGE_DECKS = {
                     "1,1,2,3,4\n1,2,1,3,4\n",
     "element_without_type": "*NODE\n1,0,0,0\n*ELEMENT\n1,1,1,1,1\n",  # data dropped
     "plus_sign_and_exponents": "*NODE\n+1,1E3,-2.5e-2,+3.\n2,inf,0,0\n",
+    # f64::from_str forms beside plain decimals: NaN / infinity spellings, out-of-range
+    # magnitudes (to inf and to zero), a bare fraction or integer part, a negative zero
+    "float_forms": "*NODE\n1,.5,5.,-0\n2,1e999,-1e-400,NaN\n3,infinity,-Inf,1E+05\n4,-.25e1,+0.0,7\n",
+    # the same forms in a block of 1,100 lines (the bulk parse of *NODE data)
+    "float_forms_bulk": "*NODE\n" + "".join(
+        "%d,%s,%s,%s\n" % (i + 1, ("0.1", ".5", "1e999", "NaN", "-Inf", "+2.5")[i % 6],
+                             ("5.", "-1e-400", "3", "-0", "1E+05", "infinity")[i % 6], repr(i * 0.37))
+        for i in range(1100)),
 }
 
 
