@@ -2384,6 +2384,10 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
     const AmgLevel& l0 = amg.L[0];
     // flexible CG (the K-cycle makes the preconditioner vary slightly between
     // iterations): z alternates between two buffers so that r.z_old is at hand
+    // the CG update and p = z + beta p with a thread per node / entry (all of them in
+    // flight at once), the update's grid within the partial-sum slots it reduces into
+    const unsigned gu = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(n), (int64_t)part_.n));
+    const unsigned gx = (unsigned)std::min<int64_t>(grid_for(nd), 4096);
     int parity = 0;
     auto iteration = [&]() {
         double* zn = parity ? z_.ptr : z2_.ptr;
@@ -2398,10 +2402,10 @@ int AmgPcg::solve(const BsrStructure& S, const double* vals64, const double* din
         o.S = sc_.ptr;
         FX_LAUNCH((k_l0_op<double, kL0Apply>), g0, 256, 0, s, o);  // q = A p, alpha
         const Amg::Start0 s0 = amg.start0();
-        FX_LAUNCH(k_amg_update_start, nb, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
+        FX_LAUNCH(k_amg_update_start, gu, 256, 0, s, n, sc_.ptr, p_.ptr, q_.ptr, x, r_.ptr, dinv64, part_.ptr,
                   counter_.ptr, s0.r, s0.x, s0.d, s0.d4, s0.c2, s0.sq4, s0.hs);  // x, r, r.D^-1 r; the V-cycle's first step
         amg.apply(r_.ptr, zn, sc_.ptr, part_.ptr, counter_.ptr, amg.kcycle() ? zo : nullptr, s, true);  // z, r.z, beta
-        FX_LAUNCH(k_xpby, nb, 256, 0, s, nd, zn, sc_.ptr, p_.ptr);
+        FX_LAUNCH(k_xpby, gx, 256, 0, s, nd, zn, sc_.ptr, p_.ptr);
     };
     // Four iterations per graph replay between host checks. (A device-side loop
     // as a WHILE graph node, one or four iterations per body, measured 1-7 %
