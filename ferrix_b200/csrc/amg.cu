@@ -750,7 +750,8 @@ struct L0Op {
     int* counter;
     double* S;
     // FP32 smoother vectors (mixed precision): the gathered vector as float4 per
-    // node (x, y, z, 0) and the new direction written into the same layout
+    // node (x, y, z, 0) and the new direction written into the same layout; with FP16
+    // values and kL0H16Vec the directions are four halves per node (8 bytes) instead
     const float4* v4;
     float* d4_out;
     // FP16 values of the diagonally scaled matrix S A S (S = diag(a_ii)^-1/2): sqrt(a_ii)
