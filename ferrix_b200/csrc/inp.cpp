@@ -27,6 +27,8 @@
 #include <string_view>
 #include <thread>
 
+#include <unistd.h>
+
 #include "common.hpp"
 #include "model.hpp"
 
@@ -242,7 +244,7 @@ double Record::eval(const SolverTime& t, int64_t current_step) const {  // ampli
 // through an atomic counter by the calling thread, which always works on its own job,
 // and by the workers that take one of its helper entries from the queue; so concurrent
 // callers (request-loop slots) share the workers, and a caller finishes its job even
-// when no worker is free (or, in a forked child, none exists).
+// when no worker is free; a forked child runs its loops on the calling thread alone.
 namespace {
 struct HostJob {
     std::function<void(size_t)> f;
@@ -271,6 +273,10 @@ class HostPool {
     // f(0 .. ntasks-1), each once, on the caller and up to max_threads - 1 workers
     void run(size_t ntasks, size_t max_threads, std::function<void(size_t)> f) {
         if (ntasks == 0) return;
+        if (getpid() != pid_) {  // a forked child: no workers, and the queue's lock may be held
+            for (size_t t = 0; t < ntasks; ++t) f(t);
+            return;
+        }
         auto job = std::make_shared<HostJob>();
         job->f = std::move(f);
         job->ntasks = ntasks;
@@ -286,7 +292,7 @@ class HostPool {
     }
 
    private:
-    HostPool() {
+    HostPool() : pid_(getpid()) {
         const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
         nworkers_ = hw - 1;
         for (size_t k = 0; k < nworkers_; ++k) std::thread([this] { loop(); }).detach();
@@ -303,6 +309,7 @@ class HostPool {
             job->work();
         }
     }
+    pid_t pid_;
     size_t nworkers_ = 0;
     std::mutex m_;
     std::condition_variable cv_;

@@ -6,6 +6,7 @@ import ctypes as C
 import threading
 
 import numpy as np
+import pytest
 
 import ferrix_b200 as fx
 from ferrix_b200 import decks
@@ -63,3 +64,34 @@ def test_concurrent_parses_match_a_parse_alone():
             assert rc == 0
             for a, b in zip(arrays, alone[i][1]):
                 assert np.array_equal(a, b)
+
+
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded:DeprecationWarning")
+def test_parse_in_a_forked_child():
+    """A child forked after the parser's workers started (they are not copied by fork, and
+    the queue's lock may be held) parses on its own thread and gets the same arrays."""
+    import os
+    import select
+    import signal
+    lib = fx._lib.load()
+    text = decks.c3d20_box(6, 6, 24).encode()
+    rc, alone = _parse_export(lib, text)  # starts the workers in this process
+    assert rc == 0
+    r, w = os.pipe()
+    pid = os.fork()
+    if pid == 0:  # child: parse, report, leave without running the parent's cleanup
+        ok = 0
+        try:
+            rc2, arrays = _parse_export(lib, text)
+            ok = int(rc2 == 0 and all(np.array_equal(a, b) for a, b in zip(arrays, alone)))
+        finally:
+            os.write(w, bytes([ok]))
+            os._exit(0)
+    os.close(w)
+    ready, _, _ = select.select([r], [], [], 60.0)  # a child stuck on an inherited lock is ended
+    got = os.read(r, 1) if ready else b""
+    os.close(r)
+    if not ready:
+        os.kill(pid, signal.SIGKILL)
+    os.waitpid(pid, 0)
+    assert got == b"\x01"
